@@ -1,0 +1,64 @@
+// Engine state behind the C ABI: device context, resident seed sets.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/rpd.h"
+#include "bins.cuh"
+#include "knn.cuh"
+
+namespace rpd {
+
+// Owning device allocation that only grows.
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t want) {
+    if (want <= bytes && ptr) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&ptr, want ? want : 16);
+    if (e == cudaSuccess) bytes = want ? want : 16;
+    return e;
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(ptr);
+  }
+};
+
+void set_error(rpd_context *ctx, const std::string &msg);
+int map_cuda(rpd_context *ctx, cudaError_t e, const char *what);
+
+}  // namespace rpd
+
+struct rpd_context {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+};
+
+struct rpd_solver {
+  rpd_context *ctx = nullptr;
+  int n = 0;
+  int dim = 0;
+  rpd::DevBuf user;            // float4[n] as given
+  rpd::DevBuf stored;          // float4[n] stored (binned) order
+  rpd::DevBuf perm;            // int[n] stored -> user
+  rpd::DevBuf user_to_stored;  // int[n]
+  rpd::DevBuf counters;        // int[dim^3+1]
+  rpd::DevBuf bin_ws;
+  rpd::DevBuf ring_bound;      // float[dim+2]
+  rpd::DevBuf knn;             // unsigned[n*K]
+  rpd::DevBuf knn_user;        // int[n*K]
+  rpd::DevBuf counter64;       // unsigned long long[4]
+};

@@ -1,0 +1,275 @@
+// K-nearest neighbours on the binned seeds, one warp per seed (replaces the
+// reference's one-work-item heap search, knearests.cl:36-78).
+//
+// The warp scans Chebyshev shells of bins around the seed's bin.  Bins are
+// stored x-fastest, so every row of a shell is one contiguous range of the
+// stored seeds: the lanes enumerate the rows, prefix-sum their point counts
+// and then take 32 candidates per round with coalesced float4 loads.
+// Candidates closer than the current K-th best are staged in a 32-entry
+// shared-memory buffer per warp; a full stage is bitonic-sorted across the
+// warp and merged into
+// the K-best list (32*S keys, S per lane, sorted lane-major) by S bitonic
+// merges.  Keys are (float distance bits << 32 | stored index): ties break
+// by index.  A shell is skipped once the K-th best is closer than the
+// shell's bound ((shell-1) * bin width)^2, checked at shell granularity
+// after every pending candidate is merged -- the exact rule of the oracle's
+// exact mode, so lists agree bit for bit.
+#include "knn.cuh"
+
+namespace rpd {
+
+namespace {
+
+constexpr unsigned long long kEmptyKey = (0x7f800000ull << 32) | 0xffffffffull;
+
+__device__ __forceinline__ unsigned long long umin64(unsigned long long a, unsigned long long b) {
+  return a < b ? a : b;
+}
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) {
+  return a < b ? b : a;
+}
+
+// Sorts a bitonic sequence held one key per lane into ascending lane order.
+__device__ __forceinline__ unsigned long long bitonic_merge32(unsigned long long v, int lane) {
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(kFull, v, j);
+    v = (lane & j) ? umax64(v, o) : umin64(v, o);
+  }
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long bitonic_sort32(unsigned long long v, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(kFull, v, j);
+      const bool up = (lane & k) == 0;
+      const bool lower = (lane & j) == 0;
+      v = (lower == up) ? umin64(v, o) : umax64(v, o);
+    }
+  }
+  return v;
+}
+
+// Merges 32 staged keys into the sorted list best[0..S) (slot s holds ranks
+// s*32 .. s*32+31).  Keeps the 32*S smallest.
+template <int S>
+__device__ __forceinline__ void merge_stage(unsigned long long (&best)[S], unsigned long long stage, int lane) {
+  unsigned long long low = bitonic_sort32(stage, lane);
+#pragma unroll
+  for (int s = S - 1; s >= 0; --s) {
+    const unsigned long long rev = __shfl_sync(kFull, low, 31 - lane);
+    const unsigned long long lo = umin64(best[s], rev);
+    const unsigned long long hi = umax64(best[s], rev);
+    if (s + 1 < S) best[s + 1] = bitonic_merge32(hi, lane);
+    low = bitonic_merge32(lo, lane);
+  }
+  best[0] = low;
+}
+
+template <int S>
+__device__ __forceinline__ unsigned long long key_at(const unsigned long long (&best)[S], int pos) {
+  const int slot = pos >> 5, src = pos & 31;
+  unsigned long long v = kEmptyKey;
+#pragma unroll
+  for (int s = 0; s < S; ++s)
+    if (s == slot) v = best[s];
+  return __shfl_sync(kFull, v, src);
+}
+
+// Row ranges of shell `ring` (rings 0 and 1 are scanned together as the
+// 3x3x3 block, "ring 0").  Row q of the shell covers bins (x, cy+j, cz+k):
+// the whole x span on the shell's faces, else the two end bins.
+struct ShellRows {
+  int cx, cy, cz, dim, ring;
+  __device__ __forceinline__ int rows() const {
+    const int w = 2 * (ring == 0 ? 1 : ring) + 1;
+    return w * w;
+  }
+  // Point ranges [a0, a0+l0) and [a1, a1+l1) of row q.
+  __device__ __forceinline__ void ranges(int q, const int *__restrict__ counters, int &a0, int &l0, int &a1,
+                                         int &l1) const {
+    const int r = ring == 0 ? 1 : ring;
+    const int w = 2 * r + 1;
+    const int j = q % w - r, k = q / w - r;
+    a0 = l0 = a1 = l1 = 0;
+    const int y = cy + j, z = cz + k;
+    if (y < 0 || y >= dim || z < 0 || z >= dim) return;
+    const int rowbase = (y + z * dim) * dim;
+    const bool face = ring == 0 || j == -r || j == r || k == -r || k == r;
+    if (face) {
+      const int x0 = max(cx - r, 0), x1 = min(cx + r, dim - 1);
+      a0 = __ldg(&counters[rowbase + x0]);
+      l0 = __ldg(&counters[rowbase + x1 + 1]) - a0;
+    } else {
+      if (cx - r >= 0) {
+        a0 = __ldg(&counters[rowbase + cx - r]);
+        l0 = __ldg(&counters[rowbase + cx - r + 1]) - a0;
+      }
+      if (cx + r < dim) {
+        a1 = __ldg(&counters[rowbase + cx + r]);
+        l1 = __ldg(&counters[rowbase + cx + r + 1]) - a1;
+      }
+    }
+  }
+};
+
+template <int S>
+__global__ void __launch_bounds__(256) k_knn(const float4 *__restrict__ stored, const int *__restrict__ counters,
+                                             int dim, const int *__restrict__ ids, int num, int K,
+                                             const float *__restrict__ ring_bound, unsigned *__restrict__ out,
+                                             unsigned long long *__restrict__ candidates) {
+  __shared__ unsigned long long stage_buf[kKnnThreads / 32][32];
+  const int lane = threadIdx.x & 31;
+  unsigned long long *stage = stage_buf[threadIdx.x >> 5];
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= num) return;  // warp-uniform
+  const int pin = ids ? ids[w] : w;
+  const float4 p = stored[pin];
+  const int cin = bin_of(p, dim);
+  ShellRows sh;
+  sh.cx = cin % dim;
+  sh.cy = (cin / dim) % dim;
+  sh.cz = cin / (dim * dim);
+  sh.dim = dim;
+
+  unsigned long long best[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) best[s] = kEmptyKey;
+  int nstage = 0;
+  unsigned long long kth = kEmptyKey;
+  unsigned long long ncand = 0;
+
+  for (int ring = 0; ring <= dim; ring = ring == 0 ? 2 : ring + 1) {
+    if (ring >= 2) {
+      // whole-shell exit: the K-th best beats the shell bound
+      const float kd = __uint_as_float(unsigned(kth >> 32));
+      if (kd < ring_bound[ring]) break;
+      if (sh.cx - ring < 0 && sh.cy - ring < 0 && sh.cz - ring < 0 && sh.cx + ring >= dim &&
+          sh.cy + ring >= dim && sh.cz + ring >= dim)
+        break;  // the shell lies outside the grid
+    }
+    sh.ring = ring;
+    const int nrows = sh.rows();
+    for (int q0 = 0; q0 < nrows; q0 += 32) {
+      int a0 = 0, l0 = 0, a1 = 0, l1 = 0;
+      if (q0 + lane < nrows) sh.ranges(q0 + lane, counters, a0, l0, a1, l1);
+      const int cnt = l0 + l1;
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int total = __shfl_sync(kFull, incl, 31);
+      for (int base = 0; base < total; base += 32) {
+        const int c = base + lane;
+        // owner lane: the first lane whose inclusive count exceeds c
+        int lo = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int v = __shfl_sync(kFull, incl, lo + step - 1);
+          if (v <= c) lo += step;
+        }
+        const int owner = lo;
+        const int o_incl = __shfl_sync(kFull, incl, owner);
+        const int o_cnt = __shfl_sync(kFull, cnt, owner);
+        const int o_a0 = __shfl_sync(kFull, a0, owner);
+        const int o_l0 = __shfl_sync(kFull, l0, owner);
+        const int o_a1 = __shfl_sync(kFull, a1, owner);
+        unsigned long long key = kEmptyKey;
+        if (c < total) {
+          const int off = c - (o_incl - o_cnt);
+          const int ptr = off < o_l0 ? o_a0 + off : o_a1 + (off - o_l0);
+          if (ptr != pin) {
+            const float4 qv = __ldg(&stored[ptr]);
+            const float dx = __fsub_rn(qv.x, p.x), dy = __fsub_rn(qv.y, p.y), dz = __fsub_rn(qv.z, p.z);
+            const float d = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            key = (static_cast<unsigned long long>(__float_as_uint(d)) << 32) | unsigned(ptr);
+            ++ncand;
+          }
+        }
+        const bool accept = key < kth;
+        const unsigned m = __ballot_sync(kFull, accept);
+        const int nacc = __popc(m);
+        if (nacc == 0) continue;
+        if (nstage + nacc > 32) {
+          __syncwarp();
+          const unsigned long long v = lane < nstage ? stage[lane] : kEmptyKey;
+          __syncwarp();
+          merge_stage<S>(best, v, lane);
+          nstage = 0;
+          kth = key_at<S>(best, K - 1);
+        }
+        if (accept) stage[nstage + __popc(m & ((1u << lane) - 1u))] = key;
+        nstage += nacc;
+      }
+    }
+    if (nstage) {
+      __syncwarp();
+      const unsigned long long v = lane < nstage ? stage[lane] : kEmptyKey;
+      __syncwarp();
+      merge_stage<S>(best, v, lane);
+      nstage = 0;
+      kth = key_at<S>(best, K - 1);
+    }
+  }
+  unsigned *row = out + size_t(w) * K;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int pos = s * 32 + lane;
+    if (pos < K) row[pos] = unsigned(best[s] & 0xffffffffull);
+  }
+  if (candidates) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(kFull, ncand, o);
+    if (lane == 0) atomicAdd(candidates, ncand);
+  }
+}
+
+}  // namespace
+
+int knn_slots(int K) {
+  const int s = (K + 31) / 32;
+  if (s <= 1) return 1;
+  if (s <= 2) return 2;
+  if (s <= 3) return 3;
+  if (s <= 4) return 4;
+  if (s <= 6) return 6;
+  if (s <= 8) return 8;
+  return -1;
+}
+
+void ring_bounds(int dim, float *bound) {
+  // ((ring-1) * 1000/dim)^2 in float, ring 0 -> 0 (knearests.cpp:84-86).
+  for (int ring = 0; ring <= dim + 1; ++ring) {
+    if (ring == 0) {
+      bound[ring] = 0.f;
+      continue;
+    }
+    const float d = 1000.f * float(ring - 1) / float(dim);
+    bound[ring] = d * d;
+  }
+}
+
+cudaError_t knn_launch(const float4 *stored, const int *counters, int dim, const int *ids, int num, int K,
+                       const float *ring_bound, unsigned *out, unsigned long long *candidates, cudaStream_t st) {
+  if (num <= 0) return cudaSuccess;
+  const int threads = kKnnThreads;
+  const long warps = num;
+  const int blocks = int((warps * 32 + threads - 1) / threads);
+  switch (knn_slots(K)) {
+    case 1: k_knn<1><<<blocks, threads, 0, st>>>(stored, counters, dim, ids, num, K, ring_bound, out, candidates); break;
+    case 2: k_knn<2><<<blocks, threads, 0, st>>>(stored, counters, dim, ids, num, K, ring_bound, out, candidates); break;
+    case 3: k_knn<3><<<blocks, threads, 0, st>>>(stored, counters, dim, ids, num, K, ring_bound, out, candidates); break;
+    case 4: k_knn<4><<<blocks, threads, 0, st>>>(stored, counters, dim, ids, num, K, ring_bound, out, candidates); break;
+    case 6: k_knn<6><<<blocks, threads, 0, st>>>(stored, counters, dim, ids, num, K, ring_bound, out, candidates); break;
+    case 8: k_knn<8><<<blocks, threads, 0, st>>>(stored, counters, dim, ids, num, K, ring_bound, out, candidates); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace rpd

@@ -1,0 +1,30 @@
+"""CPU tests of the oracle itself (no GPU)."""
+import numpy as np
+import pytest
+
+import oracle
+from seeds_util import jittered, uniform
+
+
+def test_exact_knn_matches_reference_order_on_random_input():
+    x = uniform(20000, seed=11).astype(np.float64)
+    a = oracle.knn(x, 20, knn_mode=0)
+    b = oracle.knn(x, 20, knn_mode=1)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not oracle.has_reference_kernels(), reason="reference kernels not built here")
+@pytest.mark.parametrize("use_double", [0, 1])
+def test_restatement_bitexact_with_reference_kernels_no_grid(use_double):
+    x = jittered(22, seed=4, weights=True).astype(np.float64)
+    b1, s1 = oracle.solve(x, K=20, P=25, V=30, kernels=1, use_double=use_double)
+    b0, s0 = oracle.solve(x, K=20, P=25, V=30, kernels=0, use_double=use_double)
+    assert np.array_equal(s0, s1)
+    assert np.array_equal(b0, b1)
+
+
+def test_unit_cube_volume_fp64():
+    x = uniform(5000, seed=3).astype(np.float64)
+    b, s = oracle.solve(x, K=30, P=40, V=60, use_double=True)
+    assert (s == oracle.SUCCESS).all()
+    assert abs(b[:, 3].sum() - 1e9) < 1e-3
