@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Restricted power diagram throughput on B200: cells/s.
+
+One step = one full solve (VoroAlgo::launch: kNN, clipping, domain
+restriction, integration, retry passes) of a resident seed set.  Each rank
+drives one GPU and solves its own diagram (weak scaling, no data-path
+collective); rank 0 prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gpu-restricted-power-diagrams_b200")
+for p in (PKG, ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "cells/s at 1M seeds, mass rel-err ≤1e-5 vs FP64; served p50/p99 ms"
+
+CONFIGS = {
+    # the headline: 1M weighted seeds, jittered 100^3 lattice, blob at 200^3
+    "weighted-1m": dict(kind="jittered", m=100, weights=True, grid="blob", gsize=200, nell=5, gseed=2, sseed=2,
+                        K=50, P=30, V=40, T=100,
+                        desc="1M weighted seeds on a jittered 100^3 lattice (h=0.01, +-0.25h, w~U[0,0.1h^2]), "
+                             "5-ellipsoid blob domain voxelized at 200^3 (Kuhn tets), K=50 P=30 V=40 T=100"),
+    "voronoi-100k": dict(kind="uniform", n=100_000, weights=False, grid="blob", gsize=100, nell=5, gseed=2,
+                         sseed=1, K=70, P=30, V=40, T=100,
+                         desc="100K i.i.d. uniform seeds (weights 0), 5-ellipsoid blob at 100^3, K=70 P=30 V=40"),
+}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_seeds(cfg, rank):
+    from rpd import synth
+
+    s = cfg["sseed"] + 1000 * rank
+    if cfg["kind"] == "jittered":
+        return synth.jittered_lattice(cfg["m"], seed=s, weights=cfg["weights"])
+    return synth.uniform(cfg["n"], seed=s)
+
+
+def make_grid(cfg):
+    import rpd
+
+    if cfg["grid"] == "blob":
+        return rpd.Grid.blob(cfg["gsize"], cfg["nell"], cfg["gseed"])
+    if cfg["grid"] == "cube":
+        return rpd.Grid.cube(cfg["gsize"])
+    return None
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        self.index = vis.split(",")[local_rank] if vis else str(local_rank)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", self.index], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(x, grid, cfg, target_s=10.0):
+    """The reference's own kernels compiled for the host CPU (or, when they
+    were not built here, the oracle restatement) on every host thread, over
+    a bounded sample of the same diagram: every stride-th binned seed."""
+    import oracle
+
+    kind = "reference" if oracle.has_reference_kernels() else "port"
+    a = grid.arrays() if grid is not None else None
+    ga = (oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+          if a is not None else None)
+    xd = x.astype(np.float64)
+    kw = dict(grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2, vhs1=2, use_double=False,
+              kernels=1 if kind == "reference" else 0, knn_mode=0)
+
+    def run(stride):
+        # the timed work: neighbour search + cells of every pass (binning of
+        # the seed set and the grid upload are excluded, as on the device)
+        _, _, st = oracle.solve(xd, sample_stride=stride, return_stats=True, **kw)
+        return st["knn_seconds"] + st["cell_seconds"], st
+
+    n = len(x)
+    stride0 = max(1, n // 20000)
+    t, st = run(stride0)
+    cells0 = st["pass_cells"][0]
+    rate0 = cells0 / max(t, 1e-9)
+    stride = max(1, int(round(n / max(1.0, rate0 * target_s))))
+    t, st = run(stride)
+    cells = st["pass_cells"][0]
+    return {"value": cells / t, "unit": "cells/s", "cores": os.cpu_count(), "kind": kind,
+            "sample": f"{cells} cells (every {stride}th binned seed of the same {n}-seed diagram, all passes), "
+                      f"{t:.2f} s on {os.cpu_count()} host threads"}
+
+
+def run_reference(args, cfg, rank, world):
+    """--impl reference: the reference's CPU implementation of the path on the
+    host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    x = make_seeds(cfg, 0)
+    grid = make_grid(cfg)
+    import oracle
+
+    kind = "reference" if oracle.has_reference_kernels() else "port"
+    a = grid.arrays() if grid is not None else None
+    ga = (oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+          if a is not None else None)
+    xd = x.astype(np.float64)
+    n = len(x)
+    stride = max(1, n // 100000)
+    kw = dict(grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2, vhs1=2, use_double=False,
+              kernels=1 if kind == "reference" else 0, knn_mode=0, sample_stride=stride, return_stats=True)
+    for _ in range(args.warmup):
+        oracle.solve(xd, **kw)
+    times, cells = [], 0
+    for _ in range(args.steps):
+        _, _, st = oracle.solve(xd, **kw)
+        times.append(st["knn_seconds"] + st["cell_seconds"])
+        cells = st["pass_cells"][0]
+    t = sum(times) / len(times)
+    value = cells / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 half-space predicate, VHSAlgo 2)",
+        "data": "synthetic", "config": {"workload": args.config, "description": cfg["desc"], "n_seeds": n},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": os.cpu_count(), "kind": kind,
+                         "sample": f"{cells} cells per step (every {stride}th binned seed of the {n}-seed diagram)"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg, rank, world, local):
+    import torch
+
+    import rpd
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    ctx = rpd.Context(local)
+    x = make_seeds(cfg, rank)
+    grid = make_grid(cfg)
+    n = len(x)
+    params = rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"])
+    solver = rpd.Solver(ctx).set_points(x)
+    if grid is not None:
+        solver.set_grid(grid)
+    for _ in range(args.warmup):
+        solver.launch(params)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    clocks = ClockSampler(local)
+    step_ms, cell_ms, knn_ms, launches, npasses = [], [], [], [], []
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        solver.launch(params)
+        st = solver.stats()
+        step_ms.append(st["total_ms"])
+        cell_ms.append(st["passes"][0]["cell_ms"])
+        knn_ms.append(st["passes"][0]["knn_ms"])
+        launches.append(st["kernel_launches"])
+        npasses.append(st["npasses"])
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    last_stats = solver.stats()
+    ms = sum(step_ms) / len(step_ms)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * world / (ms / 1e3)
+
+    # end to end through the C ABI from pinned host memory: binning upload,
+    # solve, moments download, every step
+    x_pin = torch.from_numpy(x).pin_memory()
+    out_pin = torch.empty((n, 4), dtype=torch.float64).pin_memory()
+    xa, oa = x_pin.numpy(), out_pin.numpy()
+    e2e_s = []
+    nrep = max(3, min(args.steps, 10))
+    for _ in range(nrep):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.check(rpd.lib().rpd_solver_set_points(solver.h, rpd._ptr(xa), n, rpd.RPD_HOST))
+        solver.launch(params)
+        ctx.check(rpd.lib().rpd_solver_get_moments(solver.h, rpd._ptr(oa), rpd.RPD_HOST))
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_t = sum(e2e_s) / len(e2e_s)
+    if world > 1:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+
+    # roofline of the dominant kernel (the cell kernel of the first pass):
+    # minimal DRAM bytes per launch = the neighbour table and the seeds read
+    # once, the moments and statuses written once, the grid arrays read once
+    a = grid.arrays() if grid is not None else None
+    grid_bytes = 0 if a is None else int(a["in_domain"].nbytes + a["offsets"].nbytes + a["tri_list"].nbytes +
+                                         a["triangles"].nbytes + len(a["points"]) * 16)
+    alg_bytes = n * (4 * cfg["K"] + 16 + 32 + 4) + grid_bytes
+    cell_avg_ms = sum(cell_ms) / len(cell_ms)
+    achieved = alg_bytes / (cell_avg_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "cell_kernel_traffic.json")
+    if os.path.exists(prof):
+        try:
+            with open(prof) as f:
+                tp = json.load(f)
+            if tp.get("workload") == args.config:
+                traffic = tp.get("bytes_per_launch")
+        except Exception:
+            pass
+    line = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 geometry on f32 seeds (FP64 cofactor predicates and integration)",
+        "data": "synthetic",
+        "config": {"workload": args.config, "description": cfg["desc"], "n_seeds_per_gpu": n,
+                   "parallelism": f"{world} independent diagrams, one per GPU",
+                   "l2": "flushed between steps (256 MB write, untimed)"},
+        "e2e": {"value": n * world / e2e_t, "unit": "cells/s", "h2d_bytes_per_step": int(x.nbytes),
+                "d2h_bytes_per_step": int(n * 32),
+                "path": "rpd_solver_set_points(host) + rpd_solver_launch + rpd_solver_get_moments(host)"},
+        "gpu_launches": int(sum(launches)),
+        "roofline": {"kernel": "k_cell (first pass)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "alg_bytes_per_launch": alg_bytes, "launch_ms": cell_avg_ms,
+                     "note": "issue-bound clipping kernel; HBM fraction shown for completeness"},
+        "clocks": clk,
+        "detail": {"knn_ms": sum(knn_ms) / len(knn_ms), "cell_ms_first_pass": cell_avg_ms,
+                   "passes": last_stats["passes"], "status": last_stats["status"],
+                   "npasses": npasses[-1], "step_ms": step_ms},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(x, grid, cfg, target_s=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="weighted-1m", choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg, rank, world)
+    else:
+        run_ours(args, cfg, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,70 @@
+// Per-seed restricted power cell: clipping, domain restriction, integration.
+#pragma once
+#include "common.cuh"
+
+namespace rpd {
+
+// Domain grid on the device (the reference Grid, Grid.h:14-70).
+struct DevGrid {
+  int size = 0;                       // voxels per axis
+  float voxel = 0.f;                  // 1000 / size
+  const signed char *flags = nullptr; // size^3 corner flags: 0 out, 1 border, 2 in
+  const float4 *points = nullptr;     // triangle vertices (w unused)
+  const int *tris = nullptr;          // 3 ids per triangle
+  const int *list = nullptr;          // per-voxel sorted triangle ids
+  const int *offsets = nullptr;       // size^3 + 1
+  int has_border_corners = 0;         // any flag == 1
+  // Summed-volume table, (size+1)^3, of voxels that are not plainly outside
+  // (first-corner flag != 0 or a non-empty triangle list); null: unused.
+  const int *sat = nullptr;
+};
+
+// Counters of one launch (optional): cells by outcome and work done.
+enum CellCounter {
+  kCtrPlanesTested = 0,   // neighbour planes tested against the cell
+  kCtrClips,              // clips that removed vertices
+  kCtrVertexTests,        // vertex half-space tests
+  kCtrVerticesMade,       // vertices created
+  kCtrBoundaryCells,      // cells with at least one boundary triangle
+  kCtrTriangles,          // boundary triangles processed
+  kCtrExports,            // integrations (cell or cone pieces)
+  kCtrExportVertices,     // vertices integrated
+  kCtrOutside,            // cells proven outside the domain before the end of clipping
+  kCtrNum
+};
+
+struct CellLaunch {
+  const float4 *stored = nullptr;  // n seeds in stored order (reference frame)
+  int n = 0;
+  const unsigned *knn = nullptr;   // num rows of K stored neighbour ids
+  int K = 0;
+  const int *ids = nullptr;        // stored ids of the rows (null: row i = seed i)
+  int num = 0;
+  int P = 0, V = 0, T = 0;         // caps of this pass
+  float cube_eps = 0.f;            // box [-eps, 1000+eps]^3
+  int out_domain = 0;              // GRID_OUT_DOMAIN fallback for the start corner
+  int early_out = 1;               // stop clipping cells proven outside the domain (needs grid.sat)
+  DevGrid grid;                    // grid.size == 0: no domain
+  int *status = nullptr;           // n, stored order
+  double4 *out = nullptr;          // n, stored order: (m*x, m*y, m*z, m)
+  unsigned long long *counters = nullptr;  // kCtrNum, optional
+  // Trace of one cell (debugging): every clip and integration of stored seed
+  // `trace_seed` appended to `trace` as records of kTraceRecord doubles;
+  // trace[0] counts the records.
+  int trace_seed = -1;
+  double *trace = nullptr;
+  int trace_cap = 0;  // records
+};
+constexpr int kTraceRecord = 12;
+
+// Largest caps of one build: P <= 255 (uchar plane ids in the reference,
+// voronoi.cpp:867), V <= 256, T <= kMaxT.
+constexpr int kMaxP = 255;
+constexpr int kMaxV = 256;
+constexpr int kMaxT = 4096;
+
+// Shared memory bytes one warp needs for these caps.
+size_t cell_warp_smem(int P, int V, int T, bool grid);
+cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st);
+
+}  // namespace rpd

@@ -1,5 +1,6 @@
 // Host side of the engine: context, seed binning and neighbour queries
 // behind the C ABI declared in include/rpd.h.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -38,9 +39,152 @@ __global__ void k_knn_to_user(const unsigned *__restrict__ knn, const int *__res
   out[i] = v == 0xffffffffu ? -1 : perm[v];
 }
 
+// Failing cells among `ids` (all seeds when null): f0 = status != success,
+// f1 = failing and (cond == 0 or status != empty_cell); status histogram of
+// the failing ones (recomputeIds, voronoi.cpp:793-826).
+__global__ void k_fail_flags(const int *__restrict__ ids, int num, const int *__restrict__ status, int cond,
+                             int *__restrict__ f0, int *__restrict__ f1, int *__restrict__ hist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > num) return;
+  if (i == num) {
+    f0[i] = 0;
+    f1[i] = 0;
+    return;
+  }
+  const int sid = ids ? ids[i] : i;
+  const int st = status[sid];
+  const bool fail = st != kSuccess;
+  f0[i] = fail;
+  f1[i] = fail && (cond == 0 || st != kEmptyCell);
+  if (fail) atomicAdd(&hist[st], 1);
+}
+
+__global__ void k_fail_scatter(const int *__restrict__ ids, int num, const int *__restrict__ f0,
+                               const int *__restrict__ s0, const int *__restrict__ f1, const int *__restrict__ s1,
+                               int *__restrict__ out0, int *__restrict__ out1, int *__restrict__ counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == num) {
+    counts[0] = s0[num];
+    counts[1] = s1[num];
+  }
+  if (i >= num) return;
+  const int sid = ids ? ids[i] : i;
+  if (f0[i]) out0[s0[i]] = sid;
+  if (f1[i]) out1[s1[i]] = sid;
+}
+
+template <class T>
+__global__ void k_gather_user(const T *__restrict__ src, const int *__restrict__ user_to_stored, int n,
+                              T *__restrict__ dst) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n) dst[u] = src[user_to_stored[u]];
+}
+
+__global__ void k_status_hist(const int *__restrict__ status, int n, int *__restrict__ hist) {
+  __shared__ int h[kStatusNum];
+  if (threadIdx.x < kStatusNum) h[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int st = status[i];
+    if (st >= 0 && st < kStatusNum) atomicAdd(&h[st], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < kStatusNum && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+}
+
 }  // namespace rpd
 
 using namespace rpd;
+
+namespace {
+
+// Failing ids of the cells in `ids_in` (null: all n) into out0 (all
+// failing) and out1 (failing, filtered by cond), their counts and the status
+// histogram; synchronous.
+int recompute_ids(rpd_solver *s, const int *ids_in, int num, int cond, int *out0, int *out1, int &n0, int &n1,
+                  int hist[kStatusNum]) {
+  rpd_context *ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const size_t nsc = scan_workspace_ints(num + 1);
+  if ((e = s->fail_ws.ensure(sizeof(int) * (4 * size_t(num + 1) + nsc))) != cudaSuccess)
+    return map_cuda(ctx, e, "alloc fail ws");
+  int *f0 = s->fail_ws.as<int>(), *f1 = f0 + (num + 1), *s0 = f1 + (num + 1), *s1 = s0 + (num + 1),
+      *tiles = s1 + (num + 1);
+  int *h = s->hist.as<int>();
+  if ((e = cudaMemsetAsync(h, 0, sizeof(int) * 16, st)) != cudaSuccess) return map_cuda(ctx, e, "memset");
+  const int tb = 256;
+  k_fail_flags<<<(num + 1 + tb - 1) / tb, tb, 0, st>>>(ids_in, num, s->status.as<int>(), cond, f0, f1, h);
+  if ((e = exclusive_scan(f0, s0, num + 1, tiles, st)) != cudaSuccess) return map_cuda(ctx, e, "scan");
+  if ((e = exclusive_scan(f1, s1, num + 1, tiles, st)) != cudaSuccess) return map_cuda(ctx, e, "scan");
+  k_fail_scatter<<<(num + 1 + tb - 1) / tb, tb, 0, st>>>(ids_in, num, f0, s0, f1, s1, out0, out1, h + 12);
+  s->stats.kernel_launches += 8;  // flags, 2 scans of 3 kernels, scatter
+  int hh[16];
+  if ((e = cudaMemcpyAsync(hh, h, sizeof(hh), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return map_cuda(ctx, e, "copy hist");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "recompute ids");
+  for (int i = 0; i < kStatusNum; ++i) hist[i] = hh[i];
+  n0 = hh[12];
+  n1 = hh[13];
+  return RPD_OK;
+}
+
+// One pass (VoroAlgoComputeData::launch, voronoi.cpp:861-1036): the K
+// nearest of the listed seeds, then their cells with this pass's caps.
+static_assert(int(RPD_CTR_NUM) == int(kCtrNum), "counter enums out of sync");
+
+int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T, float eps, int out_domain,
+             bool counters, bool early_out) {
+  rpd_context *ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  rpd_stats &S = s->stats;
+  const int pi = S.npasses;
+  if ((e = s->knn.ensure(sizeof(unsigned) * size_t(num) * K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
+  cudaEvent_t ev[3];
+  for (auto &x : ev) cudaEventCreate(&x);
+  unsigned long long *ctr = counters ? s->counter64.as<unsigned long long>() : nullptr;
+  cudaEventRecord(ev[0], st);
+  e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, ids, num, K, s->ring_bound.as<float>(),
+                 s->knn.as<unsigned>(), ctr ? ctr + RPD_CTR_NUM : nullptr, st);
+  if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
+  cudaEventRecord(ev[1], st);
+  CellLaunch a;
+  a.stored = s->stored.as<float4>();
+  a.n = s->n;
+  a.knn = s->knn.as<unsigned>();
+  a.K = K;
+  a.ids = ids;
+  a.num = num;
+  a.P = P;
+  a.V = V;
+  a.T = T;
+  a.cube_eps = eps;
+  a.out_domain = out_domain;
+  a.early_out = early_out ? 1 : 0;
+  a.grid = s->grid;
+  a.status = s->status.as<int>();
+  a.out = s->out.as<double4>();
+  a.counters = ctr;
+  if ((e = cell_launch(a, st)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+  cudaEventRecord(ev[2], st);
+  if ((e = cudaEventSynchronize(ev[2])) != cudaSuccess) return map_cuda(ctx, e, "pass");
+  if (pi < 8) {
+    S.pass_cells[pi] = num;
+    S.pass_K[pi] = K;
+    S.pass_P[pi] = P;
+    S.pass_V[pi] = V;
+    S.pass_T[pi] = T;
+    cudaEventElapsedTime(&S.pass_knn_ms[pi], ev[0], ev[1]);
+    cudaEventElapsedTime(&S.pass_cell_ms[pi], ev[1], ev[2]);
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  S.npasses++;
+  S.kernel_launches += num > 0 ? 2 : 0;  // neighbours + cells
+  return RPD_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -199,6 +343,256 @@ int rpd_solver_knn(rpd_solver *s, int K, int *knn_user, rpd_mem where, float *de
   if (device_ms) cudaEventElapsedTime(device_ms, ev[0], ev[1]);
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
+  return RPD_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+void rpd_params_default(rpd_params *p) {
+  if (!p) return;
+  p->K = 20;
+  p->P = 25;
+  p->V = 30;
+  p->T = 100;
+  p->max_extra_passes = 5;
+  p->cube_eps = -1.f;
+  p->out_domain = -1;
+  p->flags = 0;
+}
+
+int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
+  if (!s) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  s->grid = DevGrid();
+  if (!gh) return RPD_OK;
+  const HostGrid *g = host_grid(gh);
+  const size_t nv = size_t(g->size) * g->size * g->size;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  if ((e = s->g_flags.ensure(nv)) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
+  if ((e = s->g_points.ensure(sizeof(float) * g->points.size())) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
+  if ((e = s->g_tris.ensure(sizeof(int) * g->triangles.size())) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
+  if ((e = s->g_list.ensure(sizeof(int) * g->tri_list.size())) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
+  if ((e = s->g_offsets.ensure(sizeof(int) * g->offsets.size())) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
+  cudaMemcpyAsync(s->g_flags.ptr, g->in_domain.data(), nv, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->g_points.ptr, g->points.data(), sizeof(float) * g->points.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->g_tris.ptr, g->triangles.data(), sizeof(int) * g->triangles.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->g_list.ptr, g->tri_list.data(), sizeof(int) * g->tri_list.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->g_offsets.ptr, g->offsets.data(), sizeof(int) * g->offsets.size(), cudaMemcpyHostToDevice, st);
+  // summed-volume table of the voxels that are not plainly outside (a
+  // first-corner flag other than 0, or triangles): lets a cell prove early
+  // that the restriction will give it nothing
+  const int S = g->size, S1 = S + 1;
+  std::vector<int> sat(size_t(S1) * S1 * S1, 0);
+  for (int z = 0; z < S; ++z)
+    for (int y = 0; y < S; ++y)
+      for (int x = 0; x < S; ++x) {
+        const size_t v = x + size_t(S) * (y + size_t(S) * z);
+        const int f = (g->in_domain[v] != 0 || g->offsets[v + 1] > g->offsets[v]) ? 1 : 0;
+        auto at = [&](int i, int j, int k) -> int & { return sat[i + size_t(S1) * (j + size_t(S1) * k)]; };
+        at(x + 1, y + 1, z + 1) = f + at(x, y + 1, z + 1) + at(x + 1, y, z + 1) + at(x + 1, y + 1, z) -
+                                  at(x, y, z + 1) - at(x, y + 1, z) - at(x + 1, y, z) + at(x, y, z);
+      }
+  if ((e = s->g_sat.ensure(sizeof(int) * sat.size())) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
+  cudaMemcpyAsync(s->g_sat.ptr, sat.data(), sizeof(int) * sat.size(), cudaMemcpyHostToDevice, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "upload grid");
+  DevGrid d;
+  d.size = g->size;
+  d.voxel = g->voxel;
+  d.flags = s->g_flags.as<const signed char>();
+  d.points = s->g_points.as<const float4>();
+  d.tris = s->g_tris.as<const int>();
+  d.list = s->g_list.as<const int>();
+  d.offsets = s->g_offsets.as<const int>();
+  d.sat = s->g_sat.as<const int>();
+  d.has_border_corners = 0;
+  for (char c : g->in_domain)
+    if (c == 1) {
+      d.has_border_corners = 1;
+      break;
+    }
+  s->grid = d;
+  return RPD_OK;
+}
+
+int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
+  if (!s || s->n <= 0) return RPD_ERR_INVALID;
+  rpd_params p;
+  if (pp) p = *pp;
+  else rpd_params_default(&p);
+  rpd_context *ctx = s->ctx;
+  if (p.K < 1 || knn_slots(p.K) < 0 || p.P < 7 || p.P > kMaxP || p.V < 8 || p.V > kMaxV || p.T < 0 ||
+      p.T > kMaxT) {
+    set_error(ctx, "caps out of range (1<=K<=256, 7<=P<=255, 8<=V<=256, 0<=T<=4096)");
+    return RPD_ERR_CAPACITY;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const int n = s->n;
+  cudaError_t e;
+  if ((e = s->out.ensure(sizeof(double4) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc out");
+  if ((e = s->status.ensure(sizeof(int) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc status");
+  if ((e = s->ids_a.ensure(sizeof(int) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc ids");
+  if ((e = s->ids_b.ensure(sizeof(int) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc ids");
+  if ((e = s->ids_c.ensure(sizeof(int) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc ids");
+  if ((e = s->hist.ensure(sizeof(int) * 16)) != cudaSuccess) return map_cuda(ctx, e, "alloc hist");
+  if ((e = s->counter64.ensure(sizeof(unsigned long long) * (RPD_CTR_NUM + 1))) != cudaSuccess)
+    return map_cuda(ctx, e, "alloc counters");
+  const bool counters = (p.flags & RPD_FLAG_COUNTERS) != 0;
+  if (counters) cudaMemsetAsync(s->counter64.ptr, 0, sizeof(unsigned long long) * (RPD_CTR_NUM + 1), st);
+  s->stats = rpd_stats{};
+  s->have_results = false;
+  const bool grid = s->grid.size > 0;
+  const float eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, st);
+  // pass "first" + "tr_overflow" in one: T = caps.T from the start gives
+  // every cell the result the two reference passes give it
+  // (voronoi.cpp:1275-1310)
+  const int T0 = p.T;
+  const bool early = !(p.flags & RPD_FLAG_NO_EARLY_OUT);
+  int rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
+  if (rc != RPD_OK) return rc;
+  if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {
+    int hist[kStatusNum];
+    int n0 = 0, n1 = 0;
+    int *A = s->ids_a.as<int>(), *B = s->ids_b.as<int>(), *Cc = s->ids_c.as<int>();
+    // extra passes (voronoi.cpp:1311-1376): caps grow x1.5 by failing status
+    if ((rc = recompute_ids(s, nullptr, n, 0, A, Cc, n0, n1, hist)) != RPD_OK) return rc;
+    int K = p.K, P = p.P, V = p.V, T = p.T;
+    const int out_domain = p.out_domain >= 0 ? p.out_domain : (grid && s->grid.has_border_corners ? 1 : 0);
+    for (int step = 0; step < p.max_extra_passes && n0 > 0; ++step) {
+      bool relaunch = false;
+      if (hist[kVertexOverflow]) { relaunch = true; V = int(V * 1.5); }
+      if (hist[kPlaneOverflow]) { relaunch = true; P = int(P * 1.5); }
+      if (hist[kSecurityRadiusNotReached]) { relaunch = true; K = int(K * 1.5); }
+      if (hist[kTriangleOverflow]) { relaunch = true; T = int(T * 1.5); }
+      if (!relaunch) break;
+      if (P > kMaxP || knn_slots(K) < 0) break;  // the reference stops at P >= 256 (voronoi.cpp:867)
+      V = std::min(V, kMaxV);
+      T = std::min(T, kMaxT);
+      if ((rc = run_pass(s, Cc, n1, K, P, V, T, eps, out_domain, counters, early)) != RPD_OK) return rc;
+      if ((rc = recompute_ids(s, A, n0, 1, B, Cc, n0, n1, hist)) != RPD_OK) return rc;
+      std::swap(A, B);
+    }
+  }
+  cudaEventRecord(t1, st);
+  int *h = s->hist.as<int>();
+  cudaMemsetAsync(h, 0, sizeof(int) * 16, st);
+  k_status_hist<<<s->ctx->sm_count, 256, 0, st>>>(s->status.as<int>(), n, h);
+  s->stats.kernel_launches += 1;
+  int hh[16];
+  cudaMemcpyAsync(hh, h, sizeof(hh), cudaMemcpyDeviceToHost, st);
+  unsigned long long c64[RPD_CTR_NUM + 1] = {};
+  if (counters) cudaMemcpyAsync(c64, s->counter64.ptr, sizeof(c64), cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "launch");
+  cudaEventElapsedTime(&s->stats.total_ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  for (int i = 0; i < kStatusNum; ++i) s->stats.status_hist[i] = hh[i];
+  for (int i = 0; i < RPD_CTR_NUM; ++i) s->stats.counters[i] = c64[i];
+  s->stats.knn_candidates = c64[RPD_CTR_NUM];
+  s->have_results = true;
+  return RPD_OK;
+}
+
+int rpd_solver_get_moments(rpd_solver *s, double *out4, rpd_mem where) {
+  if (!s || !out4 || !s->have_results) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  double4 *dst = reinterpret_cast<double4 *>(out4);
+  if (where != RPD_DEVICE) {
+    if ((e = s->gather.ensure(sizeof(double4) * s->n)) != cudaSuccess) return map_cuda(ctx, e, "alloc gather");
+    dst = s->gather.as<double4>();
+  }
+  k_gather_user<double4><<<(s->n + 255) / 256, 256, 0, st>>>(s->out.as<double4>(), s->user_to_stored.as<int>(), s->n, dst);
+  if (where != RPD_DEVICE)
+    cudaMemcpyAsync(out4, dst, sizeof(double4) * s->n, cudaMemcpyDeviceToHost, st);
+  e = cudaStreamSynchronize(st);
+  return map_cuda(ctx, e, "get moments");
+}
+
+int rpd_solver_get_status(rpd_solver *s, int *status, rpd_mem where) {
+  if (!s || !status || !s->have_results) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  int *dst = status;
+  if (where != RPD_DEVICE) {
+    if ((e = s->gather.ensure(sizeof(double4) * s->n)) != cudaSuccess) return map_cuda(ctx, e, "alloc gather");
+    dst = s->gather.as<int>();
+  }
+  k_gather_user<int><<<(s->n + 255) / 256, 256, 0, st>>>(s->status.as<int>(), s->user_to_stored.as<int>(), s->n, dst);
+  if (where != RPD_DEVICE) cudaMemcpyAsync(status, dst, sizeof(int) * s->n, cudaMemcpyDeviceToHost, st);
+  e = cudaStreamSynchronize(st);
+  return map_cuda(ctx, e, "get status");
+}
+
+int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *pp, double *records, int cap) {
+  if (!s || !records || cap <= 0 || user_id < 0 || user_id >= s->n) return RPD_ERR_INVALID;
+  rpd_params p;
+  if (pp) p = *pp;
+  else rpd_params_default(&p);
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const int n = s->n;
+  if ((e = s->out.ensure(sizeof(double4) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc out");
+  if ((e = s->status.ensure(sizeof(int) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc status");
+  if ((e = s->knn.ensure(sizeof(unsigned) * p.K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
+  DevBuf tr, id;
+  if ((e = tr.ensure(sizeof(double) * (1 + size_t(cap) * kTraceRecord))) != cudaSuccess)
+    return map_cuda(ctx, e, "alloc trace");
+  if ((e = id.ensure(sizeof(int))) != cudaSuccess) return map_cuda(ctx, e, "alloc id");
+  int sid = 0;
+  cudaMemcpyAsync(&sid, s->user_to_stored.as<int>() + user_id, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  cudaMemcpyAsync(id.ptr, &sid, sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(tr.ptr, 0, sizeof(double), st);
+  e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, id.as<int>(), 1, p.K,
+                 s->ring_bound.as<float>(), s->knn.as<unsigned>(), nullptr, st);
+  if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
+  CellLaunch a;
+  a.stored = s->stored.as<float4>();
+  a.n = n;
+  a.knn = s->knn.as<unsigned>();
+  a.K = p.K;
+  a.ids = id.as<int>();
+  a.num = 1;
+  a.P = p.P;
+  a.V = p.V;
+  a.T = p.T;
+  const bool grid = s->grid.size > 0;
+  a.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
+  a.out_domain = p.out_domain > 0 ? 1 : 0;
+  a.early_out = (p.flags & RPD_FLAG_NO_EARLY_OUT) ? 0 : 1;
+  a.grid = s->grid;
+  a.status = s->status.as<int>();
+  a.out = s->out.as<double4>();
+  a.trace_seed = sid;
+  a.trace = tr.as<double>();
+  a.trace_cap = cap;
+  if ((e = cell_launch(a, st)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+  double count = 0;
+  cudaMemcpyAsync(&count, tr.ptr, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "trace");
+  const int nrec = int(count);
+  cudaMemcpy(records, tr.as<double>() + 1, sizeof(double) * size_t(nrec) * kTraceRecord, cudaMemcpyDeviceToHost);
+  return nrec;
+}
+
+int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st) {
+  if (!s || !st) return RPD_ERR_INVALID;
+  *st = s->stats;
   return RPD_OK;
 }
 

@@ -5,6 +5,8 @@
 
 #include "../../include/rpd.h"
 #include "bins.cuh"
+#include "cell.cuh"
+#include "grid_host.h"
 #include "knn.cuh"
 
 namespace rpd {
@@ -37,6 +39,7 @@ struct DevBuf {
 
 void set_error(rpd_context *ctx, const std::string &msg);
 int map_cuda(rpd_context *ctx, cudaError_t e, const char *what);
+const HostGrid *host_grid(const rpd_grid *g);
 
 }  // namespace rpd
 
@@ -60,5 +63,17 @@ struct rpd_solver {
   rpd::DevBuf ring_bound;      // float[dim+2]
   rpd::DevBuf knn;             // unsigned[n*K]
   rpd::DevBuf knn_user;        // int[n*K]
-  rpd::DevBuf counter64;       // unsigned long long[4]
+  rpd::DevBuf counter64;       // unsigned long long[RPD_CTR_NUM + 1]
+  // domain on the device
+  rpd::DevBuf g_flags, g_points, g_tris, g_list, g_offsets, g_sat;
+  rpd::DevGrid grid;           // grid.size == 0: no domain
+  // results (stored order) and pass bookkeeping
+  rpd::DevBuf out;             // double4[n]
+  rpd::DevBuf status;          // int[n]
+  rpd::DevBuf ids_a, ids_b, ids_c;  // int[n] failing-id lists
+  rpd::DevBuf fail_ws;         // flags + scans
+  rpd::DevBuf hist;            // int[16]: status histogram + counts
+  rpd::DevBuf gather;          // user-order staging for outputs
+  bool have_results = false;
+  rpd_stats stats{};
 };

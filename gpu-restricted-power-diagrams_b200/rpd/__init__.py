@@ -63,12 +63,80 @@ def lib():
         L.rpd_solver_set_points.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.rpd_solver_get_permutation.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_knn.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_float)]
+        L.rpd_grid_create.restype = C.c_void_p
+        L.rpd_grid_create.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                      C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
+        L.rpd_grid_load.restype = C.c_void_p
+        L.rpd_grid_load.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
+        L.rpd_grid_save.argtypes = [C.c_void_p, C.c_char_p]
+        L.rpd_grid_valid.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+        L.rpd_grid_volume.restype = C.c_double
+        L.rpd_grid_volume.argtypes = [C.c_void_p]
+        L.rpd_grid_invariants.argtypes = [C.c_void_p, C.c_void_p]
+        L.rpd_grid_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 4
+        L.rpd_grid_export.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+        L.rpd_grid_destroy.argtypes = [C.c_void_p]
+        L.rpd_grid_make_blob.restype = C.c_void_p
+        L.rpd_grid_make_blob.argtypes = [C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_int)]
+        L.rpd_grid_make_cube.restype = C.c_void_p
+        L.rpd_grid_make_cube.argtypes = [C.c_int, C.POINTER(C.c_int)]
+        L.rpd_params_default.argtypes = [C.c_void_p]
+        L.rpd_solver_set_grid.argtypes = [C.c_void_p, C.c_void_p]
+        L.rpd_solver_launch.argtypes = [C.c_void_p, C.c_void_p]
+        L.rpd_solver_get_moments.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.rpd_solver_get_status.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.rpd_solver_get_stats.argtypes = [C.c_void_p, C.c_void_p]
+        L.rpd_solver_trace_cell.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         _lib = L
     return _lib
 
 
 def _ptr(a):
     return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+FLAG_FIRST_PASS_ONLY = 1
+FLAG_COUNTERS = 2
+FLAG_NO_EARLY_OUT = 4
+COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
+                 "exports", "export_vertices", "outside_early"]
+
+
+class Params(C.Structure):
+    """rpd_params: the VoroAlgo knobs (voronoi.h:199-246)."""
+
+    _fields_ = [("K", C.c_int), ("P", C.c_int), ("V", C.c_int), ("T", C.c_int), ("max_extra_passes", C.c_int),
+                ("cube_eps", C.c_float), ("out_domain", C.c_int), ("flags", C.c_uint)]
+
+    @classmethod
+    def default(cls, **kw):
+        p = cls()
+        lib().rpd_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+
+class Stats(C.Structure):
+    _fields_ = [("npasses", C.c_int), ("pass_cells", C.c_int * 8), ("pass_K", C.c_int * 8),
+                ("pass_P", C.c_int * 8), ("pass_V", C.c_int * 8), ("pass_T", C.c_int * 8),
+                ("pass_knn_ms", C.c_float * 8), ("pass_cell_ms", C.c_float * 8), ("status_hist", C.c_int * 11),
+                ("counters", C.c_ulonglong * 9), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
+                ("kernel_launches", C.c_int)]
+
+    def as_dict(self):
+        n = self.npasses
+        return {
+            "npasses": n,
+            "passes": [{"cells": self.pass_cells[i], "K": self.pass_K[i], "P": self.pass_P[i], "V": self.pass_V[i],
+                        "T": self.pass_T[i], "knn_ms": self.pass_knn_ms[i], "cell_ms": self.pass_cell_ms[i]}
+                       for i in range(min(n, 8))],
+            "status": {STATUS_NAMES[i]: v for i, v in enumerate(self.status_hist) if v},
+            "counters": {COUNTER_NAMES[i]: int(v) for i, v in enumerate(self.counters)},
+            "knn_candidates": int(self.knn_candidates),
+            "total_ms": self.total_ms,
+            "kernel_launches": self.kernel_launches,
+        }
 
 
 class Context:
@@ -147,6 +215,42 @@ class Solver:
         self.ctx.check(lib().rpd_solver_get_permutation(self.h, _ptr(out), RPD_HOST))
         return out
 
+    def set_grid(self, grid):
+        self.ctx.check(lib().rpd_solver_set_grid(self.h, grid.h if grid is not None else None))
+        self._grid = grid
+        return self
+
+    def launch(self, params=None, **kw):
+        p = params if params is not None else Params.default(**kw)
+        self.ctx.check(lib().rpd_solver_launch(self.h, C.byref(p)))
+        return self
+
+    def moments(self) -> np.ndarray:
+        out = np.zeros((self.n, 4), np.float64)
+        self.ctx.check(lib().rpd_solver_get_moments(self.h, _ptr(out), RPD_HOST))
+        return out
+
+    def status(self) -> np.ndarray:
+        out = np.zeros(self.n, np.int32)
+        self.ctx.check(lib().rpd_solver_get_status(self.h, _ptr(out), RPD_HOST))
+        return out
+
+    def stats(self) -> dict:
+        st = Stats()
+        self.ctx.check(lib().rpd_solver_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
+
+    TRACE_KINDS = {0: "seed", 1: "plane", 2: "cavity", 3: "vertex", 4: "integrate", 5: "start", 6: "triangle"}
+
+    def trace_cell(self, user_id: int, params=None, cap: int = 20000, **kw):
+        """Debugging: the clip/integration records of one seed's cell."""
+        p = params if params is not None else Params.default(**kw)
+        rec = np.zeros((cap, 12), np.float64)
+        n = lib().rpd_solver_trace_cell(self.h, int(user_id), C.byref(p), _ptr(rec), cap)
+        if n < 0:
+            raise RpdError(n, self.ctx.error())
+        return rec[:n]
+
     def knn(self, K: int, return_ms: bool = False):
         out = np.zeros((self.n, K), np.int32)
         ms = C.c_float(0)
@@ -186,3 +290,164 @@ class KNearests:
     def getNearests(self) -> np.ndarray:
         """K nearest other seeds of every seed, in user ids (user order)."""
         return self._nearest
+
+
+class Grid:
+    """Mirror of the reference Grid (Grid.h:14-70): a volume domain in the
+    --grid layout, held by librpd (host memory)."""
+
+    def __init__(self, handle=None):
+        self.h = handle
+
+    @classmethod
+    def from_arrays(cls, size, in_domain, points, triangles, tri_list, offsets):
+        d = np.ascontiguousarray(in_domain, dtype=np.int8)
+        p = np.ascontiguousarray(np.asarray(points, np.float32)[:, :3])
+        t = np.ascontiguousarray(triangles, dtype=np.int32).reshape(-1)
+        tl = np.ascontiguousarray(tri_list, dtype=np.int32)
+        o = np.ascontiguousarray(offsets, dtype=np.int32)
+        err = C.c_int(0)
+        h = lib().rpd_grid_create(int(size), _ptr(d), _ptr(p), len(p), _ptr(t), len(t) // 3, _ptr(tl), len(tl),
+                                  _ptr(o), C.byref(err))
+        if not h:
+            raise RpdError(err.value, "bad grid arrays")
+        return cls(h)
+
+    @classmethod
+    def blob(cls, size, nellipsoids=5, seed=2):
+        err = C.c_int(0)
+        h = lib().rpd_grid_make_blob(size, nellipsoids, seed, C.byref(err))
+        if not h:
+            raise RpdError(err.value, "blob")
+        return cls(h)
+
+    @classmethod
+    def cube(cls, size):
+        err = C.c_int(0)
+        h = lib().rpd_grid_make_cube(size, C.byref(err))
+        if not h:
+            raise RpdError(err.value, "cube")
+        return cls(h)
+
+    def load(self, path) -> bool:
+        """Grid::load (Grid.cpp:186-278); False when the file is unreadable."""
+        err = C.c_int(0)
+        h = lib().rpd_grid_load(str(path).encode(), C.byref(err))
+        if not h:
+            return False
+        self.close()
+        self.h = h
+        return True
+
+    def save(self, path) -> bool:
+        return lib().rpd_grid_save(self.h, str(path).encode()) == RPD_OK
+
+    def valid(self, return_reason=False):
+        buf = C.create_string_buffer(256)
+        ok = lib().rpd_grid_valid(self.h, buf, 256) == 1
+        return (ok, buf.value.decode()) if return_reason else ok
+
+    def getVolume(self) -> float:
+        return lib().rpd_grid_volume(self.h)
+
+    def invariants(self) -> np.ndarray:
+        out = np.zeros(4, np.float64)
+        lib().rpd_grid_invariants(self.h, _ptr(out))
+        return out
+
+    def info(self):
+        v = [C.c_int(0) for _ in range(4)]
+        lib().rpd_grid_info(self.h, *[C.byref(x) for x in v])
+        return tuple(x.value for x in v)
+
+    def arrays(self):
+        size, npts, ntri, nlist = self.info()
+        d = np.zeros(size ** 3, np.int8)
+        p = np.zeros((npts, 3), np.float32)
+        t = np.zeros((ntri, 3), np.int32)
+        tl = np.zeros(nlist, np.int32)
+        o = np.zeros(size ** 3 + 1, np.int32)
+        lib().rpd_grid_export(self.h, _ptr(d), _ptr(p), _ptr(t), _ptr(tl), _ptr(o))
+        return {"size": size, "in_domain": d, "points": p, "triangles": t, "tri_list": tl, "offsets": o}
+
+    def close(self):
+        if self.h:
+            lib().rpd_grid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class VoroAlgoStat(dict):
+    """One pass record (VoroAlgoStat, voronoi.h:60-103)."""
+
+
+class VoroAlgo:
+    """Mirror of the reference VoroAlgo (voronoi.h:105-256).
+
+    Set the public knobs, call setInputPoints (and setGrid), then
+    launch(saveData, stats): saveData(algo) reads the getters and returns a
+    bool, as in the reference; results stay available afterwards too.
+    """
+
+    def __init__(self, ctx: Context | None = None, debug: bool = False):
+        self.m_K, self.m_P, self.m_T, self.m_V = 25, 35, 100, 40  # voronoi.cpp:1042-1045
+        self.m_maxKComputed = 100000
+        self.m_vhsAlgo = [1, 2]
+        self.m_keepDistance = 1
+        self.m_keepVolume = 1.0
+        self.m_PGlobalPercent = 0.0
+        self.m_H, self.m_HC = 0, 1
+        self.max_extra_passes = 5
+        self.debug = debug
+        self._s = Solver(ctx)
+        self._grid = None
+        self._n = 0
+
+    def setInputPoints(self, seeds):
+        self._s.set_points(seeds)
+        self._n = self._s.n
+
+    def setGrid(self, grid: Grid):
+        self._grid = grid
+        self._s.set_grid(grid)
+
+    def getNumInputPoints(self) -> int:
+        return self._n
+
+    def launch(self, saveData=None, stats=None) -> bool:
+        try:
+            self._s.launch(Params.default(K=self.m_K, P=self.m_P, V=self.m_V, T=self.m_T,
+                                          max_extra_passes=self.max_extra_passes))
+        except RpdError:
+            return False
+        if stats is not None:
+            d = self._s.stats()
+            names = ["first"] + ["extra"] * (d["npasses"] - 1)
+            for name, ps in zip(names, d["passes"]):
+                stats.append(VoroAlgoStat(name=name, knn=ps["knn_ms"] / 1e3, CC=ps["cell_ms"] / 1e3,
+                                          time=(ps["knn_ms"] + ps["cell_ms"]) / 1e3, nbcells=ps["cells"]))
+        if saveData is not None:
+            return bool(saveData(self))
+        return True
+
+    def getNumOutputPoints(self) -> int:
+        return self._n
+
+    def getBarycenters(self) -> np.ndarray:
+        """(n,4) float64 (m*x, m*y, m*z, m), in user order (so
+        getPermutationToUser is the identity)."""
+        return self._s.moments()
+
+    def getPermutationToUser(self) -> np.ndarray:
+        return np.arange(self._n, dtype=np.int32)
+
+    def getStatus(self) -> np.ndarray:
+        return self._s.status()
+
+    def getStats(self) -> dict:
+        return self._s.stats()

@@ -92,6 +92,120 @@ int rpd_solver_get_permutation(rpd_solver *s, int *perm, rpd_mem where);
  * USER indices (-1 where fewer than K exist), n*K ints in user order. */
 int rpd_solver_knn(rpd_solver *s, int K, int *knn_user, rpd_mem where, float *device_ms);
 
+/* ------------------------------------------------------------------ domain */
+
+/* A volume domain in the reference --grid layout (Grid.h:14-70): size^3
+ * voxel-corner flags (0 outside, 1 on the border, 2 inside), a closed
+ * triangle surface, and per voxel the sorted ids of its triangles.  Host
+ * container; solvers copy it to the device in rpd_solver_set_grid. */
+typedef struct rpd_grid rpd_grid;
+
+/* From arrays (copied).  points: 3 floats per vertex; offsets: size^3+1.
+ * The orientation is flipped when the volume is negative, as Grid::load
+ * does (Grid.cpp:270-275). */
+rpd_grid *rpd_grid_create(int size, const char *in_domain, const float *points_xyz, int npoints,
+                          const int *triangles, int ntriangles, const int *tri_list, int nlist,
+                          const int *offsets, int *err);
+/* Grid::load / Grid::save: the reference text format (Grid.cpp:186-344). */
+rpd_grid *rpd_grid_load(const char *path, int *err);
+int rpd_grid_save(const rpd_grid *g, const char *path);
+/* Grid::valid (Grid.cpp:60-184): 1 valid, 0 invalid (reason copied to why). */
+int rpd_grid_valid(const rpd_grid *g, char *why, int why_len);
+/* Grid::getVolume (Grid.cpp:30-35). */
+double rpd_grid_volume(const rpd_grid *g);
+/* Volume and first moments of the domain (Grid::printInvariants,
+ * Grid.cpp:281-288): out = (m*x, m*y, m*z, m). */
+int rpd_grid_invariants(const rpd_grid *g, double *out4);
+int rpd_grid_info(const rpd_grid *g, int *size, int *npoints, int *ntriangles, int *nlist);
+/* Copies the arrays out (sizes from rpd_grid_info; points 3 floats each). */
+int rpd_grid_export(const rpd_grid *g, char *in_domain, float *points_xyz, int *triangles, int *tri_list,
+                    int *offsets);
+void rpd_grid_destroy(rpd_grid *g);
+/* Synthetic domains.  Blob: union of `nellipsoids` seeded random ellipsoids
+ * (centres U[0.35,0.65]^3, semi-axes U[0.15,0.35] of the unit cube, random
+ * rotations) voxelized on size^3, each voxel split into the 6 Kuhn tetrahedra
+ * of its main diagonal, surface by marching tetrahedra.  Cube: the box
+ * [d, 1000-d]^3 with d half a voxel (no voxel corner on its surface), faces
+ * triangulated along the voxel columns. */
+rpd_grid *rpd_grid_make_blob(int size, int nellipsoids, uint64_t seed, int *err);
+rpd_grid *rpd_grid_make_cube(int size, int *err);
+
+/* --------------------------------------------------------------- solve */
+
+/* Launch flags. */
+#define RPD_FLAG_FIRST_PASS_ONLY 1u /* no retry passes */
+#define RPD_FLAG_COUNTERS 2u        /* collect work counters (rpd_stats.counters) */
+#define RPD_FLAG_NO_EARLY_OUT 4u    /* clip every cell to the end even when it is
+                                       provably outside the domain (same results) */
+
+/* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
+typedef struct rpd_params {
+  int K;                /* neighbours of the first pass (--K, 20) */
+  int P;                /* planes per cell (--P, 25; < 256) */
+  int V;                /* vertices per cell (--V, 30; <= 256) */
+  int T;                /* boundary triangles per cell (--T, 100) */
+  int max_extra_passes; /* retry passes with caps x1.5 (voronoi.cpp:1321: 5) */
+  float cube_eps;       /* box [-eps, 1000+eps]^3; < 0: 0.1 with a domain, else 0 */
+  int out_domain;       /* start-corner fallback one voxel layer out in the
+                           retry passes: -1 auto (when the grid has border
+                           corners, voronoi.cpp:1320), 0 never, 1 always */
+  unsigned flags;       /* RPD_FLAG_* */
+} rpd_params;
+
+void rpd_params_default(rpd_params *p);
+
+/* Work counters (RPD_FLAG_COUNTERS), summed over passes. */
+enum {
+  RPD_CTR_PLANES_TESTED = 0,
+  RPD_CTR_CLIPS,
+  RPD_CTR_VERTEX_TESTS,
+  RPD_CTR_VERTICES_MADE,
+  RPD_CTR_BOUNDARY_CELLS,
+  RPD_CTR_TRIANGLES,
+  RPD_CTR_EXPORTS,
+  RPD_CTR_EXPORT_VERTICES,
+  RPD_CTR_OUTSIDE, /* cells proven outside the domain before the end of clipping */
+  RPD_CTR_NUM
+};
+
+typedef struct rpd_stats {
+  int npasses;
+  int pass_cells[8];
+  int pass_K[8], pass_P[8], pass_V[8], pass_T[8];
+  float pass_knn_ms[8];
+  float pass_cell_ms[8];
+  int status_hist[RPD_STATUS_NUM]; /* final status of every seed */
+  unsigned long long counters[RPD_CTR_NUM];
+  unsigned long long knn_candidates;
+  float total_ms;                  /* device time of the whole launch */
+  int kernel_launches;             /* device kernels this launch ran */
+} rpd_stats;
+
+/* VoroAlgo::setGrid (voronoi.cpp:1079-1082): uploads the domain; null
+ * removes it (the cell is then restricted to the box only). */
+int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *g);
+
+/* VoroAlgo::launch (voronoi.cpp:1244-1403): every seed's power cell clipped
+ * to the box and the domain, integrated; failing cells are retried with
+ * caps x1.5 as the reference does.  Results stay on the device until the
+ * next launch or set_points. */
+int rpd_solver_launch(rpd_solver *s, const rpd_params *p);
+
+/* Per seed in USER order: (m*x, m*y, m*z, m) in the reference frame, as
+ * getBarycenters + getPermutationToUser give them (voronoi.cpp:1165-1209);
+ * zeros for failed cells; the seed itself for w <= RPD_NO_CELL_LIMITS. */
+int rpd_solver_get_moments(rpd_solver *s, double *out4, rpd_mem where);
+/* Per seed in user order: rpd_cell_status. */
+int rpd_solver_get_status(rpd_solver *s, int *status, rpd_mem where);
+int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st);
+
+/* Debugging: re-runs one seed's cell (user id) with the caps of `p` and
+ * records every clip and integration into `records` (cap records of 12
+ * doubles: kind 0 seed, 1 plane test, 2 cavity, 3 vertex, 4 integration,
+ * 5 start corner, 6 boundary triangle).  Returns the record count (>= 0) or
+ * an rpd_error. */
+int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *p, double *records, int cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,7 +40,7 @@ class OracleParams(C.Structure):
         ("K", C.c_int), ("P", C.c_int), ("V", C.c_int), ("T", C.c_int),
         ("vhs0", C.c_int), ("vhs1", C.c_int), ("use_double", C.c_int), ("kernels", C.c_int),
         ("knn_mode", C.c_int), ("max_extra_passes", C.c_int), ("first_pass_only", C.c_int),
-        ("cube_eps", C.c_double), ("nthreads", C.c_int),
+        ("cube_eps", C.c_double), ("nthreads", C.c_int), ("sample_stride", C.c_int),
     ]
 
 
@@ -113,7 +113,7 @@ class GridArrays:
 
 def solve(xyzw, grid=None, K=20, P=25, V=30, T=100, vhs0=2, vhs1=2, use_double=False, kernels=0,
           knn_mode=0, max_extra_passes=5, first_pass_only=False, cube_eps=None, nthreads=0,
-          return_stats=False):
+          return_stats=False, sample_stride=1):
     """Runs the reference host flow (VoroAlgo::launch) on the CPU.
 
     xyzw: (n,4) seeds in the reference [0,1000]^3 frame.  Returns (bary (n,4)
@@ -126,7 +126,7 @@ def solve(xyzw, grid=None, K=20, P=25, V=30, T=100, vhs0=2, vhs1=2, use_double=F
     if cube_eps is None:
         cube_eps = 0.1 if grid is not None else 0.0
     prm = OracleParams(K, P, V, T, vhs0, vhs1, int(use_double), kernels, knn_mode, max_extra_passes,
-                       int(first_pass_only), cube_eps, nthreads)
+                       int(first_pass_only), cube_eps, nthreads, sample_stride)
     st = OracleStats()
     gv = grid.view() if grid is not None else None
     rc = lib().oracle_solve(_ptr(x), n, C.byref(gv) if gv is not None else None, C.byref(prm), _ptr(bary),

@@ -1029,8 +1029,9 @@ struct Solver {
     status.assign(n, success);
     out.assign(n, Vec4<R>{0, 0, 0, 0});
     const bool dbl = std::is_same<R, double>::value;
-    std::vector<int> ids0(n), ids1;
-    for (int i = 0; i < n; ++i) ids0[i] = i;
+    std::vector<int> ids0, ids1;
+    const int stride = prm.sample_stride > 1 ? prm.sample_stride : 1;
+    for (int i = 0; i < n; i += stride) ids0.push_back(i);
     std::array<int, kStatusNum> hist{};
     // pass "first": T=0 defers every boundary cell (voronoi.cpp:1275-1297)
     const int T_first = prm.first_pass_only ? prm.T : 0;

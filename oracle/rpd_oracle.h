@@ -42,6 +42,7 @@ typedef struct OracleParams {
   int first_pass_only;      // 1: only pass "first" with T=caps.T (no retries)
   double cube_eps;          // CUBE_EPSILON: 0.1 with a grid, 0 without
   int nthreads;             // 0: all host threads
+  int sample_stride;        // >1: only every stride-th stored seed is solved (timing samples)
 } OracleParams;
 
 typedef struct OracleStats {
