@@ -244,6 +244,9 @@ def run_ours(args, cfg, rank, world, local):
     barrier()
     clk = clocks.stop()
     last_stats = solver.stats()
+    # one untimed launch with the work counters on
+    solver.launch(rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_COUNTERS))
+    work = solver.stats()["counters"]
     ms = sum(step_ms) / len(step_ms)
     if world > 1:
         import torch.distributed as dist
@@ -313,7 +316,7 @@ def run_ours(args, cfg, rank, world, local):
         "clocks": clk,
         "detail": {"knn_ms": sum(knn_ms) / len(knn_ms), "cell_ms_first_pass": cell_avg_ms,
                    "passes": last_stats["passes"], "status": last_stats["status"],
-                   "npasses": npasses[-1], "step_ms": step_ms},
+                   "npasses": npasses[-1], "step_ms": step_ms, "work_counters": work},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x, grid, cfg, target_s=args.cpu_seconds)

@@ -1,27 +1,35 @@
 // Restricted power cell of every seed, one warp per cell.  Replaces the
 // reference's one-work-item compute_voro_cell (ConvexCell.cl:812-1116).
 //
-// Geometry is in the seed's local frame (seed at the origin): planes are
-// (n, d) in double with the kept side n.x + d >= 0, built from the exact
-// seed-relative neighbour vector (float inputs, differences exact in
-// double).  A vertex is the triple of its planes (a, b, c) plus the cofactor
-// vector c of det(pi_a, pi_b, pi_c, e), so that the reference's FP64
-// half-space predicate det(...) > 0 (ConvexCell.cl:402-414, VHSAlgo 2) is
-// e . c > 0: four DFMA per test.  The vertex position is c.xyz / c.w.  In
-// the seed's frame every coordinate is of the cell's size, so thin boundary
-// slivers keep their relative accuracy.
+// Geometry is in the seed's local frame (seed at the origin), in double:
+// planes (n, d) have unit normals and keep the side n.x + d >= 0.  Bisectors
+// come from the exact double difference of the float seed coordinates, so
+// thin boundary slivers keep their relative accuracy.  A vertex is the
+// triple of its planes (a, b, c) plus the cofactor vector c of
+// det(pi_a, pi_b, pi_c, e): the reference's FP64 half-space predicate
+// det(...) > 0 (ConvexCell.cl:402-414, VHSAlgo 2) is e . c > 0, four DFMA
+// per test.  The vertex position is p = c.xyz / c.w (c.w < 0 for the
+// orientation of the reference's initial box, ConvexCell.cl:299-306).
+//
+// Ties: a vertex is cut only when it lies beyond the plane by more than
+// kTieEps (e . c > kTieEps |c.w|).  That is a cut by a slightly shifted
+// plane, consistent for coincident vertices, so the cavity in the dual is
+// always a disk even where the domain's planes pass exactly through cell
+// vertices (lattice-aligned surfaces).
 //
 // Per warp, shared memory holds the planes, the vertices (SoA), the cavity
 // scratch and, with a domain, a backup of the Voronoi cell.  One clip:
 //   1. every lane tests its vertices (v = lane + 32 s) -> ballot masks;
-//   2. boundary edges of the removed dual triangles = directed edges (u, v)
-//      whose twin (v, u) is not removed; they must form one cycle over the
-//      planes (else inconsistent_boundary, ConvexCell.cl:463-515);
-//   3. survivors are compacted by moving the ones past the new count into
-//      holes; new vertices (new plane, u, v) fill the remaining holes.
-// The cell's security radius (ConvexCell.cl:364-382) uses the cached |p|^2
-// of every vertex.  Integration (ConvexCell.cl:577-619) runs per vertex in
-// double and is reduced across the warp.
+//   2. the directed edges of the removed dual triangles are marked in a
+//      per-plane bit mask; boundary edges (u, v) are those whose twin (v, u)
+//      is unmarked; they must form one cycle over the planes (else
+//      inconsistent_boundary, ConvexCell.cl:463-515);
+//   3. survivors past the new count move into holes; new vertices
+//      (new plane, u, v) fill the remaining holes (the reference's triangle
+//      orientation (vid, cir, next[cir]), ConvexCell.cl:556-562).
+// The security radius (ConvexCell.cl:364-382) uses the cached |p|^2 of every
+// vertex.  Integration (ConvexCell.cl:577-619) runs per vertex in double and
+// is reduced across the warp.
 #include <algorithm>
 
 #include "cell.cuh"
@@ -32,11 +40,12 @@ namespace {
 
 constexpr unsigned kNone = 0xffffffffu;
 constexpr double kVolEps2 = 1e-12;  // VOLUME_EPSILON2 of the FP64 build (voronoi.cpp:922)
+constexpr double kTieEps = 1e-10;   // cut tolerance, reference-frame units
 
 struct Layout {
-  int Pc, Vc, G;
-  unsigned o_plane, o_cx, o_cy, o_cz, o_cw, o_d2, o_tri, o_next, o_rem, o_hole, o_edge;
-  unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist;
+  int Pc, Vc, G, Mw;  // Mw: 32-bit words of one plane's edge mask
+  unsigned o_plane, o_cx, o_cy, o_cz, o_cw, o_d2, o_tri, o_next, o_emask, o_rem, o_hole, o_edge;
+  unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist, o_pts;
   unsigned total;
 };
 
@@ -53,6 +62,7 @@ __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
   L.Pc = (P + 3) & ~3;
   L.Vc = (V + 31) & ~31;
   L.G = grid ? pow2_at_least(2 * T) : 0;
+  L.Mw = (L.Pc + 31) / 32;
   unsigned o = 0;
   L.o_plane = o; o = align16(o + 32u * L.Pc);
   L.o_cx = o; o = align16(o + 8u * L.Vc);
@@ -62,6 +72,7 @@ __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
   L.o_d2 = o; o = align16(o + 8u * L.Vc);
   L.o_tri = o; o = align16(o + 4u * L.Vc);
   L.o_next = o; o = align16(o + 4u * L.Pc);
+  L.o_emask = o; o = align16(o + 4u * L.Pc * L.Mw);
   L.o_rem = o; o = align16(o + 4u * L.Vc);
   L.o_hole = o; o = align16(o + 4u * L.Vc);
   L.o_edge = o; o = align16(o + 4u * L.Vc);
@@ -73,8 +84,9 @@ __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
     L.o_bd2 = o; o = align16(o + 8u * L.Vc);
     L.o_btri = o; o = align16(o + 4u * L.Vc);
     L.o_tlist = o; o = align16(o + 4u * L.G);
+    L.o_pts = o; o = align16(o + 8u * 12);
   } else {
-    L.o_bcx = L.o_bcy = L.o_bcz = L.o_bcw = L.o_bd2 = L.o_btri = L.o_tlist = 0;
+    L.o_bcx = L.o_bcy = L.o_bcz = L.o_bcw = L.o_bd2 = L.o_btri = L.o_tlist = L.o_pts = 0;
   }
   L.total = o;
   return L;
@@ -88,11 +100,13 @@ struct Plane {
 struct WarpCell {
   Plane *plane;
   double *cx, *cy, *cz, *cw, *d2;
-  unsigned *tri, *next, *rem, *hole, *edge;
+  unsigned *tri, *next, *emask, *rem, *hole, *edge;
   double *bcx, *bcy, *bcz, *bcw, *bd2;
   unsigned *btri;
   int *tlist;
+  double *pts;  // start corner and the current boundary triangle, local frame
   int nv, np;  // vertex and plane counts (warp-uniform)
+  int vc, mw;  // capacity of the vertex arrays, words per edge mask
 };
 
 __device__ __forceinline__ WarpCell bind(unsigned char *base, const Layout &L) {
@@ -105,6 +119,7 @@ __device__ __forceinline__ WarpCell bind(unsigned char *base, const Layout &L) {
   w.d2 = reinterpret_cast<double *>(base + L.o_d2);
   w.tri = reinterpret_cast<unsigned *>(base + L.o_tri);
   w.next = reinterpret_cast<unsigned *>(base + L.o_next);
+  w.emask = reinterpret_cast<unsigned *>(base + L.o_emask);
   w.rem = reinterpret_cast<unsigned *>(base + L.o_rem);
   w.hole = reinterpret_cast<unsigned *>(base + L.o_hole);
   w.edge = reinterpret_cast<unsigned *>(base + L.o_edge);
@@ -115,11 +130,39 @@ __device__ __forceinline__ WarpCell bind(unsigned char *base, const Layout &L) {
   w.bd2 = reinterpret_cast<double *>(base + L.o_bd2);
   w.btri = reinterpret_cast<unsigned *>(base + L.o_btri);
   w.tlist = reinterpret_cast<int *>(base + L.o_tlist);
+  w.pts = reinterpret_cast<double *>(base + L.o_pts);
   w.nv = w.np = 0;
+  w.vc = L.Vc;
+  w.mw = L.Mw;
   return w;
 }
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+__device__ __forceinline__ Plane shfl_plane(Plane v, int src) {
+  v.x = __shfl_sync(kFull, v.x, src);
+  v.y = __shfl_sync(kFull, v.y, src);
+  v.z = __shfl_sync(kFull, v.z, src);
+  v.w = __shfl_sync(kFull, v.w, src);
+  return v;
+}
+
+__device__ __forceinline__ void count(unsigned long long *ctr, int k, unsigned long long v, int lane) {
+  if (ctr && lane == 0) atomicAdd(&ctr[k], v);
+}
 
 // One trace record (lane 0 only): kind, 4 plane or point values, 7 extras.
 __device__ __forceinline__ void trace_rec(double *tr, int cap, int lane, double kind, double a, double b, double c,
@@ -132,29 +175,6 @@ __device__ __forceinline__ void trace_rec(double *tr, int cap, int lane, double 
   r[0] = kind; r[1] = a; r[2] = b; r[3] = c; r[4] = d;
   r[5] = e0; r[6] = e1; r[7] = e2; r[8] = e3; r[9] = e4; r[10] = e5; r[11] = e6;
   tr[0] = i + 1;
-}
-
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
-  return v;
-}
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-__device__ __forceinline__ int warp_sumi(int v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-__device__ __forceinline__ Plane shfl_plane(Plane v, int src) {
-  v.x = __shfl_sync(kFull, v.x, src);
-  v.y = __shfl_sync(kFull, v.y, src);
-  v.z = __shfl_sync(kFull, v.z, src);
-  v.w = __shfl_sync(kFull, v.w, src);
-  return v;
 }
 
 // Cofactor vector c of det(p1, p2, p3, e) = e . c, with the 2x2-minor
@@ -170,17 +190,14 @@ __device__ __forceinline__ void cofactor(const Plane &p1, const Plane &p2, const
   const double m23 = a31 * a22 - a21 * a32;
   const double m24 = a41 * a22 - a21 * a42;
   const double m34 = a41 * a32 - a31 * a42;
-  const double m123 = m23 * a13 - m13 * a23 + m12 * a33;
-  const double m124 = m24 * a13 - m14 * a23 + m12 * a43;
-  const double m134 = m34 * a13 - m14 * a33 + m13 * a43;
-  const double m234 = m34 * a23 - m24 * a33 + m23 * a43;
-  cx = m234;
-  cy = -m134;
-  cz = m124;
-  cw = -m123;
+  cx = m34 * a23 - m24 * a33 + m23 * a43;
+  cy = -(m34 * a13 - m14 * a33 + m13 * a43);
+  cz = m24 * a13 - m14 * a23 + m12 * a43;
+  cw = -(m23 * a13 - m13 * a23 + m12 * a33);
 }
 
-__device__ __forceinline__ void make_vertex(WarpCell &w, int slot, unsigned a, unsigned b, unsigned c) {
+// Makes vertex `slot` from planes (a, b, c); false when it is degenerate.
+__device__ __forceinline__ bool make_vertex(WarpCell &w, int slot, unsigned a, unsigned b, unsigned c) {
   double cx, cy, cz, cw;
   cofactor(w.plane[a], w.plane[b], w.plane[c], cx, cy, cz, cw);
   w.cx[slot] = cx;
@@ -189,8 +206,10 @@ __device__ __forceinline__ void make_vertex(WarpCell &w, int slot, unsigned a, u
   w.cw[slot] = cw;
   const double inv = 1.0 / cw;
   const double px = cx * inv, py = cy * inv, pz = cz * inv;
-  w.d2[slot] = px * px + py * py + pz * pz;
+  const double d2 = px * px + py * py + pz * pz;
+  w.d2[slot] = d2;
   w.tri[slot] = a | (b << 8) | (c << 16);
+  return d2 < 1e300;  // false for inf / NaN
 }
 
 __device__ __forceinline__ void copy_vertex(WarpCell &w, int dst, int src) {
@@ -209,7 +228,7 @@ __device__ void init_box(WarpCell &w, float4 s, float eps, int lane) {
     const double vmin = -double(eps), vmax = 1000.0 + double(eps);
     const double sc = lane < 2 ? s.x : (lane < 4 ? s.y : s.z);
     const double sign = (lane & 1) ? -1.0 : 1.0;
-    // global plane: sign * x + off, off = -vmin (sign +) or vmax (sign -)
+    // global plane sign * x + off, off = -vmin (sign +) or vmax (sign -)
     const double off = (lane & 1) ? vmax - sc : sc - vmin;
     Plane p{0.0, 0.0, 0.0, off};
     if (lane < 2) p.x = sign;
@@ -235,93 +254,123 @@ __device__ __forceinline__ double cell_radius2(const WarpCell &w, int lane) {
   double r = 0.0;
 #pragma unroll
   for (int s = 0; s < VS; ++s) {
+    if (s * 32 >= w.nv) break;
     const int v = s * 32 + lane;
     if (v < w.nv) r = fmax(r, w.d2[v]);
   }
   return warp_max(r);
 }
 
-__device__ __forceinline__ bool has_twin(const unsigned *rem, int nrem, unsigned u, unsigned v) {
-  for (int q = 0; q < nrem; ++q) {
-    const unsigned t = rem[q];
-    const unsigned x = t & 0xff, y = (t >> 8) & 0xff, z = (t >> 16) & 0xff;
-    if ((x == v && y == u) || (y == v && z == u) || (z == v && x == u)) return true;
-  }
-  return false;
-}
-
-// Clips the cell by plane e (kept side e(x) >= 0).  Returns 0 when nothing
-// is cut (the plane is not kept), 1 when the cell changed, -1 on failure
-// with `status` set.  The caller has checked np < P.
+// Vertices cut by plane e, as ballot masks per slot; returns their count.
 template <int VS>
-__device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, unsigned long long *ctr,
-                    double *tr = nullptr, int trcap = 0) {
-  const double ex = e.x, ey = e.y, ez = e.z, ew = e.w;
-  unsigned rm[VS];
+__device__ __forceinline__ int cut_masks(const WarpCell &w, const Plane &e, unsigned (&rm)[VS], int lane) {
   int nrem = 0;
 #pragma unroll
   for (int s = 0; s < VS; ++s) {
+    rm[s] = 0u;
+    if (s * 32 >= w.nv) continue;
     const int v = s * 32 + lane;
     bool r = false;
-    if (v < w.nv) r = w.cx[v] * ex + w.cy[v] * ey + w.cz[v] * ez + w.cw[v] * ew > 0.0;
+    if (v < w.nv) {
+      const double cw = w.cw[v];
+      const double d = w.cx[v] * e.x + w.cy[v] * e.y + w.cz[v] * e.z + cw * e.w;
+      r = d > kTieEps * fabs(cw);
+    }
     rm[s] = __ballot_sync(kFull, r);
     nrem += __popc(rm[s]);
   }
-  if (ctr && lane == 0) ctr[kCtrVertexTests] += w.nv;
-  trace_rec(tr, trcap, lane, 1, ex, ey, ez, ew, w.nv, nrem, w.np);
+  return nrem;
+}
+
+// Clips the cell by plane e.  Returns 0 when nothing is cut (the plane is
+// not kept), 1 when the cell changed, -1 on failure with `status` set.  The
+// caller has checked np < P.
+template <int VS>
+__device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, unsigned long long *ctr,
+                    double *tr, int trcap) {
+  unsigned rm[VS];
+  const int nrem = cut_masks<VS>(w, e, rm, lane);
+  count(ctr, kCtrVertexTests, w.nv, lane);
+  trace_rec(tr, trcap, lane, 1, e.x, e.y, e.z, e.w, w.nv, nrem, w.np);
   if (nrem == 0) return 0;
   if (nrem == w.nv) {
     status = kEmptyCell;
     return -1;
   }
   const int pid = w.np;
+  const int mw = w.mw;
   if (lane == 0) w.plane[pid] = e;
   // removed triples, in position order
   {
     int base = 0;
 #pragma unroll
     for (int s = 0; s < VS; ++s) {
-      const int v = s * 32 + lane;
-      if ((rm[s] >> lane) & 1u) w.rem[base + __popc(rm[s] & lanemask_lt(lane))] = w.tri[v];
+      if ((rm[s] >> lane) & 1u) w.rem[base + __popc(rm[s] & lanemask_lt(lane))] = w.tri[s * 32 + lane];
       base += __popc(rm[s]);
     }
   }
   __syncwarp();
+  // clear the links and edge masks of the planes of the removed triangles
   for (int r = lane; r < nrem; r += 32) {
     const unsigned t = w.rem[r];
-    w.next[t & 0xff] = kNone;
-    w.next[(t >> 8) & 0xff] = kNone;
-    w.next[(t >> 16) & 0xff] = kNone;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const unsigned p = (t >> (8 * i)) & 0xff;
+      w.next[p] = kNone;
+      for (int k = 0; k < mw; ++k) w.emask[p * mw + k] = 0u;
+    }
   }
   __syncwarp();
-  // boundary edges: link next[u] = v; a plane that starts two edges makes
-  // the cavity non-manifold
+  // mark every directed edge a->b of a removed triangle: bit b of mask a
+  for (int r = lane; r < nrem; r += 32) {
+    const unsigned t = w.rem[r];
+    const unsigned a = t & 0xff, b = (t >> 8) & 0xff, c = (t >> 16) & 0xff;
+    atomicOr(&w.emask[a * mw + (b >> 5)], 1u << (b & 31));
+    atomicOr(&w.emask[b * mw + (c >> 5)], 1u << (c & 31));
+    atomicOr(&w.emask[c * mw + (a >> 5)], 1u << (a & 31));
+  }
+  __syncwarp();
+  // boundary edges: directed edges whose twin is unmarked, in removed order;
+  // link next[u] = v (a plane starting two edges makes the cavity
+  // non-manifold)
   int nb = 0;
   bool bad = false;
   unsigned first_u = kNone;
-  for (int r = lane; r < nrem; r += 32) {
-    const unsigned t = w.rem[r];
-    const unsigned tv[3] = {t & 0xff, (t >> 8) & 0xff, (t >> 16) & 0xff};
+  for (int r0 = 0; r0 < nrem; r0 += 32) {
+    const int r = r0 + lane;
+    unsigned t = 0, bmask = 0;  // bit e3: edge (tv[e3], tv[e3+1]) is on the boundary
+    if (r < nrem) {
+      t = w.rem[r];
+#pragma unroll
+      for (int e3 = 0; e3 < 3; ++e3) {
+        const unsigned u = (t >> (8 * e3)) & 0xff, v = (t >> (8 * ((e3 + 1) % 3))) & 0xff;
+        if (!((w.emask[v * mw + (u >> 5)] >> (u & 31)) & 1u)) bmask |= 1u << e3;
+      }
+    }
+    const int cnt = __popc(bmask);
+    const int incl = warp_incl_scan(cnt, lane);
+    int pos = nb + incl - cnt;
 #pragma unroll
     for (int e3 = 0; e3 < 3; ++e3) {
-      const unsigned u = tv[e3], v = tv[(e3 + 1) % 3];
-      if (has_twin(w.rem, nrem, u, v)) continue;
+      if (!((bmask >> e3) & 1u)) continue;
+      const unsigned u = (t >> (8 * e3)) & 0xff, v = (t >> (8 * ((e3 + 1) % 3))) & 0xff;
+      if (pos < w.vc) w.edge[pos] = u | (v << 8);
+      ++pos;
       if (atomicCAS(&w.next[u], kNone, v) != kNone) bad = true;
       if (first_u == kNone) first_u = u;
-      ++nb;
     }
+    nb += __shfl_sync(kFull, incl, 31);
   }
-  nb = warp_sumi(nb);
   bad = __any_sync(kFull, bad);
   __syncwarp();
   if (!bad) {
     // the links must form a single cycle through all nb edges
     const unsigned has = __ballot_sync(kFull, first_u != kNone);
     const unsigned u0 = __shfl_sync(kFull, first_u, has ? __ffs(has) - 1 : 0);
-    int steps = 0;
     bool ok = false;
     if (lane == 0 && u0 != kNone) {
       unsigned u = u0;
+      int steps = 0;
       do {
         u = w.next[u];
         ++steps;
@@ -340,36 +389,6 @@ __device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, u
   if (F > V) {
     status = kVertexOverflow;
     return -1;
-  }
-  // boundary edge list in deterministic order
-  {
-    int base = 0;
-    for (int r0 = 0; r0 < nrem; r0 += 32) {
-      const int r = r0 + lane;
-      unsigned ue[3], ve[3];
-      int cnt = 0;
-      if (r < nrem) {
-        const unsigned t = w.rem[r];
-        const unsigned tv[3] = {t & 0xff, (t >> 8) & 0xff, (t >> 16) & 0xff};
-#pragma unroll
-        for (int e3 = 0; e3 < 3; ++e3) {
-          const unsigned u = tv[e3], v = tv[(e3 + 1) % 3];
-          if (!has_twin(w.rem, nrem, u, v)) {
-            ue[cnt] = u;
-            ve[cnt] = v;
-            ++cnt;
-          }
-        }
-      }
-      int incl = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t2 = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t2;
-      }
-      for (int k = 0; k < cnt; ++k) w.edge[base + incl - cnt + k] = ue[k] | (ve[k] << 8);
-      base += __shfl_sync(kFull, incl, 31);
-    }
   }
   // holes = removed positions below F; movers = survivors at or past F
   int nholes = 0, nmov = 0;
@@ -392,20 +411,22 @@ __device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, u
   }
   __syncwarp();
   const int in_holes = nholes - nmov;
+  bool degenerate = false;
   for (int q = lane; q < nb; q += 32) {
     const unsigned ed = w.edge[q];
     const int dst = q < in_holes ? int(w.hole[nmov + q]) : w.nv + (q - in_holes);
-    make_vertex(w, dst, unsigned(pid), ed & 0xff, (ed >> 8) & 0xff);
+    degenerate |= !make_vertex(w, dst, unsigned(pid), ed & 0xff, (ed >> 8) & 0xff);
   }
   __syncwarp();
-  if (ctr && lane == 0) {
-    ctr[kCtrClips] += 1;
-    ctr[kCtrVerticesMade] += nb;
+  if (__any_sync(kFull, degenerate)) {
+    status = kInconsistentBoundary;
+    return -1;
   }
+  count(ctr, kCtrClips, 1, lane);
+  count(ctr, kCtrVerticesMade, nb, lane);
   w.nv = F;
   w.np = pid + 1;
   if (tr) {
-    // every vertex after the clip: triple and cofactor
     for (int v = 0; v < F; ++v) {
       const unsigned t = w.tri[v];
       trace_rec(tr, trcap, lane, 3, w.cx[v], w.cy[v], w.cz[v], w.cw[v], t & 0xff, (t >> 8) & 0xff, (t >> 16) & 0xff, v);
@@ -416,84 +437,68 @@ __device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, u
 
 // Signed-tet integration of the cell (ConvexCell.cl:577-619) in the local
 // frame: per vertex A and each of its planes i, the two tets (A, C, C
-// projected on plane i, C projected on the edge line of planes i, j).
+// projected on plane i, C projected on the edge line of planes i, j), C the
+// seed at the origin.  Unit normals make the plane projection division-free.
 // Accumulates (sum w*centroid, sum w)/6 * factor into acc (warp-uniform).
 template <int VS>
-__device__ void integrate(const WarpCell &w, double factor, double acc[4], int lane,
-                          unsigned long long *ctr, double *tr = nullptr, int trcap = 0) {
+__device__ void integrate(const WarpCell &w, double factor, double acc[4], int lane, unsigned long long *ctr,
+                          double *tr, int trcap) {
   double sx = 0, sy = 0, sz = 0, sw = 0;
-#pragma unroll
+#pragma unroll 1
   for (int s = 0; s < VS; ++s) {
+    if (s * 32 >= w.nv) break;
     const int v = s * 32 + lane;
     if (v >= w.nv) continue;
     const double inv = 1.0 / w.cw[v];
     const double Ax = w.cx[v] * inv, Ay = w.cy[v] * inv, Az = w.cz[v] * inv;
-    const double ACx = -Ax, ACy = -Ay, ACz = -Az;
     const unsigned t = w.tri[v];
-    double nx[3], ny[3], nz[3];
+    // AC = -A; projections of C on plane i: P_i = AC - (AC . n_i) n_i
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const Plane &p = w.plane[(t >> (8 * i)) & 0xff];
-      nx[i] = p.x;
-      ny[i] = p.y;
-      nz[i] = p.z;
-    }
-    double Px[3], Py[3], Pz[3], Lx[3], Ly[3], Lz[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const double k = (ACx * nx[i] + ACy * ny[i] + ACz * nz[i]) / (nx[i] * nx[i] + ny[i] * ny[i] + nz[i] * nz[i]);
-      Px[i] = ACx - k * nx[i];
-      Py[i] = ACy - k * ny[i];
-      Pz[i] = ACz - k * nz[i];
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const int j = (i + 1) % 3;
-      const double cxv = ny[i] * nz[j] - nz[i] * ny[j];
-      const double cyv = nz[i] * nx[j] - nx[i] * nz[j];
-      const double czv = nx[i] * ny[j] - ny[i] * nx[j];
+      const Plane &pi = w.plane[(t >> (8 * i)) & 0xff];
+      const Plane &pj = w.plane[(t >> (8 * ((i + 1) % 3))) & 0xff];
+      const double cxv = pi.y * pj.z - pi.z * pj.y;
+      const double cyv = pi.z * pj.x - pi.x * pj.z;
+      const double czv = pi.x * pj.y - pi.y * pj.x;
       const double c2 = cxv * cxv + cyv * cyv + czv * czv;
-      const double ni2 = nx[i] * nx[i] + ny[i] * ny[i] + nz[i] * nz[i];
-      const double nj2 = nx[j] * nx[j] + ny[j] * ny[j] + nz[j] * nz[j];
-      if (c2 < kVolEps2 * ni2 * nj2) {
-        Lx[i] = Ly[i] = Lz[i] = 0.0;
-      } else {
-        const double k = (ACx * cxv + ACy * cyv + ACz * czv) / c2;
-        Lx[i] = k * cxv;
-        Ly[i] = k * cyv;
-        Lz[i] = k * czv;
+      double Lx = 0, Ly = 0, Lz = 0;
+      if (c2 >= kVolEps2) {
+        const double k = -(Ax * cxv + Ay * cyv + Az * czv) / c2;
+        Lx = k * cxv;
+        Ly = k * cyv;
+        Lz = k * czv;
       }
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
+      // line i (planes i, i+1) pairs with plane i (sign -) and plane i+1
+      // (sign +): the reference's j = (i + 3 - st) % 3, w = (2 st - 1) det
 #pragma unroll
       for (int st = 0; st < 2; ++st) {
-        const int j = (i + 3 - st) % 3;
-        // det3 of rows AC, P_i, L_j expanded along the first column
-        const double det = ACx * (Py[i] * Lz[j] - Pz[i] * Ly[j]) - Px[i] * (ACy * Lz[j] - ACz * Ly[j]) +
-                           Lx[j] * (ACy * Pz[i] - ACz * Py[i]);
-        const double wt = (2 * st - 1) * det;
+        const Plane &pp = st ? pj : pi;
+        const double k = -(Ax * pp.x + Ay * pp.y + Az * pp.z);
+        const double Px = -Ax - k * pp.x, Py = -Ay - k * pp.y, Pz = -Az - k * pp.z;
+        const double det = -Ax * (Py * Lz - Pz * Ly) - Px * (-Ay * Lz + Az * Ly) + Lx * (-Ay * Pz + Az * Py);
+        const double wt = st ? det : -det;
         sw += wt;
-        sx += wt * (Ax + 0.25 * (ACx + Px[i] + Lx[j]));
-        sy += wt * (Ay + 0.25 * (ACy + Py[i] + Ly[j]));
-        sz += wt * (Az + 0.25 * (ACz + Pz[i] + Lz[j]));
+        sx += wt * (Ax + 0.25 * (Px + Lx - Ax));
+        sy += wt * (Ay + 0.25 * (Py + Ly - Ay));
+        sz += wt * (Az + 0.25 * (Pz + Lz - Az));
       }
     }
   }
-  sx = warp_sum(sx);
-  sy = warp_sum(sy);
-  sz = warp_sum(sz);
-  sw = warp_sum(sw);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(kFull, sx, o);
+    sy += __shfl_xor_sync(kFull, sy, o);
+    sz += __shfl_xor_sync(kFull, sz, o);
+    sw += __shfl_xor_sync(kFull, sw, o);
+  }
   const double f = factor / 6.0;
   trace_rec(tr, trcap, lane, 4, f * sx, f * sy, f * sz, f * sw, factor, w.nv, w.np);
   acc[0] += f * sx;
   acc[1] += f * sy;
   acc[2] += f * sz;
   acc[3] += f * sw;
-  if (ctr && lane == 0) {
-    ctr[kCtrExports] += 1;
-    ctr[kCtrExportVertices] += w.nv;
-  }
+  count(ctr, kCtrExports, 1, lane);
+  count(ctr, kCtrExportVertices, w.nv, lane);
 }
 
 template <int VS>
@@ -532,18 +537,24 @@ __device__ void restore(WarpCell &w, int nv, int np, int lane) {
   w.np = np;
 }
 
-// Plane through three points, normal (B-A) x (C-A), kept side where the
-// normal points (get_plane_from_points, ConvexCell.cl:125-129), in the local
-// frame.
+// Plane through three points with normal (B-A) x (C-A), normalised, kept side
+// where the normal points (get_plane_from_points, ConvexCell.cl:125-129), in
+// the local frame; all zero when the points are collinear.
 __device__ __forceinline__ Plane plane_from_points(const double A[3], const double B[3], const double C[3]) {
   const double ux = B[0] - A[0], uy = B[1] - A[1], uz = B[2] - A[2];
   const double vx = C[0] - A[0], vy = C[1] - A[1], vz = C[2] - A[2];
-  const double nx = uy * vz - uz * vy, ny = uz * vx - ux * vz, nz = ux * vy - uy * vx;
+  double nx = uy * vz - uz * vy, ny = uz * vx - ux * vz, nz = ux * vy - uy * vx;
+  const double l2 = nx * nx + ny * ny + nz * nz;
+  if (!(l2 > 0.0)) return Plane{0.0, 0.0, 0.0, 0.0};
+  const double il = rsqrt(l2);
+  nx *= il;
+  ny *= il;
+  nz *= il;
   return Plane{nx, ny, nz, -(nx * A[0] + ny * A[1] + nz * A[2])};
 }
 
 // Pt0 fallback one voxel layer past the range (GRID_OUT_DOMAIN,
-// ConvexCell.cl:986-1051): lane 0 scans, others wait.
+// ConvexCell.cl:986-1051): run by one lane.
 __device__ int out_domain_corner(const DevGrid &g, const int vmin[3], const int vmax[3], int &px, int &py,
                                  int &pz) {
   const int S = g.size;
@@ -661,9 +672,8 @@ __device__ __forceinline__ bool ball_outside(const DevGrid &g, float4 s, double 
   const double c[3] = {s.x, s.y, s.z};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    lo[d] = max(0, int((c[d] - r) / double(g.voxel)));
-    hi[d] = min(g.size - 1, int((c[d] + r) / double(g.voxel)));
-    if (c[d] - r < 0.0) lo[d] = 0;
+    lo[d] = c[d] - r <= 0.0 ? 0 : min(g.size - 1, int((c[d] - r) / double(g.voxel)));
+    hi[d] = c[d] + r <= 0.0 ? 0 : min(g.size - 1, int((c[d] + r) / double(g.voxel)));
   }
   const int S1 = g.size + 1;
   int v = 0;
@@ -679,8 +689,202 @@ __device__ __forceinline__ bool ball_outside(const DevGrid &g, float4 s, double 
   return __shfl_sync(kFull, v, 0) == 0;
 }
 
+// Domain restriction of the clipped cell (ConvexCell.cl:918-1116): start
+// corner, boundary triangles, signed cone decomposition.  Adds the cell's
+// moments to acc; returns the status.
+template <int VS>
+__device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout &L, float4 s, double acc[4],
+                                  int lane, unsigned long long *ctr, double *tr, int trcap) {
+  const DevGrid &g = a.grid;
+  // bounding box -> voxel range (ConvexCell.cl:924-940)
+  double lo[3] = {1000.0, 1000.0, 1000.0}, hi[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int sl = 0; sl < VS; ++sl) {
+    const int v = sl * 32 + lane;
+    if (v < w.nv) {
+      const double inv = 1.0 / w.cw[v];
+      const double p[3] = {w.cx[v] * inv + s.x, w.cy[v] * inv + s.y, w.cz[v] * inv + s.z};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fmin(lo[d], p[d]);
+        hi[d] = fmax(hi[d], p[d]);
+      }
+    }
+  }
+  int vmin[3], vmax[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(kFull, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(kFull, hi[d], o));
+    }
+    vmin[d] = max(0, int(lo[d] / double(g.voxel)));
+    vmax[d] = min(g.size - 1, int(hi[d] / double(g.voxel)));
+  }
+  const int S = g.size;
+  const int ex = vmax[0] - vmin[0] + 1, ey = vmax[1] - vmin[1] + 1, ez = vmax[2] - vmin[2] + 1;
+  const int nvox = (ex > 0 && ey > 0 && ez > 0) ? ex * ey * ez : 0;
+  // first corner with flag != 1 in (z, y, x) scan order, and the triangle ids
+  // of every voxel in the range
+  int in_domain = 1, c0 = -1;
+  int ntr = 0;
+  bool spill = false;
+  for (int b0 = 0; b0 < nvox; b0 += 32) {
+    const int q = b0 + lane;
+    int vid = -1, lo_off = 0, cntv = 0;
+    int f = 1;
+    if (q < nvox) {
+      const int x = vmin[0] + q % ex, y = vmin[1] + (q / ex) % ey, z = vmin[2] + q / (ex * ey);
+      vid = x + y * S + z * S * S;
+      f = g.flags[vid];
+      lo_off = __ldg(&g.offsets[vid]);
+      cntv = __ldg(&g.offsets[vid + 1]) - lo_off;
+    }
+    if (in_domain == 1) {
+      const unsigned fm = __ballot_sync(kFull, f != 1);
+      if (fm) {
+        const int src = __ffs(fm) - 1;
+        in_domain = __shfl_sync(kFull, f, src);
+        c0 = __shfl_sync(kFull, vid, src);
+      }
+    }
+    const int incl = warp_incl_scan(cntv, lane);
+    const int tot = __shfl_sync(kFull, incl, 31);
+    if (ntr + tot > L.G) {
+      spill = true;
+    } else if (!spill) {
+      for (int k = 0; k < cntv; ++k) w.tlist[ntr + incl - cntv + k] = __ldg(&g.list[lo_off + k]);
+    }
+    ntr += tot;
+  }
+  __syncwarp();
+  int nuniq = 0;
+  if (g.lists_disjoint) {
+    // no triangle is listed twice: the union is the concatenation
+    if (ntr > a.T) return kTriangleOverflow;
+    nuniq = ntr;
+  } else if (spill) {
+    // more ids (with repeats) than the sort buffer holds: one lane builds the
+    // sorted union voxel by voxel, failing past T like the reference's merge
+    int cntu = 0;
+    if (lane == 0) cntu = serial_union(g, vmin, vmax, a.T, w.tlist, L.G);
+    cntu = __shfl_sync(kFull, cntu, 0);
+    __syncwarp();
+    if (cntu < 0) return kTriangleOverflow;
+    nuniq = cntu;
+  } else if (ntr > 0) {
+    const int n2 = pow2_at_least(ntr);
+    for (int i = ntr + lane; i < n2; i += 32) w.tlist[i] = 0x7fffffff;
+    __syncwarp();
+    warp_sort_ints(w.tlist, n2, lane);
+    for (int i0 = 0; i0 < ntr; i0 += 32) {
+      const int i = i0 + lane;
+      const int v = i < ntr ? w.tlist[i] : 0x7fffffff;
+      const bool keep = i < ntr && (i == 0 || w.tlist[i - 1] != v);
+      const unsigned km = __ballot_sync(kFull, keep);
+      __syncwarp();
+      if (keep) w.tlist[nuniq + __popc(km & lanemask_lt(lane))] = v;
+      __syncwarp();
+      nuniq += __popc(km);
+    }
+    if (nuniq > a.T) return kTriangleOverflow;
+  }
+  double pt0[3] = {0, 0, 0};
+  if (in_domain == 1) {
+    int px = 0, py = 0, pz = 0, f = 1;
+    if (a.out_domain && lane == 0) f = out_domain_corner(g, vmin, vmax, px, py, pz);
+    f = __shfl_sync(kFull, f, 0);
+    if (f == 1) return kFindAnotherBeginningVertex;
+    in_domain = f;
+    pt0[0] = __shfl_sync(kFull, px, 0) * double(g.voxel) - s.x;
+    pt0[1] = __shfl_sync(kFull, py, 0) * double(g.voxel) - s.y;
+    pt0[2] = __shfl_sync(kFull, pz, 0) * double(g.voxel) - s.z;
+  } else {
+    const int x = c0 % S, y = (c0 / S) % S, z = c0 / (S * S);
+    pt0[0] = x * double(g.voxel) - s.x;
+    pt0[1] = y * double(g.voxel) - s.y;
+    pt0[2] = z * double(g.voxel) - s.z;
+  }
+  trace_rec(tr, trcap, lane, 5, pt0[0], pt0[1], pt0[2], in_domain, nuniq);
+  if (in_domain == 2) integrate<VS>(w, 1.0, acc, lane, ctr, tr, trcap);
+  if (nuniq == 0) return kSuccess;
+  count(ctr, kCtrBoundaryCells, 1, lane);
+  count(ctr, kCtrTriangles, nuniq, lane);
+  const int bk_nv = w.nv, bk_np = w.np;
+  backup<VS>(w, lane);
+  // signed cone decomposition over the boundary triangles
+  // (ConvexCell.cl:1082-1115)
+  if (lane < 3) w.pts[lane] = pt0[lane];
+  for (int ti = 0; ti < nuniq; ++ti) {
+    const int tri = w.tlist[ti];
+    bool go_out = false;
+    if (lane == 0) {
+      // triangle in the local frame, oriented to go out from pt0
+      const int i1 = __ldg(&g.tris[3 * tri]), i2 = __ldg(&g.tris[3 * tri + 1]), i3 = __ldg(&g.tris[3 * tri + 2]);
+      const float4 q1 = __ldg(&g.points[i1]), q2 = __ldg(&g.points[i2]), q3 = __ldg(&g.points[i3]);
+      const double P1[3] = {double(q1.x) - s.x, double(q1.y) - s.y, double(q1.z) - s.z};
+      const double P2[3] = {double(q2.x) - s.x, double(q2.y) - s.y, double(q2.z) - s.z};
+      const double P3[3] = {double(q3.x) - s.x, double(q3.y) - s.y, double(q3.z) - s.z};
+      const double ax = P1[0] - pt0[0], ay = P1[1] - pt0[1], az = P1[2] - pt0[2];
+      const double bx = P2[0] - pt0[0], by = P2[1] - pt0[1], bz = P2[2] - pt0[2];
+      const double cx = P3[0] - pt0[0], cy = P3[1] - pt0[1], cz = P3[2] - pt0[2];
+      const double det = ax * (by * cz - bz * cy) - bx * (ay * cz - az * cy) + cx * (ay * bz - az * by);
+      go_out = det > 0;
+      trace_rec(tr, trcap, lane, 6, tri, det, go_out, 0);
+      for (int d = 0; d < 3; ++d) {
+        w.pts[3 + d] = P1[d];
+        w.pts[6 + d] = go_out ? P2[d] : P3[d];
+        w.pts[9 + d] = go_out ? P3[d] : P2[d];
+      }
+    }
+    go_out = __shfl_sync(kFull, go_out, 0);
+    __syncwarp();
+    // the cone beyond triangle (P1, P2, P3) seen from pt0
+    // (CCClipTetFromPointsInfinite, ConvexCell.cl:565-575): faces
+    // (pt0, P1, P2), (pt0, P3, P1), (pt0, P2, P3), (P2, P3, P1)
+    if (w.np >= a.P) return kPlaneOverflow;
+    const double *q0 = w.pts, *q1 = w.pts + 3, *q2 = w.pts + 6, *q3 = w.pts + 9;
+    auto cone = [&](int f4) {
+      return f4 == 0 ? plane_from_points(q0, q1, q2)
+                     : f4 == 1 ? plane_from_points(q0, q3, q1)
+                               : f4 == 2 ? plane_from_points(q0, q2, q3) : plane_from_points(q2, q3, q1);
+    };
+    // quick classification: a plane that cuts every vertex empties the
+    // piece; no plane cutting any vertex means the cell lies in the cone
+    bool empty = false, any_cut = false;
+#pragma unroll 1
+    for (int f4 = 0; f4 < 4 && !empty; ++f4) {
+      unsigned rm[VS];
+      const int nr = cut_masks<VS>(w, cone(f4), rm, lane);
+      empty |= nr == w.nv;
+      any_cut |= nr > 0;
+    }
+    if (empty) continue;
+    if (any_cut) {
+      int cstat = kSuccess;
+#pragma unroll 1
+      for (int f4 = 0; f4 < 4 && cstat == kSuccess; ++f4) {
+        if (w.np >= a.P) {
+          cstat = kPlaneOverflow;
+          break;
+        }
+        clip<VS>(w, cone(f4), a.V, cstat, lane, ctr, tr, trcap);
+      }
+      if (cstat == kEmptyCell) {
+        restore<VS>(w, bk_nv, bk_np, lane);
+        continue;
+      }
+      if (cstat != kSuccess) return cstat;
+    }
+    integrate<VS>(w, go_out ? 1.0 : -1.0, acc, lane, ctr, tr, trcap);
+    if (any_cut) restore<VS>(w, bk_nv, bk_np, lane);
+  }
+  return kSuccess;
+}
+
 template <int VS, bool GRID>
-__global__ void __launch_bounds__(128) k_cell(CellLaunch a, Layout L) {
+__global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -688,12 +892,6 @@ __global__ void __launch_bounds__(128) k_cell(CellLaunch a, Layout L) {
   if (row >= a.num) return;
   WarpCell w = bind(smem + size_t(wib) * L.total, L);
   unsigned long long *ctr = a.counters;
-  // per-warp counters are accumulated in lane 0's registers, flushed once
-  unsigned long long lc[kCtrNum];
-#pragma unroll
-  for (int i = 0; i < kCtrNum; ++i) lc[i] = 0;
-  unsigned long long *lcp = ctr ? lc : nullptr;
-
   const int sid = a.ids ? a.ids[row] : row;
   const float4 s = a.stored[sid];
   double *tr = (a.trace && sid == a.trace_seed) ? a.trace : nullptr;
@@ -711,7 +909,7 @@ __global__ void __launch_bounds__(128) k_cell(CellLaunch a, Layout L) {
   init_box(w, s, a.cube_eps, lane);
   double R2 = cell_radius2<VS>(w, lane);
 
-  // ---- Voronoi / power clipping by the K nearest, in order ----
+  // ---- power clipping by the K nearest, in order ----
   const unsigned *nrow = a.knn + size_t(row) * a.K;
   bool reached = false, exhausted = false, outside = false;
   const bool early = GRID && a.early_out && a.grid.sat != nullptr;
@@ -728,7 +926,7 @@ __global__ void __launch_bounds__(128) k_cell(CellLaunch a, Layout L) {
         const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
         nd2 = bx * bx + by * by + bz * bz;
         const double len = sqrt(nd2);
-        // kept side contains the seed: n = -(b - s)/|b - s|, offset from the
+        // kept side contains the seed: n = -(b - s)/|b - s|, offset of the
         // power bisector (ConvexCell.cl:321-328) or, for a wall neighbour,
         // through the neighbour itself
         const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) / (2.0 * len);
@@ -745,12 +943,12 @@ __global__ void __launch_bounds__(128) k_cell(CellLaunch a, Layout L) {
       }
       const Plane e = shfl_plane(pl, j);
       const double d2j = __shfl_sync(kFull, nd2, j);
-      if (lcp && lane == 0) ++lcp[kCtrPlanesTested];
+      count(ctr, kCtrPlanesTested, 1, lane);
       if (w.np >= a.P) {
         status = kPlaneOverflow;
         break;
       }
-      const int r = clip<VS>(w, e, a.V, status, lane, lcp, tr, trcap);
+      const int r = clip<VS>(w, e, a.V, status, lane, ctr, tr, trcap);
       if (r < 0) break;
       if (r > 0) {
         R2 = cell_radius2<VS>(w, lane);
@@ -766,194 +964,12 @@ __global__ void __launch_bounds__(128) k_cell(CellLaunch a, Layout L) {
     }
   }
   if (status == kSuccess && !reached && !exhausted && !outside) status = kSecurityRadiusNotReached;
-  if (outside && lcp && lane == 0) lcp[kCtrOutside] += 1;
-
+  if (outside) count(ctr, kCtrOutside, 1, lane);
   if (status == kSuccess && !outside) {
-    bool add_volume = true;
-    if (GRID) {
-      const DevGrid &g = a.grid;
-      // bounding box -> voxel range (ConvexCell.cl:924-940)
-      double lo[3] = {1000.0, 1000.0, 1000.0}, hi[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-      for (int sl = 0; sl < VS; ++sl) {
-        const int v = sl * 32 + lane;
-        if (v < w.nv) {
-          const double inv = 1.0 / w.cw[v];
-          const double p[3] = {w.cx[v] * inv + s.x, w.cy[v] * inv + s.y, w.cz[v] * inv + s.z};
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            lo[d] = fmin(lo[d], p[d]);
-            hi[d] = fmax(hi[d], p[d]);
-          }
-        }
-      }
-      int vmin[3], vmax[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          lo[d] = fmin(lo[d], __shfl_xor_sync(kFull, lo[d], o));
-          hi[d] = fmax(hi[d], __shfl_xor_sync(kFull, hi[d], o));
-        }
-        vmin[d] = max(0, int(lo[d] / double(g.voxel)));
-        vmax[d] = min(g.size - 1, int(hi[d] / double(g.voxel)));
-      }
-      const int S = g.size;
-      const int ex = vmax[0] - vmin[0] + 1, ey = vmax[1] - vmin[1] + 1, ez = vmax[2] - vmin[2] + 1;
-      const int nvox = (ex > 0 && ey > 0 && ez > 0) ? ex * ey * ez : 0;
-      // first corner with flag != 1 in (z, y, x) scan order, and the gathered
-      // triangle ids of every voxel in the range
-      int in_domain = 1, c0 = -1;
-      int ntr = 0;
-      bool spill = false;
-      for (int b0 = 0; b0 < nvox; b0 += 32) {
-        const int q = b0 + lane;
-        int vid = -1, lo_off = 0, cntv = 0;
-        int f = 1;
-        if (q < nvox) {
-          const int x = vmin[0] + q % ex, y = vmin[1] + (q / ex) % ey, z = vmin[2] + q / (ex * ey);
-          vid = x + y * S + z * S * S;
-          f = g.flags[vid];
-          lo_off = __ldg(&g.offsets[vid]);
-          cntv = __ldg(&g.offsets[vid + 1]) - lo_off;
-        }
-        if (in_domain == 1) {
-          const unsigned fm = __ballot_sync(kFull, f != 1);
-          if (fm) {
-            const int src = __ffs(fm) - 1;
-            in_domain = __shfl_sync(kFull, f, src);
-            c0 = __shfl_sync(kFull, vid, src);
-          }
-        }
-        int incl = cntv;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int t2 = __shfl_up_sync(kFull, incl, o);
-          if (lane >= o) incl += t2;
-        }
-        const int tot = __shfl_sync(kFull, incl, 31);
-        if (ntr + tot > L.G) {
-          spill = true;
-        } else {
-          for (int k = 0; k < cntv; ++k) w.tlist[ntr + incl - cntv + k] = __ldg(&g.list[lo_off + k]);
-        }
-        ntr += tot;
-      }
-      __syncwarp();
-      int nuniq = 0;
-      if (spill) {
-        // more ids (with repeats) than the sort buffer holds: lane 0 builds
-        // the sorted union voxel by voxel, failing past T like the
-        // reference's merge (ConvexCell.cl:722-749)
-        int cntu = 0;
-        if (lane == 0) cntu = serial_union(g, vmin, vmax, a.T, w.tlist, L.G);
-        cntu = __shfl_sync(kFull, cntu, 0);
-        __syncwarp();
-        if (cntu < 0) status = kTriangleOverflow;
-        else nuniq = cntu;
-      } else if (ntr > 0) {
-        const int n2 = pow2_at_least(ntr);
-        for (int i = ntr + lane; i < n2; i += 32) w.tlist[i] = 0x7fffffff;
-        __syncwarp();
-        warp_sort_ints(w.tlist, n2, lane);
-        // unique in place
-        for (int i0 = 0; i0 < ntr; i0 += 32) {
-          const int i = i0 + lane;
-          const int v = i < ntr ? w.tlist[i] : 0x7fffffff;
-          const bool keep = i < ntr && (i == 0 || w.tlist[i - 1] != v);
-          const unsigned km = __ballot_sync(kFull, keep);
-          __syncwarp();
-          if (keep) w.tlist[nuniq + __popc(km & lanemask_lt(lane))] = v;
-          __syncwarp();
-          nuniq += __popc(km);
-        }
-        if (nuniq > a.T) status = kTriangleOverflow;
-      }
-      double pt0[3] = {0, 0, 0};
-      if (status == kSuccess) {
-        if (in_domain == 1) {
-          int px = 0, py = 0, pz = 0, f = 1;
-          if (a.out_domain && lane == 0) f = out_domain_corner(g, vmin, vmax, px, py, pz);
-          f = __shfl_sync(kFull, f, 0);
-          if (f == 1) {
-            status = kFindAnotherBeginningVertex;
-          } else {
-            in_domain = f;
-            pt0[0] = __shfl_sync(kFull, px, 0) * double(g.voxel) - s.x;
-            pt0[1] = __shfl_sync(kFull, py, 0) * double(g.voxel) - s.y;
-            pt0[2] = __shfl_sync(kFull, pz, 0) * double(g.voxel) - s.z;
-          }
-        } else {
-          const int x = c0 % S, y = (c0 / S) % S, z = c0 / (S * S);
-          pt0[0] = x * double(g.voxel) - s.x;
-          pt0[1] = y * double(g.voxel) - s.y;
-          pt0[2] = z * double(g.voxel) - s.z;
-        }
-      }
-      if (status == kSuccess) {
-        add_volume = in_domain == 2;
-        trace_rec(tr, trcap, lane, 5, pt0[0], pt0[1], pt0[2], in_domain, nuniq, status);
-        if (add_volume) integrate<VS>(w, 1.0, acc, lane, lcp, tr, trcap);
-        if (nuniq > 0) {
-          if (lcp && lane == 0) {
-            lcp[kCtrBoundaryCells] += 1;
-            lcp[kCtrTriangles] += nuniq;
-          }
-          const int bk_nv = w.nv, bk_np = w.np;
-          backup<VS>(w, lane);
-          // signed cone decomposition over the boundary triangles
-          // (ConvexCell.cl:1082-1115)
-          for (int ti = 0; ti < nuniq && status == kSuccess; ++ti) {
-            const int tri = w.tlist[ti];
-            double P1[3], P2[3], P3[3];
-            const int i1 = __ldg(&g.tris[3 * tri]), i2 = __ldg(&g.tris[3 * tri + 1]), i3 = __ldg(&g.tris[3 * tri + 2]);
-            const float4 q1 = __ldg(&g.points[i1]), q2 = __ldg(&g.points[i2]), q3 = __ldg(&g.points[i3]);
-            P1[0] = double(q1.x) - s.x; P1[1] = double(q1.y) - s.y; P1[2] = double(q1.z) - s.z;
-            P2[0] = double(q2.x) - s.x; P2[1] = double(q2.y) - s.y; P2[2] = double(q2.z) - s.z;
-            P3[0] = double(q3.x) - s.x; P3[1] = double(q3.y) - s.y; P3[2] = double(q3.z) - s.z;
-            const double ax = P1[0] - pt0[0], ay = P1[1] - pt0[1], az = P1[2] - pt0[2];
-            const double bx = P2[0] - pt0[0], by = P2[1] - pt0[1], bz = P2[2] - pt0[2];
-            const double cx = P3[0] - pt0[0], cy = P3[1] - pt0[1], cz = P3[2] - pt0[2];
-            const double det = ax * (by * cz - bz * cy) - bx * (ay * cz - az * cy) + cx * (ay * bz - az * by);
-            const bool go_out = det > 0;
-            trace_rec(tr, trcap, lane, 6, tri, det, go_out, 0);
-            if (!go_out) {
-#pragma unroll
-              for (int d = 0; d < 3; ++d) {
-                const double tmp = P2[d];
-                P2[d] = P3[d];
-                P3[d] = tmp;
-              }
-            }
-            // cone beyond triangle (P1, P2, P3) seen from pt0
-            // (CCClipTetFromPointsInfinite, ConvexCell.cl:565-575)
-            const double *faces[4][3] = {{pt0, P1, P2}, {pt0, P3, P1}, {pt0, P2, P3}, {P2, P3, P1}};
-            int cstat = kSuccess;
-            for (int f4 = 0; f4 < 4 && cstat == kSuccess; ++f4) {
-              if (w.np >= a.P) {
-                cstat = kPlaneOverflow;
-                break;
-              }
-              const Plane e = plane_from_points(faces[f4][0], faces[f4][1], faces[f4][2]);
-              clip<VS>(w, e, a.V, cstat, lane, lcp, tr, trcap);
-            }
-            if (cstat == kEmptyCell) {
-              restore<VS>(w, bk_nv, bk_np, lane);
-              continue;
-            }
-            if (cstat != kSuccess) {
-              status = cstat;
-              acc[3] = 0.0;
-              break;
-            }
-            integrate<VS>(w, go_out ? 1.0 : -1.0, acc, lane, lcp, tr, trcap);
-            restore<VS>(w, bk_nv, bk_np, lane);
-          }
-        }
-      }
-    }
-    if (!GRID && status == kSuccess) integrate<VS>(w, 1.0, acc, lane, lcp, tr, trcap);
-    (void)add_volume;
+    if (GRID)
+      status = restrict_to_domain<VS>(w, a, L, s, acc, lane, ctr, tr, trcap);
+    else
+      integrate<VS>(w, 1.0, acc, lane, ctr, tr, trcap);
   }
   if (lane == 0) {
     a.status[sid] = status;
@@ -963,11 +979,6 @@ __global__ void __launch_bounds__(128) k_cell(CellLaunch a, Layout L) {
       a.out[sid] = make_double4(acc[0] + m * double(s.x), acc[1] + m * double(s.y), acc[2] + m * double(s.z), m);
     else
       a.out[sid] = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (ctr) {
-#pragma unroll
-      for (int i = 0; i < kCtrNum; ++i)
-        if (lc[i]) atomicAdd(&ctr[i], lc[i]);
-    }
   }
 }
 

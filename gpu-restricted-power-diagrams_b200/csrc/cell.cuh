@@ -17,6 +17,9 @@ struct DevGrid {
   // Summed-volume table, (size+1)^3, of voxels that are not plainly outside
   // (first-corner flag != 0 or a non-empty triangle list); null: unused.
   const int *sat = nullptr;
+  // No triangle id appears in two voxel lists: the union of the lists of a
+  // voxel range is their concatenation (no sort needed).
+  int lists_disjoint = 0;
 };
 
 // Counters of one launch (optional): cells by outcome and work done.

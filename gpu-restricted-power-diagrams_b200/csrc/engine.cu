@@ -408,6 +408,17 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
   d.list = s->g_list.as<const int>();
   d.offsets = s->g_offsets.as<const int>();
   d.sat = s->g_sat.as<const int>();
+  {
+    std::vector<unsigned char> seen(size_t(g->num_triangles()), 0);
+    d.lists_disjoint = 1;
+    for (int t : g->tri_list) {
+      if (seen[size_t(t)]) {
+        d.lists_disjoint = 0;
+        break;
+      }
+      seen[size_t(t)] = 1;
+    }
+  }
   d.has_border_corners = 0;
   for (char c : g->in_domain)
     if (c == 1) {
