@@ -206,6 +206,34 @@ int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st);
  * an rpd_error. */
 int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *p, double *records, int cap);
 
+/* --------------------------------------------------- allocation-free binning */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (code running inside another framework's memory pool, plugins whose
+ * host forbids allocation after start-up, paths that must not synchronize
+ * the device the way cudaMalloc/cudaFree do): bins n seeds that are already
+ * on the device into caller-owned device buffers, exactly as
+ * rpd_solver_set_points does (stable counting sort, same permutation and bin
+ * prefix sums), without allocating.  Its scratch lives in a fixed array of
+ * the library's static device memory (about 1.7 MB, held by every GPU that
+ * loads the library until the process exits).
+ *
+ *   xyzw      device, 4n floats, 16-byte aligned
+ *   stored    device, 4n floats, 16-byte aligned: seeds in stored order
+ *   perm      device, n ints: stored index -> user index
+ *   counters  device, counters_cap ints (>= dim^3 + 1): bin prefix sums
+ *   dim_out   receives dim = round((n / 3.1)^(1/3))
+ *   stream    cudaStream_t (null: the default stream)
+ *
+ * n > RPD_NOALLOC_MAX_SEEDS returns RPD_ERR_CAPACITY.  The first call on a
+ * device looks up the array's device address; make that first call before
+ * any stream capture.  Every call shares the one array, so calls that
+ * overlap on the GPU (other streams, other host threads) race: serialize
+ * them.  The call waits for its stream before returning. */
+#define RPD_NOALLOC_MAX_SEEDS 262144
+int rpd_bin_seeds_noalloc(const float *xyzw, int n, float *stored, int *perm, int *counters, int counters_cap,
+                          int *dim_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
