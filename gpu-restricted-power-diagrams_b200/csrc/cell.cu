@@ -41,6 +41,7 @@ namespace {
 constexpr unsigned kNone = 0xffffffffu;
 constexpr double kVolEps2 = 1e-12;  // VOLUME_EPSILON2 of the FP64 build (voronoi.cpp:922)
 constexpr double kTieEps = 1e-10;   // cut tolerance, reference-frame units
+constexpr int kDeferred = 100;      // internal status: cell parked for k_cone
 
 struct Layout {
   int Pc, Vc, G, Mw;  // Mw: 32-bit words of one plane's edge mask
@@ -689,12 +690,139 @@ __device__ __forceinline__ bool ball_outside(const DevGrid &g, float4 s, double 
   return __shfl_sync(kFull, v, 0) == 0;
 }
 
+// Signed cone decomposition over boundary triangles tids[t0, t1)
+// (ConvexCell.cl:1082-1115): for each, the cone beyond the triangle seen
+// from the start corner (w.pts[0..2]) clips the backed-up cell, the piece is
+// integrated with the triangle's sign, and the cell is restored.  Returns
+// the status; on failure fail_at is the failing triangle's position.
+template <int VS>
+__device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const int *tids, int t0, int t1,
+                              int bk_nv, int bk_np, double acc[4], int &fail_at, int lane, unsigned long long *ctr,
+                              double *tr, int trcap) {
+  const DevGrid &g = a.grid;
+  for (int ti = t0; ti < t1; ++ti) {
+    const int tri = tids[ti];
+    bool go_out = false;
+    if (lane == 0) {
+      // triangle in the local frame, oriented to go out from pt0
+      const double p0x = w.pts[0], p0y = w.pts[1], p0z = w.pts[2];
+      const int i1 = __ldg(&g.tris[3 * tri]), i2 = __ldg(&g.tris[3 * tri + 1]), i3 = __ldg(&g.tris[3 * tri + 2]);
+      const float4 q1 = __ldg(&g.points[i1]), q2 = __ldg(&g.points[i2]), q3 = __ldg(&g.points[i3]);
+      const double P1[3] = {double(q1.x) - s.x, double(q1.y) - s.y, double(q1.z) - s.z};
+      const double P2[3] = {double(q2.x) - s.x, double(q2.y) - s.y, double(q2.z) - s.z};
+      const double P3[3] = {double(q3.x) - s.x, double(q3.y) - s.y, double(q3.z) - s.z};
+      const double ax = P1[0] - p0x, ay = P1[1] - p0y, az = P1[2] - p0z;
+      const double bx = P2[0] - p0x, by = P2[1] - p0y, bz = P2[2] - p0z;
+      const double cx = P3[0] - p0x, cy = P3[1] - p0y, cz = P3[2] - p0z;
+      const double det = ax * (by * cz - bz * cy) - bx * (ay * cz - az * cy) + cx * (ay * bz - az * by);
+      go_out = det > 0;
+      trace_rec(tr, trcap, lane, 6, tri, det, go_out, 0);
+      for (int d = 0; d < 3; ++d) {
+        w.pts[3 + d] = P1[d];
+        w.pts[6 + d] = go_out ? P2[d] : P3[d];
+        w.pts[9 + d] = go_out ? P3[d] : P2[d];
+      }
+    }
+    go_out = __shfl_sync(kFull, go_out, 0);
+    __syncwarp();
+    // the cone beyond triangle (P1, P2, P3) seen from pt0
+    // (CCClipTetFromPointsInfinite, ConvexCell.cl:565-575): faces
+    // (pt0, P1, P2), (pt0, P3, P1), (pt0, P2, P3), (P2, P3, P1)
+    if (w.np >= a.P) {
+      fail_at = ti;
+      return kPlaneOverflow;
+    }
+    const double *q0 = w.pts, *q1 = w.pts + 3, *q2 = w.pts + 6, *q3 = w.pts + 9;
+    auto cone = [&](int f4) {
+      return f4 == 0 ? plane_from_points(q0, q1, q2)
+                     : f4 == 1 ? plane_from_points(q0, q3, q1)
+                               : f4 == 2 ? plane_from_points(q0, q2, q3) : plane_from_points(q2, q3, q1);
+    };
+    // quick classification: a plane that cuts every vertex empties the
+    // piece; no plane cutting any vertex means the cell lies in the cone
+    bool empty = false, any_cut = false;
+#pragma unroll 1
+    for (int f4 = 0; f4 < 4 && !empty; ++f4) {
+      unsigned rm[VS];
+      const int nr = cut_masks<VS>(w, cone(f4), rm, lane);
+      empty |= nr == w.nv;
+      any_cut |= nr > 0;
+    }
+    if (empty) continue;
+    if (any_cut) {
+      int cstat = kSuccess;
+#pragma unroll 1
+      for (int f4 = 0; f4 < 4 && cstat == kSuccess; ++f4) {
+        if (w.np >= a.P) {
+          cstat = kPlaneOverflow;
+          break;
+        }
+        clip<VS>(w, cone(f4), a.V, cstat, lane, ctr, tr, trcap);
+      }
+      if (cstat == kEmptyCell) {
+        restore<VS>(w, bk_nv, bk_np, lane);
+        continue;
+      }
+      if (cstat != kSuccess) {
+        fail_at = ti;
+        return cstat;
+      }
+    }
+    integrate<VS>(w, go_out ? 1.0 : -1.0, acc, lane, ctr, tr, trcap);
+    if (any_cut) restore<VS>(w, bk_nv, bk_np, lane);
+  }
+  return kSuccess;
+}
+
+// Parked boundary cell: header, planes, vertices, triangle ids.
+struct DeferHeader {
+  int sid, nuniq, nv, np;
+  double pt0[3];
+  double acc[4];
+  double pad[9];
+};
+static_assert(sizeof(DeferHeader) == 144, "defer header size");
+
+__host__ __device__ inline size_t slot_bytes_for(const Layout &L, int T) {
+  return size_t(align16(unsigned(sizeof(DeferHeader) + 32u * L.Pc + 44u * L.Vc + 4u * ((T + 3) & ~3))));
+}
+
+__device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, const Layout &L, int T, int sid,
+                          int nuniq, const double acc[4], int lane) {
+  unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
+  DeferHeader *h = reinterpret_cast<DeferHeader *>(base);
+  Plane *pl = reinterpret_cast<Plane *>(base + sizeof(DeferHeader));
+  double *vx = reinterpret_cast<double *>(pl + L.Pc);
+  double *vy = vx + L.Vc, *vz = vy + L.Vc, *vw = vz + L.Vc, *vd = vw + L.Vc;
+  unsigned *vt = reinterpret_cast<unsigned *>(vd + L.Vc);
+  int *tl = reinterpret_cast<int *>(vt + L.Vc);
+  if (lane == 0) {
+    h->sid = sid;
+    h->nuniq = nuniq;
+    h->nv = w.nv;
+    h->np = w.np;
+    for (int d = 0; d < 3; ++d) h->pt0[d] = w.pts[d];
+    for (int d = 0; d < 4; ++d) h->acc[d] = acc[d];
+  }
+  for (int i = lane; i < w.np; i += 32) pl[i] = w.plane[i];
+  for (int v = lane; v < w.nv; v += 32) {
+    vx[v] = w.cx[v];
+    vy[v] = w.cy[v];
+    vz[v] = w.cz[v];
+    vw[v] = w.cw[v];
+    vd[v] = w.d2[v];
+    vt[v] = w.tri[v];
+  }
+  for (int i = lane; i < nuniq; i += 32) tl[i] = w.tlist[i];
+  (void)T;
+}
+
 // Domain restriction of the clipped cell (ConvexCell.cl:918-1116): start
 // corner, boundary triangles, signed cone decomposition.  Adds the cell's
 // moments to acc; returns the status.
 template <int VS>
-__device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout &L, float4 s, double acc[4],
-                                  int lane, unsigned long long *ctr, double *tr, int trcap) {
+__device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout &L, float4 s, int sid_of_cell,
+                                  double acc[4], int lane, unsigned long long *ctr, double *tr, int trcap) {
   const DevGrid &g = a.grid;
   // bounding box -> voxel range (ConvexCell.cl:924-940)
   double lo[3] = {1000.0, 1000.0, 1000.0}, hi[3] = {0.0, 0.0, 0.0};
@@ -811,76 +939,23 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   if (nuniq == 0) return kSuccess;
   count(ctr, kCtrBoundaryCells, 1, lane);
   count(ctr, kCtrTriangles, nuniq, lane);
+  if (lane < 3) w.pts[lane] = pt0[lane];
+  __syncwarp();
+  const DeferQueue &dq = a.defer;
+  if (dq.slots && nuniq > dq.inline_max) {
+    // park the cell: its triangles become work items of k_cone
+    int slot = 0;
+    if (lane == 0) slot = atomicAdd(&dq.counters[0], 1);
+    slot = __shfl_sync(kFull, slot, 0);
+    if (slot < dq.capacity) {
+      park_cell(w, dq, slot, L, a.T, sid_of_cell, nuniq, acc, lane);
+      return kDeferred;
+    }
+  }
   const int bk_nv = w.nv, bk_np = w.np;
   backup<VS>(w, lane);
-  // signed cone decomposition over the boundary triangles
-  // (ConvexCell.cl:1082-1115)
-  if (lane < 3) w.pts[lane] = pt0[lane];
-  for (int ti = 0; ti < nuniq; ++ti) {
-    const int tri = w.tlist[ti];
-    bool go_out = false;
-    if (lane == 0) {
-      // triangle in the local frame, oriented to go out from pt0
-      const int i1 = __ldg(&g.tris[3 * tri]), i2 = __ldg(&g.tris[3 * tri + 1]), i3 = __ldg(&g.tris[3 * tri + 2]);
-      const float4 q1 = __ldg(&g.points[i1]), q2 = __ldg(&g.points[i2]), q3 = __ldg(&g.points[i3]);
-      const double P1[3] = {double(q1.x) - s.x, double(q1.y) - s.y, double(q1.z) - s.z};
-      const double P2[3] = {double(q2.x) - s.x, double(q2.y) - s.y, double(q2.z) - s.z};
-      const double P3[3] = {double(q3.x) - s.x, double(q3.y) - s.y, double(q3.z) - s.z};
-      const double ax = P1[0] - pt0[0], ay = P1[1] - pt0[1], az = P1[2] - pt0[2];
-      const double bx = P2[0] - pt0[0], by = P2[1] - pt0[1], bz = P2[2] - pt0[2];
-      const double cx = P3[0] - pt0[0], cy = P3[1] - pt0[1], cz = P3[2] - pt0[2];
-      const double det = ax * (by * cz - bz * cy) - bx * (ay * cz - az * cy) + cx * (ay * bz - az * by);
-      go_out = det > 0;
-      trace_rec(tr, trcap, lane, 6, tri, det, go_out, 0);
-      for (int d = 0; d < 3; ++d) {
-        w.pts[3 + d] = P1[d];
-        w.pts[6 + d] = go_out ? P2[d] : P3[d];
-        w.pts[9 + d] = go_out ? P3[d] : P2[d];
-      }
-    }
-    go_out = __shfl_sync(kFull, go_out, 0);
-    __syncwarp();
-    // the cone beyond triangle (P1, P2, P3) seen from pt0
-    // (CCClipTetFromPointsInfinite, ConvexCell.cl:565-575): faces
-    // (pt0, P1, P2), (pt0, P3, P1), (pt0, P2, P3), (P2, P3, P1)
-    if (w.np >= a.P) return kPlaneOverflow;
-    const double *q0 = w.pts, *q1 = w.pts + 3, *q2 = w.pts + 6, *q3 = w.pts + 9;
-    auto cone = [&](int f4) {
-      return f4 == 0 ? plane_from_points(q0, q1, q2)
-                     : f4 == 1 ? plane_from_points(q0, q3, q1)
-                               : f4 == 2 ? plane_from_points(q0, q2, q3) : plane_from_points(q2, q3, q1);
-    };
-    // quick classification: a plane that cuts every vertex empties the
-    // piece; no plane cutting any vertex means the cell lies in the cone
-    bool empty = false, any_cut = false;
-#pragma unroll 1
-    for (int f4 = 0; f4 < 4 && !empty; ++f4) {
-      unsigned rm[VS];
-      const int nr = cut_masks<VS>(w, cone(f4), rm, lane);
-      empty |= nr == w.nv;
-      any_cut |= nr > 0;
-    }
-    if (empty) continue;
-    if (any_cut) {
-      int cstat = kSuccess;
-#pragma unroll 1
-      for (int f4 = 0; f4 < 4 && cstat == kSuccess; ++f4) {
-        if (w.np >= a.P) {
-          cstat = kPlaneOverflow;
-          break;
-        }
-        clip<VS>(w, cone(f4), a.V, cstat, lane, ctr, tr, trcap);
-      }
-      if (cstat == kEmptyCell) {
-        restore<VS>(w, bk_nv, bk_np, lane);
-        continue;
-      }
-      if (cstat != kSuccess) return cstat;
-    }
-    integrate<VS>(w, go_out ? 1.0 : -1.0, acc, lane, ctr, tr, trcap);
-    if (any_cut) restore<VS>(w, bk_nv, bk_np, lane);
-  }
-  return kSuccess;
+  int fail_at = 0;
+  return cone_triangles<VS>(w, a, s, w.tlist, 0, nuniq, bk_nv, bk_np, acc, fail_at, lane, ctr, tr, trcap);
 }
 
 template <int VS, bool GRID>
@@ -967,10 +1042,11 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   if (outside) count(ctr, kCtrOutside, 1, lane);
   if (status == kSuccess && !outside) {
     if (GRID)
-      status = restrict_to_domain<VS>(w, a, L, s, acc, lane, ctr, tr, trcap);
+      status = restrict_to_domain<VS>(w, a, L, s, sid, acc, lane, ctr, tr, trcap);
     else
       integrate<VS>(w, 1.0, acc, lane, ctr, tr, trcap);
   }
+  if (status == kDeferred) return;  // k_cone_finish writes it
   if (lane == 0) {
     a.status[sid] = status;
     // local moments -> global: sum w*(x_local + s) = m_local + m * s
@@ -982,8 +1058,95 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   }
 }
 
+// Triangles of the parked boundary cells, CH at a time: every warp takes
+// work items (cell, chunk) from a counter, loads the cell into its shared
+// memory and runs the chunk's cones.  Partial moments and the first failure
+// go to per-item slots; k_cone_finish reduces them in order.
 template <int VS>
-cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st) {
+__global__ void __launch_bounds__(128, 5) k_cone(CellLaunch a, Layout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  WarpCell w = bind(smem + size_t(wib) * L.total, L);
+  const DeferQueue &dq = a.defer;
+  const int parked = min(*(volatile int *)&dq.counters[0], dq.capacity);
+  const int items = parked * dq.max_chunks;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(&dq.counters[1], 1);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= items) break;
+    const int slot = item / dq.max_chunks, chunk = item % dq.max_chunks;
+    const unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
+    const DeferHeader *h = reinterpret_cast<const DeferHeader *>(base);
+    const int nuniq = h->nuniq;
+    const int t0 = chunk * dq.chunk;
+    if (t0 >= nuniq) continue;
+    const int t1 = min(t0 + dq.chunk, nuniq);
+    const int nv = h->nv, np = h->np, sid = h->sid;
+    const Plane *pl = reinterpret_cast<const Plane *>(base + sizeof(DeferHeader));
+    const double *vx = reinterpret_cast<const double *>(pl + L.Pc);
+    const double *vy = vx + L.Vc, *vz = vy + L.Vc, *vw = vz + L.Vc, *vd = vw + L.Vc;
+    const unsigned *vt = reinterpret_cast<const unsigned *>(vd + L.Vc);
+    const int *tl = reinterpret_cast<const int *>(vt + L.Vc);
+    for (int i = lane; i < np; i += 32) w.plane[i] = pl[i];
+    for (int v = lane; v < nv; v += 32) {
+      w.cx[v] = w.bcx[v] = vx[v];
+      w.cy[v] = w.bcy[v] = vy[v];
+      w.cz[v] = w.bcz[v] = vz[v];
+      w.cw[v] = w.bcw[v] = vw[v];
+      w.d2[v] = w.bd2[v] = vd[v];
+      w.tri[v] = w.btri[v] = vt[v];
+    }
+    if (lane < 3) w.pts[lane] = h->pt0[lane];
+    __syncwarp();
+    w.nv = nv;
+    w.np = np;
+    const float4 s = a.stored[sid];
+    double acc[4] = {0, 0, 0, 0};
+    int fail_at = 0;
+    const int st = cone_triangles<VS>(w, a, s, tl, t0, t1, nv, np, acc, fail_at, lane, a.counters, nullptr, 0);
+    if (lane == 0) {
+      double *part = dq.part + size_t(item) * 4;
+      for (int d = 0; d < 4; ++d) part[d] = acc[d];
+      dq.fail[item] = st == kSuccess ? 0x7fffffff : ((fail_at << 4) | st);
+    }
+    __syncwarp();
+  }
+}
+
+// Per parked cell: its in-domain part plus the chunk partials in order; the
+// first failing chunk decides the status (the reference stops at the first
+// failing triangle, ConvexCell.cl:1104-1107).
+__global__ void k_cone_finish(CellLaunch a) {
+  const DeferQueue &dq = a.defer;
+  const int parked = min(dq.counters[0], dq.capacity);
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= parked) return;
+  const DeferHeader *h = reinterpret_cast<const DeferHeader *>(dq.slots + size_t(slot) * dq.slot_bytes);
+  const int sid = h->sid, nch = (h->nuniq + dq.chunk - 1) / dq.chunk;
+  double acc[4] = {h->acc[0], h->acc[1], h->acc[2], h->acc[3]};
+  int status = kSuccess;
+  for (int c = 0; c < nch; ++c) {
+    const int item = slot * dq.max_chunks + c;
+    const int f = dq.fail[item];
+    if (f != 0x7fffffff) {
+      status = f & 15;
+      break;
+    }
+    const double *part = dq.part + size_t(item) * 4;
+    for (int d = 0; d < 4; ++d) acc[d] += part[d];
+  }
+  const float4 s = a.stored[sid];
+  a.status[sid] = status;
+  const double m = acc[3];
+  a.out[sid] = status == kSuccess
+                   ? make_double4(acc[0] + m * double(s.x), acc[1] + m * double(s.y), acc[2] + m * double(s.z), m)
+                   : make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+template <int VS>
+cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int sm_count, int *launches) {
   const int warps_per_block = 4;
   const size_t smem = size_t(L.total) * warps_per_block;
   const int blocks = (a.num + warps_per_block - 1) / warps_per_block;
@@ -992,10 +1155,19 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st) {
     e = cudaFuncSetAttribute(k_cell<VS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     k_cell<VS, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    if (launches) ++*launches;
+    if (a.defer.slots) {
+      e = cudaFuncSetAttribute(k_cone<VS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      if (e != cudaSuccess) return e;
+      k_cone<VS><<<sm_count * 5, warps_per_block * 32, smem, st>>>(a, L);
+      k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a);
+      if (launches) *launches += 2;
+    }
   } else {
     e = cudaFuncSetAttribute(k_cell<VS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     k_cell<VS, false><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    if (launches) ++*launches;
   }
   return cudaGetLastError();
 }
@@ -1004,16 +1176,19 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st) {
 
 size_t cell_warp_smem(int P, int V, int T, bool grid) { return make_layout(P, V, T, grid).total; }
 
-cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st) {
+size_t defer_slot_bytes(int P, int V, int T) { return slot_bytes_for(make_layout(P, V, T, true), T); }
+
+cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count, int *launches) {
   if (a.num <= 0) return cudaSuccess;
   if (a.P > kMaxP || a.V > kMaxV || a.T > kMaxT || a.P < 7 || a.V < 8) return cudaErrorInvalidValue;
   const Layout L = make_layout(a.P, a.V, a.T, a.grid.size > 0);
+  if (a.defer.slots && a.defer.slot_bytes < slot_bytes_for(L, a.T)) return cudaErrorInvalidValue;
   const int vs = L.Vc / 32;
-  if (vs <= 2) return launch_vs<2>(a, L, st);
-  if (vs <= 3) return launch_vs<3>(a, L, st);
-  if (vs <= 4) return launch_vs<4>(a, L, st);
-  if (vs <= 6) return launch_vs<6>(a, L, st);
-  return launch_vs<8>(a, L, st);
+  if (vs <= 2) return launch_vs<2>(a, L, st, sm_count, launches);
+  if (vs <= 3) return launch_vs<3>(a, L, st, sm_count, launches);
+  if (vs <= 4) return launch_vs<4>(a, L, st, sm_count, launches);
+  if (vs <= 6) return launch_vs<6>(a, L, st, sm_count, launches);
+  return launch_vs<8>(a, L, st, sm_count, launches);
 }
 
 }  // namespace rpd

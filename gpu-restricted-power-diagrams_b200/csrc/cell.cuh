@@ -36,6 +36,20 @@ enum CellCounter {
   kCtrNum
 };
 
+// Boundary cells with many triangles park their clipped cell here; a second
+// kernel spreads their triangles over all warps in chunks.
+struct DeferQueue {
+  unsigned char *slots = nullptr;  // capacity slots of slot_bytes
+  int capacity = 0;
+  size_t slot_bytes = 0;
+  int *counters = nullptr;         // [0] cells parked, [1] next work item (zeroed before a pass)
+  double *part = nullptr;          // capacity * max_chunks * 4 partial moments
+  int *fail = nullptr;             // capacity * max_chunks: (triangle << 4) | status, or INT_MAX
+  int max_chunks = 0;              // ceil(T / chunk)
+  int chunk = 16;                  // triangles per work item
+  int inline_max = 16;             // cells with at most this many triangles stay inline
+};
+
 struct CellLaunch {
   const float4 *stored = nullptr;  // n seeds in stored order (reference frame)
   int n = 0;
@@ -57,6 +71,7 @@ struct CellLaunch {
   int trace_seed = -1;
   double *trace = nullptr;
   int trace_cap = 0;  // records
+  DeferQueue defer;   // slots == null: every boundary cell inline
 };
 constexpr int kTraceRecord = 12;
 
@@ -68,6 +83,10 @@ constexpr int kMaxT = 4096;
 
 // Shared memory bytes one warp needs for these caps.
 size_t cell_warp_smem(int P, int V, int T, bool grid);
-cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st);
+// Bytes of one parked boundary cell for these caps.
+size_t defer_slot_bytes(int P, int V, int T);
+// k_cell over the rows; with a domain and a defer queue, also the chunked
+// boundary-triangle kernel and the per-cell reduction (3 launches).
+cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count = 148, int *launches = nullptr);
 
 }  // namespace rpd

@@ -166,7 +166,29 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.status = s->status.as<int>();
   a.out = s->out.as<double4>();
   a.counters = ctr;
-  if ((e = cell_launch(a, st)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+  if (s->grid.size > 0 && s->use_defer) {
+    // boundary cells with many triangles are parked and their triangles
+    // spread over all warps; cells past the capacity stay inline
+    DeferQueue &dq = a.defer;
+    dq.capacity = std::min(num, std::max(32768, num / 8));
+    dq.slot_bytes = defer_slot_bytes(P, V, T);
+    dq.chunk = 16;
+    dq.inline_max = 16;
+    dq.max_chunks = std::max(1, (T + dq.chunk - 1) / dq.chunk);
+    const size_t items = size_t(dq.capacity) * dq.max_chunks;
+    if ((e = s->defer_slots.ensure(dq.slot_bytes * dq.capacity)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
+    if ((e = s->defer_part.ensure(sizeof(double) * 4 * items)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
+    if ((e = s->defer_fail.ensure(sizeof(int) * items)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
+    if ((e = s->defer_ctr.ensure(sizeof(int) * 2)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
+    cudaMemsetAsync(s->defer_ctr.ptr, 0, sizeof(int) * 2, st);
+    dq.slots = s->defer_slots.as<unsigned char>();
+    dq.part = s->defer_part.as<double>();
+    dq.fail = s->defer_fail.as<int>();
+    dq.counters = s->defer_ctr.as<int>();
+  }
+  int launches = 0;
+  if ((e = cell_launch(a, st, ctx->sm_count, &launches)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+  S.kernel_launches += launches - 1;
   cudaEventRecord(ev[2], st);
   if ((e = cudaEventSynchronize(ev[2])) != cudaSuccess) return map_cuda(ctx, e, "pass");
   if (pi < 8) {
@@ -467,6 +489,7 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   // (voronoi.cpp:1275-1310)
   const int T0 = p.T;
   const bool early = !(p.flags & RPD_FLAG_NO_EARLY_OUT);
+  s->use_defer = !(p.flags & RPD_FLAG_NO_DEFER);
   int rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
   if (rc != RPD_OK) return rc;
   if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {

@@ -74,6 +74,8 @@ struct rpd_solver {
   rpd::DevBuf fail_ws;         // flags + scans
   rpd::DevBuf hist;            // int[16]: status histogram + counts
   rpd::DevBuf gather;          // user-order staging for outputs
+  rpd::DevBuf defer_slots, defer_part, defer_fail, defer_ctr;  // parked boundary cells
   bool have_results = false;
+  bool use_defer = true;       // park heavy boundary cells for the chunked kernel
   rpd_stats stats{};
 };

@@ -98,6 +98,7 @@ def _ptr(a):
 FLAG_FIRST_PASS_ONLY = 1
 FLAG_COUNTERS = 2
 FLAG_NO_EARLY_OUT = 4
+FLAG_NO_DEFER = 8
 COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
                  "exports", "export_vertices", "outside_early"]
 

@@ -137,6 +137,8 @@ rpd_grid *rpd_grid_make_cube(int size, int *err);
 #define RPD_FLAG_COUNTERS 2u        /* collect work counters (rpd_stats.counters) */
 #define RPD_FLAG_NO_EARLY_OUT 4u    /* clip every cell to the end even when it is
                                        provably outside the domain (same results) */
+#define RPD_FLAG_NO_DEFER 8u        /* run every boundary cell's triangles in the
+                                       cell's own warp (same results, slower) */
 
 /* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
 typedef struct rpd_params {

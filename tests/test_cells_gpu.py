@@ -97,3 +97,27 @@ def test_wall_seeds(rpd):
     assert_parity(met)
     walls = x[:, 3] <= rpd.NO_CELL_LIMITS
     assert np.array_equal(got[walls], x[walls].astype(np.float64))
+
+
+def test_early_out_and_parking_do_not_change_results(rpd):
+    g = rpd.Grid.blob(60, 5, 2)
+    x = jittered(40, seed=6, weights=True)
+    s = rpd.Solver().set_points(x).set_grid(g)
+    res = {}
+    for name, flags in [("default", 0), ("no_early", rpd.FLAG_NO_EARLY_OUT), ("no_defer", rpd.FLAG_NO_DEFER),
+                        ("plain", rpd.FLAG_NO_EARLY_OUT | rpd.FLAG_NO_DEFER)]:
+        s.launch(K=50, P=30, V=40, T=60, flags=flags)
+        res[name] = (s.moments(), s.status())
+    m0, s0 = res["plain"]
+    # parking sums a cell's cone pieces per chunk, so small restricted
+    # pieces that cancel against whole-cell volumes differ in rounding: the
+    # scale of every cell is the typical cell volume (moments x1000)
+    typ = np.median(np.abs(m0[:, 3][np.abs(m0[:, 3]) > 0]))
+    scale = np.maximum(np.abs(m0[:, 3]), typ)[:, None] * np.array([1000.0, 1000.0, 1000.0, 1.0])
+    for name, (m, st) in res.items():
+        assert np.array_equal(st, s0), name
+        err = np.abs(m - m0) / scale
+        print(name, "max rel", err.max())
+        assert err.max() < 1e-12, name
+    early = res["no_defer"][0]
+    assert np.array_equal(early, m0), "the early exit must not change any bit"
