@@ -748,7 +748,10 @@ __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const 
       empty |= nr == w.nv;
       any_cut |= nr > 0;
     }
-    if (empty) continue;
+    if (empty) {
+      count(ctr, kCtrConeEmpty, 1, lane);
+      continue;
+    }
     if (any_cut) {
       int cstat = kSuccess;
 #pragma unroll 1
@@ -772,6 +775,96 @@ __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const 
     if (any_cut) restore<VS>(w, bk_nv, bk_np, lane);
   }
   return kSuccess;
+}
+
+// Apex inside the cell.  The signed cone decomposition holds for any apex on
+// a known side of the surface.  From a grid corner with flag 0 or 2 that lies
+// inside the convex cell, the segment to any point of the cell stays in the
+// cell, so a triangle that misses the cell crosses none of them and its cone
+// holds no part of the cell.  Picks the corner of the voxel range deepest in
+// the cell (lowest corner id on ties); returns its flag, or -1 when no corner
+// lies at least kApexDepth voxels inside.
+constexpr double kApexDepth = 1e-3;   // voxels
+constexpr double kSeparation = 1e-9;  // reference-frame units
+
+__device__ int inner_apex(const WarpCell &w, const DevGrid &g, float4 s, const int vmin[3], const int vmax[3],
+                          double apex[3], int lane) {
+  const int S = g.size;
+  int lo[3], n[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = vmin[d];
+    n[d] = min(vmax[d] + 1, S - 1) - vmin[d] + 1;
+  }
+  const int ncorner = (n[0] > 0 && n[1] > 0 && n[2] > 0) ? n[0] * n[1] * n[2] : 0;
+  const double h = double(g.voxel);
+  double best = kApexDepth * h;
+  int best_id = 0x7fffffff;
+  for (int q = lane; q < ncorner; q += 32) {
+    const int x = lo[0] + q % n[0], y = lo[1] + (q / n[0]) % n[1], z = lo[2] + q / (n[0] * n[1]);
+    const int vid = x + y * S + z * S * S;
+    if (g.flags[vid] == 1) continue;
+    const double cx = x * h - s.x, cy = y * h - s.y, cz = z * h - s.z;
+    double depth = 1e300;
+    for (int i = 0; i < w.np && depth > best; ++i) {
+      const Plane p = w.plane[i];
+      depth = fmin(depth, fma(p.x, cx, fma(p.y, cy, fma(p.z, cz, p.w))));
+    }
+    if (depth > best || (depth == best && vid < best_id)) {
+      best = depth;
+      best_id = vid;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(kFull, best, o);
+    const int oi = __shfl_xor_sync(kFull, best_id, o);
+    if (ob > best || (ob == best && oi < best_id)) {
+      best = ob;
+      best_id = oi;
+    }
+  }
+  if (best_id == 0x7fffffff) return -1;
+  const int x = best_id % S, y = (best_id / S) % S, z = best_id / (S * S);
+  apex[0] = x * h - s.x;
+  apex[1] = y * h - s.y;
+  apex[2] = z * h - s.z;
+  return g.flags[best_id];
+}
+
+// Drops from tids[0, n) the triangles that a plane of the cell separates
+// from it (all three corners more than kSeparation outside), keeping the
+// order; returns the number kept.
+__device__ int drop_separated(const WarpCell &w, const DevGrid &g, float4 s, int *tids, int n, int lane) {
+  int kept = 0;
+  for (int i0 = 0; i0 < n; i0 += 32) {
+    const int i = i0 + lane;
+    int tri = 0;
+    bool keep = false;
+    if (i < n) {
+      tri = tids[i];
+      const float4 q1 = __ldg(&g.points[__ldg(&g.tris[3 * tri])]);
+      const float4 q2 = __ldg(&g.points[__ldg(&g.tris[3 * tri + 1])]);
+      const float4 q3 = __ldg(&g.points[__ldg(&g.tris[3 * tri + 2])]);
+      const double x1 = double(q1.x) - s.x, y1 = double(q1.y) - s.y, z1 = double(q1.z) - s.z;
+      const double x2 = double(q2.x) - s.x, y2 = double(q2.y) - s.y, z2 = double(q2.z) - s.z;
+      const double x3 = double(q3.x) - s.x, y3 = double(q3.y) - s.y, z3 = double(q3.z) - s.z;
+      keep = true;
+      for (int k = 0; k < w.np && keep; ++k) {
+        const Plane p = w.plane[k];
+        const double d1 = fma(p.x, x1, fma(p.y, y1, fma(p.z, z1, p.w)));
+        const double d2 = fma(p.x, x2, fma(p.y, y2, fma(p.z, z2, p.w)));
+        const double d3 = fma(p.x, x3, fma(p.y, y3, fma(p.z, z3, p.w)));
+        keep = fmax(d1, fmax(d2, d3)) >= -kSeparation;
+      }
+    }
+    const unsigned km = __ballot_sync(kFull, keep);
+    __syncwarp();
+    if (keep) tids[kept + __popc(km & lanemask_lt(lane))] = tri;
+    __syncwarp();
+    kept += __popc(km);
+  }
+  return kept;
 }
 
 // Parked boundary cell: header, planes, vertices, triangle ids.
@@ -820,7 +913,7 @@ __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, con
 // Domain restriction of the clipped cell (ConvexCell.cl:918-1116): start
 // corner, boundary triangles, signed cone decomposition.  Adds the cell's
 // moments to acc; returns the status.
-template <int VS>
+template <int VS, bool INL>
 __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout &L, float4 s, int sid_of_cell,
                                   double acc[4], int lane, unsigned long long *ctr, double *tr, int trcap) {
   const DevGrid &g = a.grid;
@@ -934,15 +1027,28 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     pt0[1] = y * double(g.voxel) - s.y;
     pt0[2] = z * double(g.voxel) - s.z;
   }
+  if (nuniq > 0) {
+    count(ctr, kCtrBoundaryCells, 1, lane);
+    count(ctr, kCtrTriangles, nuniq, lane);
+  }
+  if (nuniq > 0 && a.inner_apex) {
+    double ap[3];
+    const int f = inner_apex(w, g, s, vmin, vmax, ap, lane);
+    if (f >= 0) {
+      in_domain = f;
+      for (int d = 0; d < 3; ++d) pt0[d] = ap[d];
+      const int kept = drop_separated(w, g, s, w.tlist, nuniq, lane);
+      count(ctr, kCtrConesSkipped, nuniq - kept, lane);
+      nuniq = kept;
+    }
+  }
   trace_rec(tr, trcap, lane, 5, pt0[0], pt0[1], pt0[2], in_domain, nuniq);
   if (in_domain == 2) integrate<VS>(w, 1.0, acc, lane, ctr, tr, trcap);
   if (nuniq == 0) return kSuccess;
-  count(ctr, kCtrBoundaryCells, 1, lane);
-  count(ctr, kCtrTriangles, nuniq, lane);
   if (lane < 3) w.pts[lane] = pt0[lane];
   __syncwarp();
   const DeferQueue &dq = a.defer;
-  if (dq.slots && nuniq > dq.inline_max) {
+  if (dq.slots && (!INL || nuniq > dq.inline_max)) {
     // park the cell: its triangles become work items of k_cone
     int slot = 0;
     if (lane == 0) slot = atomicAdd(&dq.counters[0], 1);
@@ -952,13 +1058,17 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
       return kDeferred;
     }
   }
-  const int bk_nv = w.nv, bk_np = w.np;
-  backup<VS>(w, lane);
-  int fail_at = 0;
-  return cone_triangles<VS>(w, a, s, w.tlist, 0, nuniq, bk_nv, bk_np, acc, fail_at, lane, ctr, tr, trcap);
+  if constexpr (!INL) {
+    return kParkOverflow;  // re-run by the inline variant
+  } else {
+    const int bk_nv = w.nv, bk_np = w.np;
+    backup<VS>(w, lane);
+    int fail_at = 0;
+    return cone_triangles<VS>(w, a, s, w.tlist, 0, nuniq, bk_nv, bk_np, acc, fail_at, lane, ctr, tr, trcap);
+  }
 }
 
-template <int VS, bool GRID>
+template <int VS, bool GRID, bool INL>
 __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
@@ -968,6 +1078,7 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   WarpCell w = bind(smem + size_t(wib) * L.total, L);
   unsigned long long *ctr = a.counters;
   const int sid = a.ids ? a.ids[row] : row;
+  if (a.only_status >= 0 && a.status[sid] != a.only_status) return;
   const float4 s = a.stored[sid];
   double *tr = (a.trace && sid == a.trace_seed) ? a.trace : nullptr;
   const int trcap = a.trace_cap;
@@ -1042,11 +1153,15 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   if (outside) count(ctr, kCtrOutside, 1, lane);
   if (status == kSuccess && !outside) {
     if (GRID)
-      status = restrict_to_domain<VS>(w, a, L, s, sid, acc, lane, ctr, tr, trcap);
+      status = restrict_to_domain<VS, INL>(w, a, L, s, sid, acc, lane, ctr, tr, trcap);
     else
       integrate<VS>(w, 1.0, acc, lane, ctr, tr, trcap);
   }
   if (status == kDeferred) return;  // k_cone_finish writes it
+  if (status == kParkOverflow) {
+    if (lane == 0) a.status[sid] = kParkOverflow;
+    return;
+  }
   if (lane == 0) {
     a.status[sid] = status;
     // local moments -> global: sum w*(x_local + s) = m_local + m * s
@@ -1151,22 +1266,25 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
   const size_t smem = size_t(L.total) * warps_per_block;
   const int blocks = (a.num + warps_per_block - 1) / warps_per_block;
   cudaError_t e;
-  if (a.grid.size > 0) {
-    e = cudaFuncSetAttribute(k_cell<VS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (a.grid.size > 0 && a.defer.slots) {
+    // every boundary cell parks; the chunked kernel does the triangles
+    e = cudaFuncSetAttribute(k_cell<VS, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    k_cell<VS, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    k_cell<VS, true, false><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    e = cudaFuncSetAttribute(k_cone<VS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    k_cone<VS><<<sm_count * 5, warps_per_block * 32, smem, st>>>(a, L);
+    k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a);
+    if (launches) *launches += 3;
+  } else if (a.grid.size > 0) {
+    e = cudaFuncSetAttribute(k_cell<VS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    k_cell<VS, true, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (launches) ++*launches;
-    if (a.defer.slots) {
-      e = cudaFuncSetAttribute(k_cone<VS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-      if (e != cudaSuccess) return e;
-      k_cone<VS><<<sm_count * 5, warps_per_block * 32, smem, st>>>(a, L);
-      k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a);
-      if (launches) *launches += 2;
-    }
   } else {
-    e = cudaFuncSetAttribute(k_cell<VS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    e = cudaFuncSetAttribute(k_cell<VS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    k_cell<VS, false><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    k_cell<VS, false, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (launches) ++*launches;
   }
   return cudaGetLastError();

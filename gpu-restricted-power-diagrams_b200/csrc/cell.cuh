@@ -33,6 +33,8 @@ enum CellCounter {
   kCtrExports,            // integrations (cell or cone pieces)
   kCtrExportVertices,     // vertices integrated
   kCtrOutside,            // cells proven outside the domain before the end of clipping
+  kCtrConeEmpty,          // boundary triangles whose cone misses the cell
+  kCtrConesSkipped,       // boundary triangles dropped: they miss the cell (apex inside it)
   kCtrNum
 };
 
@@ -61,6 +63,7 @@ struct CellLaunch {
   float cube_eps = 0.f;            // box [-eps, 1000+eps]^3
   int out_domain = 0;              // GRID_OUT_DOMAIN fallback for the start corner
   int early_out = 1;               // stop clipping cells proven outside the domain (needs grid.sat)
+  int inner_apex = 1;              // cone apex at a grid corner inside the cell when there is one
   DevGrid grid;                    // grid.size == 0: no domain
   int *status = nullptr;           // n, stored order
   double4 *out = nullptr;          // n, stored order: (m*x, m*y, m*z, m)
@@ -72,7 +75,9 @@ struct CellLaunch {
   double *trace = nullptr;
   int trace_cap = 0;  // records
   DeferQueue defer;   // slots == null: every boundary cell inline
+  int only_status = -1;  // >= 0: process only the rows whose status equals it
 };
+constexpr int kParkOverflow = 101;  // internal status: the queue was full
 constexpr int kTraceRecord = 12;
 
 // Largest caps of one build: P <= 255 (uchar plane ids in the reference,

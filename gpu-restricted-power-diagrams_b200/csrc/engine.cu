@@ -162,6 +162,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.cube_eps = eps;
   a.out_domain = out_domain;
   a.early_out = early_out ? 1 : 0;
+  a.inner_apex = s->inner_apex ? 1 : 0;
   a.grid = s->grid;
   a.status = s->status.as<int>();
   a.out = s->out.as<double4>();
@@ -188,6 +189,18 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   }
   int launches = 0;
   if ((e = cell_launch(a, st, ctx->sm_count, &launches)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+  if (a.defer.slots) {
+    // cells that found the queue full run again with their cones inline
+    int parked = 0;
+    cudaMemcpyAsync(&parked, a.defer.counters, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+    if (parked > a.defer.capacity) {
+      CellLaunch b = a;
+      b.defer = DeferQueue();
+      b.only_status = kParkOverflow;
+      if ((e = cell_launch(b, st, ctx->sm_count, &launches)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+    }
+  }
   S.kernel_launches += launches - 1;
   cudaEventRecord(ev[2], st);
   if ((e = cudaEventSynchronize(ev[2])) != cudaSuccess) return map_cuda(ctx, e, "pass");
@@ -490,6 +503,7 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   const int T0 = p.T;
   const bool early = !(p.flags & RPD_FLAG_NO_EARLY_OUT);
   s->use_defer = !(p.flags & RPD_FLAG_NO_DEFER);
+  s->inner_apex = !(p.flags & RPD_FLAG_REFERENCE_APEX);
   int rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
   if (rc != RPD_OK) return rc;
   if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {
@@ -609,6 +623,7 @@ int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *pp, doub
   a.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
   a.out_domain = p.out_domain > 0 ? 1 : 0;
   a.early_out = (p.flags & RPD_FLAG_NO_EARLY_OUT) ? 0 : 1;
+  a.inner_apex = (p.flags & RPD_FLAG_REFERENCE_APEX) ? 0 : 1;
   a.grid = s->grid;
   a.status = s->status.as<int>();
   a.out = s->out.as<double4>();

@@ -77,5 +77,6 @@ struct rpd_solver {
   rpd::DevBuf defer_slots, defer_part, defer_fail, defer_ctr;  // parked boundary cells
   bool have_results = false;
   bool use_defer = true;       // park heavy boundary cells for the chunked kernel
+  bool inner_apex = true;      // cone apex at a grid corner inside the cell
   rpd_stats stats{};
 };

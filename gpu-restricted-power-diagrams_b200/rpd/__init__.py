@@ -99,8 +99,9 @@ FLAG_FIRST_PASS_ONLY = 1
 FLAG_COUNTERS = 2
 FLAG_NO_EARLY_OUT = 4
 FLAG_NO_DEFER = 8
+FLAG_REFERENCE_APEX = 16
 COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
-                 "exports", "export_vertices", "outside_early"]
+                 "exports", "export_vertices", "outside_early", "cone_empty", "cones_skipped"]
 
 
 class Params(C.Structure):
@@ -122,7 +123,7 @@ class Stats(C.Structure):
     _fields_ = [("npasses", C.c_int), ("pass_cells", C.c_int * 8), ("pass_K", C.c_int * 8),
                 ("pass_P", C.c_int * 8), ("pass_V", C.c_int * 8), ("pass_T", C.c_int * 8),
                 ("pass_knn_ms", C.c_float * 8), ("pass_cell_ms", C.c_float * 8), ("status_hist", C.c_int * 11),
-                ("counters", C.c_ulonglong * 9), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
+                ("counters", C.c_ulonglong * 11), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
                 ("kernel_launches", C.c_int)]
 
     def as_dict(self):

@@ -139,6 +139,9 @@ rpd_grid *rpd_grid_make_cube(int size, int *err);
                                        provably outside the domain (same results) */
 #define RPD_FLAG_NO_DEFER 8u        /* run every boundary cell's triangles in the
                                        cell's own warp (same results, slower) */
+#define RPD_FLAG_REFERENCE_APEX 16u /* cone apex at the reference's start corner for
+                                       every cell, with all triangles of its voxels
+                                       (same results up to rounding, slower) */
 
 /* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
 typedef struct rpd_params {
@@ -167,6 +170,9 @@ enum {
   RPD_CTR_EXPORTS,
   RPD_CTR_EXPORT_VERTICES,
   RPD_CTR_OUTSIDE, /* cells proven outside the domain before the end of clipping */
+  RPD_CTR_CONE_EMPTY,   /* boundary triangles whose cone misses the cell */
+  RPD_CTR_CONES_SKIPPED, /* boundary triangles dropped because they miss the cell
+                            (cone apex at a grid corner inside the cell) */
   RPD_CTR_NUM
 };
 

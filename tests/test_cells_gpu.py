@@ -104,14 +104,24 @@ def test_early_out_and_parking_do_not_change_results(rpd):
     x = jittered(40, seed=6, weights=True)
     s = rpd.Solver().set_points(x).set_grid(g)
     res = {}
+    ref = rpd.FLAG_REFERENCE_APEX
     for name, flags in [("default", 0), ("no_early", rpd.FLAG_NO_EARLY_OUT), ("no_defer", rpd.FLAG_NO_DEFER),
-                        ("plain", rpd.FLAG_NO_EARLY_OUT | rpd.FLAG_NO_DEFER)]:
+                        ("inline", rpd.FLAG_NO_EARLY_OUT | rpd.FLAG_NO_DEFER),
+                        ("ref_apex", ref), ("ref_apex_no_defer", ref | rpd.FLAG_NO_DEFER),
+                        ("plain", rpd.FLAG_NO_EARLY_OUT | rpd.FLAG_NO_DEFER | ref)]:
         s.launch(K=50, P=30, V=40, T=60, flags=flags)
         res[name] = (s.moments(), s.status())
+    s.launch(K=50, P=30, V=40, T=60, flags=ref | rpd.FLAG_COUNTERS)
+    assert s.stats()["counters"]["cones_skipped"] == 0
+    s.launch(K=50, P=30, V=40, T=60, flags=rpd.FLAG_COUNTERS)
+    ctr = s.stats()["counters"]
+    print("counters", ctr)
+    assert 0 < ctr["cones_skipped"] < ctr["triangles"]
     m0, s0 = res["plain"]
-    # parking sums a cell's cone pieces per chunk, so small restricted
-    # pieces that cancel against whole-cell volumes differ in rounding: the
-    # scale of every cell is the typical cell volume (moments x1000)
+    # parking sums a cell's cone pieces per chunk, and another apex gives
+    # other pieces, so small restricted pieces that cancel against whole-cell
+    # volumes differ in rounding: the scale of every cell is the typical cell
+    # volume (moments x1000)
     typ = np.median(np.abs(m0[:, 3][np.abs(m0[:, 3]) > 0]))
     scale = np.maximum(np.abs(m0[:, 3]), typ)[:, None] * np.array([1000.0, 1000.0, 1000.0, 1.0])
     for name, (m, st) in res.items():
@@ -119,5 +129,5 @@ def test_early_out_and_parking_do_not_change_results(rpd):
         err = np.abs(m - m0) / scale
         print(name, "max rel", err.max())
         assert err.max() < 1e-12, name
-    early = res["no_defer"][0]
-    assert np.array_equal(early, m0), "the early exit must not change any bit"
+    assert np.array_equal(res["no_defer"][0], res["inline"][0]), "the early exit must not change any bit"
+    assert np.array_equal(res["ref_apex_no_defer"][0], m0), "the early exit must not change any bit"
