@@ -663,31 +663,45 @@ __device__ void warp_sort_ints(int *a, int n, int lane) {
   }
 }
 
-// Whether every voxel that a ball of radius sqrt(r2) around the seed can
-// touch is plainly outside (flag 0 and no triangles).  The final cell lies in
-// that ball, so the reference's restriction would find the start corner
-// outside and no triangle: mass 0.  Ranges as ConvexCell.cl:937-940.
-__device__ __forceinline__ bool ball_outside(const DevGrid &g, float4 s, double r2, int lane) {
-  const double r = sqrt(r2);
-  int lo[3], hi[3];
+// Squared radius of a ball around the seed whose voxels are all plainly
+// outside (flag 0 and no triangles), or -1.  The final cell lies in any ball
+// around the seed that holds its current vertices, so once that ball fits,
+// the reference's restriction would find the start corner outside and no
+// triangle in the cell's voxel range (ConvexCell.cl:924-940): mass 0.  Lane k
+// counts the non-plain voxels of the cube of half-size k voxels around the
+// seed's voxel from the summed-volume table; below the first non-empty cube,
+// the ball may reach the cube's faces that are not on the grid's border.
+__device__ double plain_radius2(const DevGrid &g, float4 s, int lane) {
+  const int S = g.size, S1 = S + 1;
+  const double h = double(g.voxel);
   const double c[3] = {s.x, s.y, s.z};
+  int v[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) v[d] = min(S - 1, max(0, int(c[d] / h)));
+  int lo[3], hi[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    lo[d] = c[d] - r <= 0.0 ? 0 : min(g.size - 1, int((c[d] - r) / double(g.voxel)));
-    hi[d] = c[d] + r <= 0.0 ? 0 : min(g.size - 1, int((c[d] + r) / double(g.voxel)));
+    lo[d] = max(0, v[d] - lane);
+    hi[d] = min(S - 1, v[d] + lane) + 1;
   }
-  const int S1 = g.size + 1;
-  int v = 0;
-  if (lane < 8) {
-    const int x = (lane & 1) ? hi[0] + 1 : lo[0];
-    const int y = (lane & 2) ? hi[1] + 1 : lo[1];
-    const int z = (lane & 4) ? hi[2] + 1 : lo[2];
-    const int sign = ((lane & 1) ^ ((lane >> 1) & 1) ^ ((lane >> 2) & 1)) ? 1 : -1;
-    v = sign * __ldg(&g.sat[x + S1 * (y + S1 * z)]);
-  }
+  int cnt = 0;
 #pragma unroll
-  for (int o = 4; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return __shfl_sync(kFull, v, 0) == 0;
+  for (int q = 0; q < 8; ++q) {
+    const int x = (q & 1) ? hi[0] : lo[0], y = (q & 2) ? hi[1] : lo[1], z = (q & 4) ? hi[2] : lo[2];
+    const int sign = ((q & 1) ^ ((q >> 1) & 1) ^ ((q >> 2) & 1)) ? 1 : -1;
+    cnt -= sign * __ldg(&g.sat[x + S1 * (y + S1 * z)]);
+  }
+  const unsigned hit = __ballot_sync(kFull, cnt != 0);
+  const int k = hit ? __ffs(hit) - 1 : 32;  // cubes below k are plain
+  if (k == 0) return -1.0;
+  double r = 1e300;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (v[d] - (k - 1) > 0) r = fmin(r, c[d] - (v[d] - (k - 1)) * h);
+    if (v[d] + (k - 1) < S - 1) r = fmin(r, (v[d] + k) * h - c[d]);
+  }
+  r -= 1e-6 * h;
+  return r > 0.0 ? (r >= 1e150 ? 1e300 : r * r) : -1.0;
 }
 
 // Signed cone decomposition over boundary triangles tids[t0, t1)
@@ -695,10 +709,12 @@ __device__ __forceinline__ bool ball_outside(const DevGrid &g, float4 s, double 
 // from the start corner (w.pts[0..2]) clips the backed-up cell, the piece is
 // integrated with the triangle's sign, and the cell is restored.  Returns
 // the status; on failure fail_at is the failing triangle's position.
+// With the apex inside the cell (inner), a cone rarely misses the cell: the
+// quick classification is skipped and the triangle's plane clips first.
 template <int VS>
 __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const int *tids, int t0, int t1,
-                              int bk_nv, int bk_np, double acc[4], int &fail_at, int lane, unsigned long long *ctr,
-                              double *tr, int trcap) {
+                              int bk_nv, int bk_np, bool inner, double acc[4], int &fail_at, int lane,
+                              unsigned long long *ctr, double *tr, int trcap) {
   const DevGrid &g = a.grid;
   for (int ti = t0; ti < t1; ++ti) {
     const int tri = tids[ti];
@@ -740,9 +756,9 @@ __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const 
     };
     // quick classification: a plane that cuts every vertex empties the
     // piece; no plane cutting any vertex means the cell lies in the cone
-    bool empty = false, any_cut = false;
+    bool empty = false, any_cut = inner;
 #pragma unroll 1
-    for (int f4 = 0; f4 < 4 && !empty; ++f4) {
+    for (int f4 = 0; f4 < 4 && !empty && !inner; ++f4) {
       unsigned rm[VS];
       const int nr = cut_masks<VS>(w, cone(f4), rm, lane);
       empty |= nr == w.nv;
@@ -755,14 +771,15 @@ __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const 
     if (any_cut) {
       int cstat = kSuccess;
 #pragma unroll 1
-      for (int f4 = 0; f4 < 4 && cstat == kSuccess; ++f4) {
+      for (int k = 0; k < 4 && cstat == kSuccess; ++k) {
         if (w.np >= a.P) {
           cstat = kPlaneOverflow;
           break;
         }
-        clip<VS>(w, cone(f4), a.V, cstat, lane, ctr, tr, trcap);
+        clip<VS>(w, cone(inner ? (k + 3) & 3 : k), a.V, cstat, lane, ctr, tr, trcap);
       }
       if (cstat == kEmptyCell) {
+        if (inner) count(ctr, kCtrConeEmpty, 1, lane);
         restore<VS>(w, bk_nv, bk_np, lane);
         continue;
       }
@@ -872,7 +889,8 @@ struct DeferHeader {
   int sid, nuniq, nv, np;
   double pt0[3];
   double acc[4];
-  double pad[9];
+  int inner, pad_i;
+  double pad[8];
 };
 static_assert(sizeof(DeferHeader) == 144, "defer header size");
 
@@ -881,7 +899,7 @@ __host__ __device__ inline size_t slot_bytes_for(const Layout &L, int T) {
 }
 
 __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, const Layout &L, int T, int sid,
-                          int nuniq, const double acc[4], int lane) {
+                          int nuniq, bool inner, const double acc[4], int lane) {
   unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
   DeferHeader *h = reinterpret_cast<DeferHeader *>(base);
   Plane *pl = reinterpret_cast<Plane *>(base + sizeof(DeferHeader));
@@ -894,6 +912,7 @@ __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, con
     h->nuniq = nuniq;
     h->nv = w.nv;
     h->np = w.np;
+    h->inner = inner ? 1 : 0;
     for (int d = 0; d < 3; ++d) h->pt0[d] = w.pts[d];
     for (int d = 0; d < 4; ++d) h->acc[d] = acc[d];
   }
@@ -1031,10 +1050,12 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     count(ctr, kCtrBoundaryCells, 1, lane);
     count(ctr, kCtrTriangles, nuniq, lane);
   }
+  bool inner = false;
   if (nuniq > 0 && a.inner_apex) {
     double ap[3];
     const int f = inner_apex(w, g, s, vmin, vmax, ap, lane);
     if (f >= 0) {
+      inner = true;
       in_domain = f;
       for (int d = 0; d < 3; ++d) pt0[d] = ap[d];
       const int kept = drop_separated(w, g, s, w.tlist, nuniq, lane);
@@ -1054,7 +1075,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     if (lane == 0) slot = atomicAdd(&dq.counters[0], 1);
     slot = __shfl_sync(kFull, slot, 0);
     if (slot < dq.capacity) {
-      park_cell(w, dq, slot, L, a.T, sid_of_cell, nuniq, acc, lane);
+      park_cell(w, dq, slot, L, a.T, sid_of_cell, nuniq, inner, acc, lane);
       return kDeferred;
     }
   }
@@ -1064,7 +1085,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     const int bk_nv = w.nv, bk_np = w.np;
     backup<VS>(w, lane);
     int fail_at = 0;
-    return cone_triangles<VS>(w, a, s, w.tlist, 0, nuniq, bk_nv, bk_np, acc, fail_at, lane, ctr, tr, trcap);
+    return cone_triangles<VS>(w, a, s, w.tlist, 0, nuniq, bk_nv, bk_np, inner, acc, fail_at, lane, ctr, tr, trcap);
   }
 }
 
@@ -1099,6 +1120,7 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   const unsigned *nrow = a.knn + size_t(row) * a.K;
   bool reached = false, exhausted = false, outside = false;
   const bool early = GRID && a.early_out && a.grid.sat != nullptr;
+  const double plain2 = early ? plain_radius2(a.grid, s, lane) : -1.0;
   for (int i0 = 0; i0 < a.K && status == kSuccess && !reached && !exhausted && !outside; i0 += 32) {
     // every lane builds the bisector of one neighbour, in double
     const int i = i0 + lane;
@@ -1138,7 +1160,7 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
       if (r < 0) break;
       if (r > 0) {
         R2 = cell_radius2<VS>(w, lane);
-        if (early && ball_outside(a.grid, s, R2, lane)) {
+        if (R2 <= plain2) {
           outside = true;
           break;
         }
@@ -1220,7 +1242,8 @@ __global__ void __launch_bounds__(128, 5) k_cone(CellLaunch a, Layout L) {
     const float4 s = a.stored[sid];
     double acc[4] = {0, 0, 0, 0};
     int fail_at = 0;
-    const int st = cone_triangles<VS>(w, a, s, tl, t0, t1, nv, np, acc, fail_at, lane, a.counters, nullptr, 0);
+    const int st =
+        cone_triangles<VS>(w, a, s, tl, t0, t1, nv, np, h->inner != 0, acc, fail_at, lane, a.counters, nullptr, 0);
     if (lane == 0) {
       double *part = dq.part + size_t(item) * 4;
       for (int d = 0; d < 4; ++d) part[d] = acc[d];
