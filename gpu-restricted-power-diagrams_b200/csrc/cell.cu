@@ -301,91 +301,150 @@ __device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, u
   const int pid = w.np;
   const int mw = w.mw;
   if (lane == 0) w.plane[pid] = e;
-  // removed triples, in position order
+  const int nkeep = w.nv - nrem;
+  // The cavity boundary is the set of directed edges of removed triangles
+  // whose twin belongs to a kept triangle: the edges that occur once among
+  // the removed (or, reversed, among the kept) triangles.  When the smaller
+  // side has at most 10 triangles, its edges fit one per lane and a match on
+  // the undirected plane pair finds them; otherwise edge bitmasks do.
+  const bool fast = min(nrem, nkeep) <= 10;
+  const bool from_kept = fast && nkeep < nrem;
+  const int nside = from_kept ? nkeep : nrem;
+  // the side's triples, in position order
   {
     int base = 0;
 #pragma unroll
     for (int s = 0; s < VS; ++s) {
-      if ((rm[s] >> lane) & 1u) w.rem[base + __popc(rm[s] & lanemask_lt(lane))] = w.tri[s * 32 + lane];
-      base += __popc(rm[s]);
+      const int v = s * 32 + lane;
+      const unsigned valid = s * 32 >= w.nv ? 0u : (w.nv - s * 32 >= 32 ? kFull : (1u << (w.nv - s * 32)) - 1u);
+      const unsigned side = from_kept ? (~rm[s] & valid) : rm[s];
+      if ((side >> lane) & 1u) w.rem[base + __popc(side & lanemask_lt(lane))] = w.tri[v];
+      base += __popc(side);
     }
   }
   __syncwarp();
-  // clear the links and edge masks of the planes of the removed triangles
-  for (int r = lane; r < nrem; r += 32) {
-    const unsigned t = w.rem[r];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const unsigned p = (t >> (8 * i)) & 0xff;
-      w.next[p] = kNone;
-      for (int k = 0; k < mw; ++k) w.emask[p * mw + k] = 0u;
-    }
-  }
-  __syncwarp();
-  // mark every directed edge a->b of a removed triangle: bit b of mask a
-  for (int r = lane; r < nrem; r += 32) {
-    const unsigned t = w.rem[r];
-    const unsigned a = t & 0xff, b = (t >> 8) & 0xff, c = (t >> 16) & 0xff;
-    atomicOr(&w.emask[a * mw + (b >> 5)], 1u << (b & 31));
-    atomicOr(&w.emask[b * mw + (c >> 5)], 1u << (c & 31));
-    atomicOr(&w.emask[c * mw + (a >> 5)], 1u << (a & 31));
-  }
-  __syncwarp();
-  // boundary edges: directed edges whose twin is unmarked, in removed order;
-  // link next[u] = v (a plane starting two edges makes the cavity
-  // non-manifold)
   int nb = 0;
   bool bad = false;
-  unsigned first_u = kNone;
-  for (int r0 = 0; r0 < nrem; r0 += 32) {
-    const int r = r0 + lane;
-    unsigned t = 0, bmask = 0;  // bit e3: edge (tv[e3], tv[e3+1]) is on the boundary
-    if (r < nrem) {
-      t = w.rem[r];
+  bool bnd = false;          // fast path: this lane holds boundary edge (bu -> bv)
+  unsigned bu = 0, bv = 0;
+  int bpos = 0;
+  if (fast) {
+    const bool act = lane < 3 * nside;
+    unsigned key = 0x10000u + lane;  // unique for idle lanes
+    if (act) {
+      const unsigned t = w.rem[lane / 3];
+      const int e3 = lane % 3;
+      bu = (t >> (8 * e3)) & 0xff;
+      bv = (t >> (8 * ((e3 + 1) % 3))) & 0xff;
+      if (from_kept) {
+        const unsigned x = bu;
+        bu = bv;
+        bv = x;
+      }
+      key = bu < bv ? (bu << 8 | bv) : (bv << 8 | bu);
+    }
+    const int cnt = __popc(__match_any_sync(kFull, key));
+    bnd = act && cnt == 1;
+    bad = act && cnt > 2;
+    const unsigned bmask = __ballot_sync(kFull, bnd);
+    nb = __popc(bmask);
+    bpos = __popc(bmask & lanemask_lt(lane));
+    // every plane starts and ends at most one boundary edge (every lane
+    // takes part in both matches)
+    const unsigned mu = __match_any_sync(kFull, bnd ? bu : 0x10000u + lane);
+    const unsigned mv = __match_any_sync(kFull, bnd ? bv : 0x10000u + lane);
+    bad |= bnd && (__popc(mu) != 1 || __popc(mv) != 1);
+    if (bnd) w.next[bu] = lane;
+    __syncwarp();
+    int succ = bnd ? int(w.next[bv] & 31u) : lane;
+    const unsigned su = __shfl_sync(kFull, bu, succ);
+    bad |= bnd && (!((bmask >> succ) & 1u) || su != bv);
+    bad = __any_sync(kFull, bad);
+    if (!bad) {
+      // one cycle: the lowest lane of every orbit, by pointer jumping
+      int mn = lane;
 #pragma unroll
-      for (int e3 = 0; e3 < 3; ++e3) {
-        const unsigned u = (t >> (8 * e3)) & 0xff, v = (t >> (8 * ((e3 + 1) % 3))) & 0xff;
-        if (!((w.emask[v * mw + (u >> 5)] >> (u & 31)) & 1u)) bmask |= 1u << e3;
+      for (int k = 0; k < 5; ++k) {
+        const int om = __shfl_sync(kFull, mn, succ);
+        succ = __shfl_sync(kFull, succ, succ);
+        mn = min(mn, om);
+      }
+      bad = __popc(__ballot_sync(kFull, bnd && mn == lane)) != 1;
+    }
+  } else {
+    // clear the links and edge masks of the planes of the removed triangles
+    for (int r = lane; r < nrem; r += 32) {
+      const unsigned t = w.rem[r];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const unsigned p = (t >> (8 * i)) & 0xff;
+        w.next[p] = kNone;
+        for (int k = 0; k < mw; ++k) w.emask[p * mw + k] = 0u;
       }
     }
-    const int cnt = __popc(bmask);
-    const int incl = warp_incl_scan(cnt, lane);
-    int pos = nb + incl - cnt;
+    __syncwarp();
+    // mark every directed edge a->b of a removed triangle: bit b of mask a
+    for (int r = lane; r < nrem; r += 32) {
+      const unsigned t = w.rem[r];
+      const unsigned a = t & 0xff, b = (t >> 8) & 0xff, c = (t >> 16) & 0xff;
+      atomicOr(&w.emask[a * mw + (b >> 5)], 1u << (b & 31));
+      atomicOr(&w.emask[b * mw + (c >> 5)], 1u << (c & 31));
+      atomicOr(&w.emask[c * mw + (a >> 5)], 1u << (a & 31));
+    }
+    __syncwarp();
+    // boundary edges: directed edges whose twin is unmarked, in removed
+    // order; link next[u] = v (a plane starting two edges makes the cavity
+    // non-manifold)
+    unsigned first_u = kNone;
+    for (int r0 = 0; r0 < nrem; r0 += 32) {
+      const int r = r0 + lane;
+      unsigned t = 0, bmask = 0;  // bit e3: edge (tv[e3], tv[e3+1]) is on the boundary
+      if (r < nrem) {
+        t = w.rem[r];
 #pragma unroll
-    for (int e3 = 0; e3 < 3; ++e3) {
-      if (!((bmask >> e3) & 1u)) continue;
-      const unsigned u = (t >> (8 * e3)) & 0xff, v = (t >> (8 * ((e3 + 1) % 3))) & 0xff;
-      if (pos < w.vc) w.edge[pos] = u | (v << 8);
-      ++pos;
-      if (atomicCAS(&w.next[u], kNone, v) != kNone) bad = true;
-      if (first_u == kNone) first_u = u;
+        for (int e3 = 0; e3 < 3; ++e3) {
+          const unsigned u = (t >> (8 * e3)) & 0xff, v = (t >> (8 * ((e3 + 1) % 3))) & 0xff;
+          if (!((w.emask[v * mw + (u >> 5)] >> (u & 31)) & 1u)) bmask |= 1u << e3;
+        }
+      }
+      const int cnt = __popc(bmask);
+      const int incl = warp_incl_scan(cnt, lane);
+      int pos = nb + incl - cnt;
+#pragma unroll
+      for (int e3 = 0; e3 < 3; ++e3) {
+        if (!((bmask >> e3) & 1u)) continue;
+        const unsigned u = (t >> (8 * e3)) & 0xff, v = (t >> (8 * ((e3 + 1) % 3))) & 0xff;
+        if (pos < w.vc) w.edge[pos] = u | (v << 8);
+        ++pos;
+        if (atomicCAS(&w.next[u], kNone, v) != kNone) bad = true;
+        if (first_u == kNone) first_u = u;
+      }
+      nb += __shfl_sync(kFull, incl, 31);
     }
-    nb += __shfl_sync(kFull, incl, 31);
-  }
-  bad = __any_sync(kFull, bad);
-  __syncwarp();
-  if (!bad) {
-    // the links must form a single cycle through all nb edges
-    const unsigned has = __ballot_sync(kFull, first_u != kNone);
-    const unsigned u0 = __shfl_sync(kFull, first_u, has ? __ffs(has) - 1 : 0);
-    bool ok = false;
-    if (lane == 0 && u0 != kNone) {
-      unsigned u = u0;
-      int steps = 0;
-      do {
-        u = w.next[u];
-        ++steps;
-      } while (u != kNone && u != u0 && steps <= nb);
-      ok = u == u0 && steps == nb;
+    bad = __any_sync(kFull, bad);
+    __syncwarp();
+    if (!bad) {
+      // the links must form a single cycle through all nb edges
+      const unsigned has = __ballot_sync(kFull, first_u != kNone);
+      const unsigned u0 = __shfl_sync(kFull, first_u, has ? __ffs(has) - 1 : 0);
+      bool ok = false;
+      if (lane == 0 && u0 != kNone) {
+        unsigned u = u0;
+        int steps = 0;
+        do {
+          u = w.next[u];
+          ++steps;
+        } while (u != kNone && u != u0 && steps <= nb);
+        ok = u == u0 && steps == nb;
+      }
+      bad = !__shfl_sync(kFull, ok, 0);
     }
-    bad = !__shfl_sync(kFull, ok, 0);
   }
   trace_rec(tr, trcap, lane, 2, nb, bad, 0, 0);
   if (bad || nb < 3) {
     status = kInconsistentBoundary;
     return -1;
   }
-  const int nkeep = w.nv - nrem;
   const int F = nkeep + nb;
   if (F > V) {
     status = kVertexOverflow;
@@ -413,10 +472,17 @@ __device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, u
   __syncwarp();
   const int in_holes = nholes - nmov;
   bool degenerate = false;
-  for (int q = lane; q < nb; q += 32) {
-    const unsigned ed = w.edge[q];
-    const int dst = q < in_holes ? int(w.hole[nmov + q]) : w.nv + (q - in_holes);
-    degenerate |= !make_vertex(w, dst, unsigned(pid), ed & 0xff, (ed >> 8) & 0xff);
+  if (fast) {
+    if (bnd) {
+      const int dst = bpos < in_holes ? int(w.hole[nmov + bpos]) : w.nv + (bpos - in_holes);
+      degenerate = !make_vertex(w, dst, unsigned(pid), bu, bv);
+    }
+  } else {
+    for (int q = lane; q < nb; q += 32) {
+      const unsigned ed = w.edge[q];
+      const int dst = q < in_holes ? int(w.hole[nmov + q]) : w.nv + (q - in_holes);
+      degenerate |= !make_vertex(w, dst, unsigned(pid), ed & 0xff, (ed >> 8) & 0xff);
+    }
   }
   __syncwarp();
   if (__any_sync(kFull, degenerate)) {
@@ -1133,12 +1199,12 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
         const float4 b = __ldg(&a.stored[z]);
         const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
         nd2 = bx * bx + by * by + bz * bz;
-        const double len = sqrt(nd2);
+        const double len = sqrt(nd2), inv = 1.0 / len;
         // kept side contains the seed: n = -(b - s)/|b - s|, offset of the
         // power bisector (ConvexCell.cl:321-328) or, for a wall neighbour,
         // through the neighbour itself
-        const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) / (2.0 * len);
-        pl = Plane{-bx / len, -by / len, -bz / len, off};
+        const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) * (0.5 * inv);
+        pl = Plane{-bx * inv, -by * inv, -bz * inv, off};
         valid = true;
       }
     }
