@@ -46,7 +46,7 @@ constexpr int kDeferred = 100;      // internal status: cell parked for k_cone
 struct Layout {
   int Pc, Vc, G, Mw;  // Mw: 32-bit words of one plane's edge mask
   unsigned o_plane, o_cx, o_cy, o_cz, o_cw, o_d2, o_tri, o_next, o_emask, o_rem, o_hole, o_edge;
-  unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist, o_pts;
+  unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist, o_pts, o_fstart, o_fv;
   unsigned total;
 };
 
@@ -86,8 +86,10 @@ __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
     L.o_btri = o; o = align16(o + 4u * L.Vc);
     L.o_tlist = o; o = align16(o + 4u * L.G);
     L.o_pts = o; o = align16(o + 8u * 12);
+    L.o_fstart = o; o = align16(o + 4u * (L.Pc + 1));
+    L.o_fv = o; o = align16(o + 3u * L.Vc);
   } else {
-    L.o_bcx = L.o_bcy = L.o_bcz = L.o_bcw = L.o_bd2 = L.o_btri = L.o_tlist = L.o_pts = 0;
+    L.o_bcx = L.o_bcy = L.o_bcz = L.o_bcw = L.o_bd2 = L.o_btri = L.o_tlist = L.o_pts = L.o_fstart = L.o_fv = 0;
   }
   L.total = o;
   return L;
@@ -106,6 +108,8 @@ struct WarpCell {
   unsigned *btri;
   int *tlist;
   double *pts;  // start corner and the current boundary triangle, local frame
+  int *fstart;         // per plane: first entry of its face in fv (np + 1 entries)
+  unsigned char *fv;   // vertex ids of every face, in cyclic order
   int nv, np;  // vertex and plane counts (warp-uniform)
   int vc, mw;  // capacity of the vertex arrays, words per edge mask
 };
@@ -132,6 +136,8 @@ __device__ __forceinline__ WarpCell bind(unsigned char *base, const Layout &L) {
   w.btri = reinterpret_cast<unsigned *>(base + L.o_btri);
   w.tlist = reinterpret_cast<int *>(base + L.o_tlist);
   w.pts = reinterpret_cast<double *>(base + L.o_pts);
+  w.fstart = reinterpret_cast<int *>(base + L.o_fstart);
+  w.fv = base + L.o_fv;
   w.nv = w.np = 0;
   w.vc = L.Vc;
   w.mw = L.Mw;
@@ -950,6 +956,469 @@ __device__ int drop_separated(const WarpCell &w, const DevGrid &g, float4 s, int
   return kept;
 }
 
+// ---- Cone pieces from their facets, for an apex inside the cell ----
+//
+// With the apex a inside the convex cell C, the piece C ∩ cone(a, t) beyond
+// triangle t is bounded by t ∩ C, by the parts of the cell's faces inside the
+// cone beyond t, and by the cone's three sides.  Its volume and first moment
+// are sums over the facets of the cones from a, and the cone over a facet G
+// is a sum over G's boundary edges (u, v), counter-clockwise around the
+// outward normal, of the signed tetrahedra (a, c, u, v), c any point of G's
+// plane.  The sides pass through a and give nothing.  Every edge is a
+// segment clipped by a few planes, so a piece needs neither 3D clipping nor
+// polygon buffers: one triangle per lane, registers only.  Equal to the
+// reference's clipped-cone integral (ConvexCell.cl:1082-1115) in exact
+// arithmetic.
+constexpr int kFaceCap = 64;  // faces of one cell culled per batch of a 64-bit mask
+
+// Face lists of the cell, each counter-clockwise around the face's outward
+// normal (-n of its plane), and vertex positions (local frame) in px/py/pz.
+// Angular bounds of the faces seen from the apex: per face, the unit axis
+// and the half-angle (with cos, sin) of a cone from a that holds the face,
+// as floats in the backup arrays (unused on this path); kAngFaces faces fit.
+__device__ __forceinline__ float *face_angles(const WarpCell &w) { return reinterpret_cast<float *>(w.bcw); }
+__device__ __forceinline__ int face_angle_cap(const WarpCell &w) { return (20 * w.vc) / 24; }
+__device__ __forceinline__ unsigned char *face_nb(const WarpCell &w) { return reinterpret_cast<unsigned char *>(w.edge); }
+
+__device__ void build_faces(const WarpCell &w, double *px, double *py, double *pz, const double a[3], int lane) {
+  const int np = w.np, nv = w.nv;
+  int *fstart = w.fstart;
+  unsigned char *fv = w.fv;
+  for (int p = lane; p <= np; p += 32) fstart[p] = 0;
+  __syncwarp();
+  for (int v = lane; v < nv; v += 32) {
+    const double inv = 1.0 / w.cw[v];
+    px[v] = w.cx[v] * inv;
+    py[v] = w.cy[v] * inv;
+    pz[v] = w.cz[v] * inv;
+    const unsigned t = w.tri[v];
+    atomicAdd(&fstart[(t & 0xff) + 1], 1);
+    atomicAdd(&fstart[((t >> 8) & 0xff) + 1], 1);
+    atomicAdd(&fstart[((t >> 16) & 0xff) + 1], 1);
+  }
+  __syncwarp();
+  int carry = 0;
+  for (int b0 = 1; b0 <= np; b0 += 32) {
+    const int p = b0 + lane;
+    const int c = p <= np ? fstart[p] : 0;
+    const int incl = warp_incl_scan(c, lane);
+    __syncwarp();
+    if (p <= np) fstart[p] = carry + incl;
+    carry += __shfl_sync(kFull, incl, 31);
+  }
+  __syncwarp();
+  // lane per face: its vertices, chained (vertex (p, y, z) is followed by
+  // the vertex (p, z, .)), then turned counter-clockwise around -n_p
+  for (int p = lane; p < np; p += 32) {
+    const int f0 = fstart[p], k = fstart[p + 1] - f0;
+    int m = 0;
+    for (int v = 0; v < nv && m < k; ++v) {
+      const unsigned t = w.tri[v];
+      if ((t & 0xff) == unsigned(p) || ((t >> 8) & 0xff) == unsigned(p) || ((t >> 16) & 0xff) == unsigned(p))
+        fv[f0 + m++] = (unsigned char)v;
+    }
+    auto rot = [&](int v, bool to) {
+      const unsigned t = w.tri[v];
+      const unsigned a = t & 0xff, b = (t >> 8) & 0xff, c = (t >> 16) & 0xff;
+      if (to) return a == unsigned(p) ? c : (b == unsigned(p) ? a : b);
+      return a == unsigned(p) ? b : (b == unsigned(p) ? c : a);
+    };
+    for (int i = 1; i < k; ++i) {
+      const unsigned want = rot(fv[f0 + i - 1], true);
+      for (int j = i; j < k; ++j) {
+        if (rot(fv[f0 + j], false) == want) {
+          const unsigned char x = fv[f0 + i];
+          fv[f0 + i] = fv[f0 + j];
+          fv[f0 + j] = x;
+          break;
+        }
+      }
+    }
+    if (k >= 3) {
+      const Plane pl = w.plane[p];
+      double sx = 0, sy = 0, sz = 0;
+      for (int i = 0; i < k; ++i) {
+        const int u = fv[f0 + i], v = fv[f0 + (i + 1 == k ? 0 : i + 1)];
+        sx += py[u] * pz[v] - pz[u] * py[v];
+        sy += pz[u] * px[v] - px[u] * pz[v];
+        sz += px[u] * py[v] - py[u] * px[v];
+      }
+      if (sx * pl.x + sy * pl.y + sz * pl.z > 0.0) {
+        for (int i = 0, j = k - 1; i < j; ++i, --j) {
+          const unsigned char x = fv[f0 + i];
+          fv[f0 + i] = fv[f0 + j];
+          fv[f0 + j] = x;
+        }
+      }
+    }
+    // plane of edge (i, i+1): shared by the two vertices, other than p
+    unsigned char *nb = face_nb(w);
+    for (int i = 0; i < k; ++i) {
+      const unsigned t1 = w.tri[fv[f0 + i]], t2 = w.tri[fv[f0 + (i + 1 == k ? 0 : i + 1)]];
+      unsigned e = 0xffu;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const unsigned x = (t1 >> (8 * b)) & 0xff;
+        if (x != unsigned(p) && (x == (t2 & 0xff) || x == ((t2 >> 8) & 0xff) || x == ((t2 >> 16) & 0xff))) e = x;
+      }
+      nb[f0 + i] = (unsigned char)e;
+    }
+    if (p < face_angle_cap(w)) {
+      float *ang = face_angles(w) + 6 * p;
+      float ux = 0.f, uy = 0.f, uz = 0.f;
+      for (int i = 0; i < k; ++i) {
+        const int v = fv[f0 + i];
+        const float dx = float(px[v] - a[0]), dy = float(py[v] - a[1]), dz = float(pz[v] - a[2]);
+        const float il = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+        ux += dx * il;
+        uy += dy * il;
+        uz += dz * il;
+      }
+      const float ul = rsqrtf(fmaxf(ux * ux + uy * uy + uz * uz, 1e-30f));
+      ux *= ul;
+      uy *= ul;
+      uz *= ul;
+      float cmin = 1.f;
+      for (int i = 0; i < k; ++i) {
+        const int v = fv[f0 + i];
+        const float dx = float(px[v] - a[0]), dy = float(py[v] - a[1]), dz = float(pz[v] - a[2]);
+        const float il = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+        cmin = fminf(cmin, (dx * ux + dy * uy + dz * uz) * il);
+      }
+      const float th = acosf(fmaxf(-1.f, fminf(1.f, cmin)));
+      ang[0] = ux;
+      ang[1] = uy;
+      ang[2] = uz;
+      ang[3] = th;
+      ang[4] = cosf(th);
+      ang[5] = sinf(th);
+    }
+  }
+  __syncwarp();
+}
+
+struct ConePiece {
+  double a[3];      // apex
+  double c[4][4];   // side planes (through a) and the triangle's plane, inside >= 0
+  double t[3][3];   // triangle corners, counter-clockwise around c[3]
+  double acc[4];    // sum of w*x, w*y, w*z, w (unscaled: 6x the volume)
+};
+
+__device__ __forceinline__ double pval(const double *n, double x, double y, double z) {
+  return fma(n[0], x, fma(n[1], y, fma(n[2], z, n[3])));
+}
+
+// Signed tetrahedron (a, c, u, v) into acc: 6 * volume and 6 * volume * 4 * centroid.
+__device__ __forceinline__ void edge_tet(ConePiece &q, const double c[3], const double u[3], const double v[3]) {
+  const double cx = c[0] - q.a[0], cy = c[1] - q.a[1], cz = c[2] - q.a[2];
+  const double ux = u[0] - q.a[0], uy = u[1] - q.a[1], uz = u[2] - q.a[2];
+  const double vx = v[0] - q.a[0], vy = v[1] - q.a[1], vz = v[2] - q.a[2];
+  const double det = cx * (uy * vz - uz * vy) - cy * (ux * vz - uz * vx) + cz * (ux * vy - uy * vx);
+  q.acc[0] += det * (q.a[0] + c[0] + u[0] + v[0]);
+  q.acc[1] += det * (q.a[1] + c[1] + u[1] + v[1]);
+  q.acc[2] += det * (q.a[2] + c[2] + u[2] + v[2]);
+  q.acc[3] += det * 4.0;
+}
+
+// Clips segment u + s (v - u), s in [lo, hi], by plane n (inside >= 0).
+__device__ __forceinline__ void clip_seg(double eu, double ev, double &lo, double &hi) {
+  if (eu >= 0.0 && ev >= 0.0) return;
+  if (eu < 0.0 && ev < 0.0) {
+    hi = -1.0;
+    return;
+  }
+  const double s = eu / (eu - ev);
+  if (eu < 0.0) lo = fmax(lo, s);
+  else hi = fmin(hi, s);
+}
+
+// Line of planes n1 and n2 (inside >= 0 each) as x0 + s d with d = n1 x n2;
+// false when they are parallel.
+__device__ __forceinline__ bool plane_line(const double *n1, const double *n2, double x0[3], double d[3]) {
+  d[0] = n1[1] * n2[2] - n1[2] * n2[1];
+  d[1] = n1[2] * n2[0] - n1[0] * n2[2];
+  d[2] = n1[0] * n2[1] - n1[1] * n2[0];
+  const double dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  const double nn = (n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2]) * (n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]);
+  if (!(dd > 1e-24 * nn)) return false;
+  // x0 = (-w1 (n2 x d) - w2 (d x n1)) / |d|^2
+  const double a0 = n2[1] * d[2] - n2[2] * d[1], a1 = n2[2] * d[0] - n2[0] * d[2], a2 = n2[0] * d[1] - n2[1] * d[0];
+  const double b0 = d[1] * n1[2] - d[2] * n1[1], b1 = d[2] * n1[0] - d[0] * n1[2], b2 = d[0] * n1[1] - d[1] * n1[0];
+  const double inv = 1.0 / dd;
+  x0[0] = (-n1[3] * a0 - n2[3] * b0) * inv;
+  x0[1] = (-n1[3] * a1 - n2[3] * b1) * inv;
+  x0[2] = (-n1[3] * a2 - n2[3] * b2) * inv;
+  return true;
+}
+
+// Parameter range of the line x0 + s d inside plane n.
+__device__ __forceinline__ void clip_line(const double *n, const double x0[3], const double d[3], double &lo, double &hi) {
+  const double v0 = pval(n, x0[0], x0[1], x0[2]);
+  const double sl = n[0] * d[0] + n[1] * d[1] + n[2] * d[2];
+  if (sl > 0.0) lo = fmax(lo, -v0 / sl);
+  else if (sl < 0.0) hi = fmin(hi, -v0 / sl);
+  else if (v0 < 0.0) hi = -1e300;
+}
+
+// Face f's facet: its edges inside the cone, and the cone planes' lines
+// inside the face (bounded by the face's edge planes and the other cone
+// planes).
+__device__ void face_facet(ConePiece &q, const WarpCell &w, const double *px, const double *py, const double *pz,
+                           int f) {
+  const int f0 = w.fstart[f], k = w.fstart[f + 1] - f0;
+  const int v0 = w.fv[f0];
+  const double c[3] = {px[v0], py[v0], pz[v0]};
+  for (int i = 0; i < k; ++i) {
+    const int iu = w.fv[f0 + i], iv = w.fv[f0 + (i + 1 == k ? 0 : i + 1)];
+    const double u[3] = {px[iu], py[iu], pz[iu]}, v[3] = {px[iv], py[iv], pz[iv]};
+    double lo = 0.0, hi = 1.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) clip_seg(pval(q.c[j], u[0], u[1], u[2]), pval(q.c[j], v[0], v[1], v[2]), lo, hi);
+    if (lo < hi) {
+      const double U[3] = {fma(lo, v[0] - u[0], u[0]), fma(lo, v[1] - u[1], u[1]), fma(lo, v[2] - u[2], u[2])};
+      const double V[3] = {fma(hi, v[0] - u[0], u[0]), fma(hi, v[1] - u[1], u[1]), fma(hi, v[2] - u[2], u[2])};
+      edge_tet(q, c, U, V);
+    }
+  }
+  const Plane pf = w.plane[f];
+  const double nf[4] = {pf.x, pf.y, pf.z, pf.w};
+#pragma unroll 1
+  for (int j = 0; j < 4; ++j) {
+    double x0[3], d[3];
+    if (!plane_line(nf, q.c[j], x0, d)) continue;
+    double lo = -1e300, hi = 1e300;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+      if (jj != j) clip_line(q.c[jj], x0, d, lo, hi);
+    const unsigned char *nb = face_nb(w);
+    for (int i = 0; i < k && lo < hi; ++i) {
+      // the plane of the face's edge (i, i+1)
+      const unsigned e = nb[f0 + i];
+      if (e == 0xffu) continue;
+      const Plane pe = w.plane[e];
+      const double ne[4] = {pe.x, pe.y, pe.z, pe.w};
+      clip_line(ne, x0, d, lo, hi);
+    }
+    if (lo < hi) {
+      const double U[3] = {fma(lo, d[0], x0[0]), fma(lo, d[1], x0[1]), fma(lo, d[2], x0[2])};
+      const double V[3] = {fma(hi, d[0], x0[0]), fma(hi, d[1], x0[1]), fma(hi, d[2], x0[2])};
+      edge_tet(q, c, U, V);
+    }
+  }
+}
+
+// Sets up the cone of triangle tri from apex a; false for a flat cone.
+__device__ bool cone_setup(ConePiece &q, const DevGrid &g, float4 s, int tri, const double a[3], double &sgn) {
+  const float4 q1 = __ldg(&g.points[__ldg(&g.tris[3 * tri])]);
+  const float4 q2 = __ldg(&g.points[__ldg(&g.tris[3 * tri + 1])]);
+  const float4 q3 = __ldg(&g.points[__ldg(&g.tris[3 * tri + 2])]);
+  const float4 qs[3] = {q1, q2, q3};
+  double d[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    q.t[i][0] = double(qs[i].x) - s.x;
+    q.t[i][1] = double(qs[i].y) - s.y;
+    q.t[i][2] = double(qs[i].z) - s.z;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[i][k] = q.t[i][k] - a[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) q.a[k] = a[k];
+  const double det = d[0][0] * (d[1][1] * d[2][2] - d[1][2] * d[2][1]) -
+                     d[0][1] * (d[1][0] * d[2][2] - d[1][2] * d[2][0]) +
+                     d[0][2] * (d[1][0] * d[2][1] - d[1][1] * d[2][0]);
+  if (!(fabs(det) > 0.0)) return false;
+  // the reference's sign: + when the triangle is seen positively from a
+  sgn = det > 0.0 ? 1.0 : -1.0;
+  if (det < 0.0) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double x = q.t[1][k];
+      q.t[1][k] = q.t[2][k];
+      q.t[2][k] = x;
+      x = d[1][k];
+      d[1][k] = d[2][k];
+      d[2][k] = x;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double *u = d[j], *v = d[(j + 1) % 3];
+    q.c[j][0] = u[1] * v[2] - u[2] * v[1];
+    q.c[j][1] = u[2] * v[0] - u[0] * v[2];
+    q.c[j][2] = u[0] * v[1] - u[1] * v[0];
+    q.c[j][3] = -(q.c[j][0] * a[0] + q.c[j][1] * a[1] + q.c[j][2] * a[2]);
+  }
+  const double e1[3] = {q.t[1][0] - q.t[0][0], q.t[1][1] - q.t[0][1], q.t[1][2] - q.t[0][2]};
+  const double e2[3] = {q.t[2][0] - q.t[0][0], q.t[2][1] - q.t[0][1], q.t[2][2] - q.t[0][2]};
+  q.c[3][0] = e1[1] * e2[2] - e1[2] * e2[1];
+  q.c[3][1] = e1[2] * e2[0] - e1[0] * e2[2];
+  q.c[3][2] = e1[0] * e2[1] - e1[1] * e2[0];
+  q.c[3][3] = -(q.c[3][0] * q.t[0][0] + q.c[3][1] * q.t[0][1] + q.c[3][2] * q.t[0][2]);
+  q.acc[0] = q.acc[1] = q.acc[2] = q.acc[3] = 0.0;
+  return true;
+}
+
+// Cone pieces of triangles tids[t0, t1) (at most 32), one per lane, summed
+// over the warp into acc.  Needs build_faces.
+__device__ void facet_triangles(const WarpCell &w, const double *px, const double *py, const double *pz,
+                                const DevGrid &g, float4 s, const int *tids, int t0, int t1, const double a[3],
+                                double acc[4], int lane, unsigned long long *ctr) {
+  ConePiece q;
+  double sgn = 0.0;
+  const bool act = t0 + lane < t1 && cone_setup(q, g, s, tids[t0 + lane], a, sgn);
+  if (!act) q.acc[0] = q.acc[1] = q.acc[2] = q.acc[3] = 0.0;
+  const int np = w.np;
+  // t ∩ C, seen from a (outer side): edges t0 -> t2 -> t1 -> t0 clipped by
+  // the cell planes, and the lines of the cell planes that cut t
+  // cone axis and half-angle seen from a (floats, for culling the faces)
+  float tux = 0.f, tuy = 0.f, tuz = 0.f, tth = 4.f, tc = -1.f, ts = 0.f;
+  if (act) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float dx = float(q.t[i][0] - a[0]), dy = float(q.t[i][1] - a[1]), dz = float(q.t[i][2] - a[2]);
+      const float il = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+      tux += dx * il;
+      tuy += dy * il;
+      tuz += dz * il;
+    }
+    const float ul = rsqrtf(fmaxf(tux * tux + tuy * tuy + tuz * tuz, 1e-30f));
+    tux *= ul;
+    tuy *= ul;
+    tuz *= ul;
+    float cmin = 1.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float dx = float(q.t[i][0] - a[0]), dy = float(q.t[i][1] - a[1]), dz = float(q.t[i][2] - a[2]);
+      const float il = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+      cmin = fminf(cmin, (dx * tux + dy * tuy + dz * tuz) * il);
+    }
+    tth = acosf(fmaxf(-1.f, fminf(1.f, cmin)));
+    tc = cosf(tth);
+    ts = sinf(tth);
+  }
+  if (act) {
+    // bounding sphere of t: a plane farther than its radius does not cut t
+    const double gx = (q.t[0][0] + q.t[1][0] + q.t[2][0]) * (1.0 / 3.0);
+    const double gy = (q.t[0][1] + q.t[1][1] + q.t[2][1]) * (1.0 / 3.0);
+    const double gz = (q.t[0][2] + q.t[1][2] + q.t[2][2]) * (1.0 / 3.0);
+    double r2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double dx = q.t[i][0] - gx, dy = q.t[i][1] - gy, dz = q.t[i][2] - gz;
+      r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+    }
+    const double rad = sqrt(r2) * (1.0 + 1e-9) + 1e-9;
+    double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {1.0, 1.0, 1.0};
+    for (int kb = 0; kb < np; kb += 64) {
+      unsigned long long cutm = 0;
+      const int ke = min(np, kb + 64);
+      for (int kp = kb; kp < ke; ++kp) {
+        const Plane pl = w.plane[kp];
+        const double n[4] = {pl.x, pl.y, pl.z, pl.w};
+        if (pval(n, gx, gy, gz) > rad) continue;
+        const double e0 = pval(n, q.t[0][0], q.t[0][1], q.t[0][2]);
+        const double e1 = pval(n, q.t[1][0], q.t[1][1], q.t[1][2]);
+        const double e2 = pval(n, q.t[2][0], q.t[2][1], q.t[2][2]);
+        if (e0 >= 0.0 && e1 >= 0.0 && e2 >= 0.0) continue;
+        cutm |= 1ull << (kp - kb);
+        clip_seg(e0, e2, lo[0], hi[0]);
+        clip_seg(e2, e1, lo[1], hi[1]);
+        clip_seg(e1, e0, lo[2], hi[2]);
+      }
+      // lines of the cutting planes in the triangle's plane (direction
+      // n_3 x n_k keeps t ∩ C on the left seen from a), bounded by t's edges
+      // and the other cutting planes: every other plane holds all of t
+      const unsigned long long all = cutm;
+      while (cutm) {
+        const int kp = kb + __ffsll(cutm) - 1;
+        cutm &= cutm - 1;
+        const Plane pl = w.plane[kp];
+        const double n[4] = {pl.x, pl.y, pl.z, pl.w};
+        double x0[3], d[3];
+        if (!plane_line(q.c[3], n, x0, d)) continue;
+        double l = -1e300, h = 1e300;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) clip_line(q.c[j], x0, d, l, h);
+        unsigned long long others = all & ~(1ull << (kp - kb));
+        while (others && l < h) {
+          const int k2 = kb + __ffsll(others) - 1;
+          others &= others - 1;
+          const Plane p2 = w.plane[k2];
+          const double n2[4] = {p2.x, p2.y, p2.z, p2.w};
+          clip_line(n2, x0, d, l, h);
+        }
+        // cutting planes of the other batches
+        for (int k2 = 0; k2 < np && l < h && np > 64; ++k2) {
+          if (k2 >= kb && k2 < ke) continue;
+          const Plane p2 = w.plane[k2];
+          const double n2[4] = {p2.x, p2.y, p2.z, p2.w};
+          clip_line(n2, x0, d, l, h);
+        }
+        if (l < h) {
+          const double U[3] = {fma(l, d[0], x0[0]), fma(l, d[1], x0[1]), fma(l, d[2], x0[2])};
+          const double V[3] = {fma(h, d[0], x0[0]), fma(h, d[1], x0[1]), fma(h, d[2], x0[2])};
+          edge_tet(q, q.t[0], U, V);
+        }
+      }
+    }
+    const int ord[4] = {0, 2, 1, 0};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (!(lo[i] < hi[i])) continue;
+      const double *u = q.t[ord[i]], *v = q.t[ord[i + 1]];
+      const double U[3] = {fma(lo[i], v[0] - u[0], u[0]), fma(lo[i], v[1] - u[1], u[1]), fma(lo[i], v[2] - u[2], u[2])};
+      const double V[3] = {fma(hi[i], v[0] - u[0], u[0]), fma(hi[i], v[1] - u[1], u[1]), fma(hi[i], v[2] - u[2], u[2])};
+      edge_tet(q, q.t[0], U, V);
+    }
+  }
+  // faces of the cell that the cone meets beyond t, 64 at a time
+  for (int fb = 0; fb < np; fb += kFaceCap) {
+    unsigned long long hit = 0;
+    if (act) {
+      const int fe = min(np, fb + kFaceCap);
+      const float *ang = face_angles(w);
+      const int acap = face_angle_cap(w);
+      for (int f = fb; f < fe; ++f) {
+        const int f0 = w.fstart[f], k = w.fstart[f + 1] - f0;
+        if (k < 3) continue;
+        if (f < acap) {
+          // the cones from a around the face and around t must meet (both
+          // narrower than a half-space, so each holds its convex hull)
+          const float *g4 = ang + 6 * f;
+          if (g4[3] < 1.5f && tth < 1.5f) {
+            const float cosang = g4[0] * tux + g4[1] * tuy + g4[2] * tuz;
+            if (cosang < g4[4] * tc - g4[5] * ts - 1e-3f) continue;
+          }
+        }
+        unsigned any_in = 0;
+        for (int i = 0; i < k && any_in != 15u; ++i) {
+          const int v = w.fv[f0 + i];
+          const double x = px[v], y = py[v], z = pz[v];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) any_in |= (pval(q.c[j], x, y, z) >= 0.0 ? 1u : 0u) << j;
+        }
+        if (any_in == 15u) hit |= 1ull << (f - fb);
+      }
+    }
+    while (__any_sync(kFull, hit != 0)) {
+      if (hit) {
+        const int f = fb + __ffsll(hit) - 1;
+        hit &= hit - 1;
+        face_facet(q, w, px, py, pz, f);
+      }
+    }
+  }
+  count(ctr, kCtrExports, t1 - t0, lane);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double v = act ? sgn * q.acc[k] * (1.0 / 24.0) : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    acc[k] += v;
+  }
+}
+
 // Parked boundary cell: header, planes, vertices, triangle ids.
 struct DeferHeader {
   int sid, nuniq, nv, np;
@@ -1148,6 +1617,12 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   if constexpr (!INL) {
     return kParkOverflow;  // re-run by the inline variant
   } else {
+    if (inner) {
+      build_faces(w, w.bcx, w.bcy, w.bcz, pt0, lane);
+      for (int b0 = 0; b0 < nuniq; b0 += 32)
+        facet_triangles(w, w.bcx, w.bcy, w.bcz, g, s, w.tlist, b0, min(nuniq, b0 + 32), pt0, acc, lane, ctr);
+      return kSuccess;
+    }
     const int bk_nv = w.nv, bk_np = w.np;
     backup<VS>(w, lane);
     int fail_at = 0;
@@ -1266,7 +1741,7 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
 // memory and runs the chunk's cones.  Partial moments and the first failure
 // go to per-item slots; k_cone_finish reduces them in order.
 template <int VS>
-__global__ void __launch_bounds__(128, 5) k_cone(CellLaunch a, Layout L) {
+__global__ void __launch_bounds__(128, 4) k_cone(CellLaunch a, Layout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -1292,14 +1767,23 @@ __global__ void __launch_bounds__(128, 5) k_cone(CellLaunch a, Layout L) {
     const double *vy = vx + L.Vc, *vz = vy + L.Vc, *vw = vz + L.Vc, *vd = vw + L.Vc;
     const unsigned *vt = reinterpret_cast<const unsigned *>(vd + L.Vc);
     const int *tl = reinterpret_cast<const int *>(vt + L.Vc);
+    const bool inner = h->inner != 0;
     for (int i = lane; i < np; i += 32) w.plane[i] = pl[i];
     for (int v = lane; v < nv; v += 32) {
-      w.cx[v] = w.bcx[v] = vx[v];
-      w.cy[v] = w.bcy[v] = vy[v];
-      w.cz[v] = w.bcz[v] = vz[v];
-      w.cw[v] = w.bcw[v] = vw[v];
-      w.d2[v] = w.bd2[v] = vd[v];
-      w.tri[v] = w.btri[v] = vt[v];
+      w.cx[v] = vx[v];
+      w.cy[v] = vy[v];
+      w.cz[v] = vz[v];
+      w.cw[v] = vw[v];
+      w.d2[v] = vd[v];
+      w.tri[v] = vt[v];
+      if (!inner) {
+        w.bcx[v] = vx[v];
+        w.bcy[v] = vy[v];
+        w.bcz[v] = vz[v];
+        w.bcw[v] = vw[v];
+        w.bd2[v] = vd[v];
+        w.btri[v] = vt[v];
+      }
     }
     if (lane < 3) w.pts[lane] = h->pt0[lane];
     __syncwarp();
@@ -1308,8 +1792,16 @@ __global__ void __launch_bounds__(128, 5) k_cone(CellLaunch a, Layout L) {
     const float4 s = a.stored[sid];
     double acc[4] = {0, 0, 0, 0};
     int fail_at = 0;
-    const int st =
-        cone_triangles<VS>(w, a, s, tl, t0, t1, nv, np, h->inner != 0, acc, fail_at, lane, a.counters, nullptr, 0);
+    int st;
+    if (inner) {
+      const double ap[3] = {h->pt0[0], h->pt0[1], h->pt0[2]};
+      build_faces(w, w.bcx, w.bcy, w.bcz, ap, lane);
+      for (int b0 = t0; b0 < t1; b0 += 32)
+        facet_triangles(w, w.bcx, w.bcy, w.bcz, a.grid, s, tl, b0, min(t1, b0 + 32), ap, acc, lane, a.counters);
+      st = kSuccess;
+    } else {
+      st = cone_triangles<VS>(w, a, s, tl, t0, t1, nv, np, false, acc, fail_at, lane, a.counters, nullptr, 0);
+    }
     if (lane == 0) {
       double *part = dq.part + size_t(item) * 4;
       for (int d = 0; d < 4; ++d) part[d] = acc[d];
@@ -1362,7 +1854,7 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
     k_cell<VS, true, false><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     e = cudaFuncSetAttribute(k_cone<VS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    k_cone<VS><<<sm_count * 5, warps_per_block * 32, smem, st>>>(a, L);
+    k_cone<VS><<<sm_count * 4, warps_per_block * 32, smem, st>>>(a, L);
     k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a);
     if (launches) *launches += 3;
   } else if (a.grid.size > 0) {

@@ -48,7 +48,7 @@ struct DeferQueue {
   double *part = nullptr;          // capacity * max_chunks * 4 partial moments
   int *fail = nullptr;             // capacity * max_chunks: (triangle << 4) | status, or INT_MAX
   int max_chunks = 0;              // ceil(T / chunk)
-  int chunk = 16;                  // triangles per work item
+  int chunk = 32;                  // triangles per work item
   int inline_max = 16;             // cells with at most this many triangles stay inline
 };
 

@@ -173,7 +173,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
     DeferQueue &dq = a.defer;
     dq.capacity = std::min(num, std::max(32768, num / 8));
     dq.slot_bytes = defer_slot_bytes(P, V, T);
-    dq.chunk = 16;
+    dq.chunk = 32;  // a warp's lanes take one triangle each
     dq.inline_max = 16;
     dq.max_chunks = std::max(1, (T + dq.chunk - 1) / dq.chunk);
     const size_t items = size_t(dq.capacity) * dq.max_chunks;
