@@ -140,19 +140,29 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   cudaError_t e;
   rpd_stats &S = s->stats;
   const int pi = S.npasses;
-  if ((e = s->knn.ensure(sizeof(unsigned) * size_t(num) * K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
+  // the neighbours of every cell depend on the positions only: a table for
+  // all cells with this K is kept across weight-only re-solves
+  const bool all_cells = ids == nullptr && num == s->n;
+  rpd::DevBuf &kb = all_cells ? s->knn : s->knn_part;
+  const bool reuse = all_cells && s->knn_full_K == K && !counters;
+  if ((e = kb.ensure(sizeof(unsigned) * size_t(num) * K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
   cudaEvent_t ev[3];
   for (auto &x : ev) cudaEventCreate(&x);
   unsigned long long *ctr = counters ? s->counter64.as<unsigned long long>() : nullptr;
   cudaEventRecord(ev[0], st);
-  e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, ids, num, K, s->ring_bound.as<float>(),
-                 s->knn.as<unsigned>(), ctr ? ctr + RPD_CTR_NUM : nullptr, st);
-  if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
+  if (!reuse) {
+    if (all_cells) s->knn_full_K = 0;
+    e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, ids, num, K, s->ring_bound.as<float>(),
+                   kb.as<unsigned>(), ctr ? ctr + RPD_CTR_NUM : nullptr, st);
+    if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
+    if (all_cells) s->knn_full_K = K;
+    S.kernel_launches += 1;
+  }
   cudaEventRecord(ev[1], st);
   CellLaunch a;
   a.stored = s->stored.as<float4>();
   a.n = s->n;
-  a.knn = s->knn.as<unsigned>();
+  a.knn = kb.as<unsigned>();
   a.K = K;
   a.ids = ids;
   a.num = num;
@@ -215,7 +225,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   }
   for (auto &x : ev) cudaEventDestroy(x);
   S.npasses++;
-  S.kernel_launches += num > 0 ? 2 : 0;  // neighbours + cells
+  S.kernel_launches += num > 0 ? 1 : 0;  // the cell kernel (the neighbour kernel counted above)
   return RPD_OK;
 }
 
@@ -328,6 +338,39 @@ int rpd_solver_set_points(rpd_solver *s, const float *xyzw, int n, rpd_mem where
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "bin seeds");
   s->n = n;
   s->dim = dim;
+  s->knn_full_K = 0;
+  return RPD_OK;
+}
+
+// New weights for the seeds already set (user order): the bins and, while K
+// stays the same, the neighbour table of the last launch are kept.
+__global__ void k_set_weights(const float *w, const int *user_to_stored, int n, float4 *user, float4 *stored) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float x = w[i];
+  user[i].w = x;
+  stored[user_to_stored[i]].w = x;
+}
+
+int rpd_solver_set_weights(rpd_solver *s, const float *w, rpd_mem where) {
+  if (!s || !w || s->n <= 0) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const int n = s->n;
+  cudaError_t e;
+  const float *src = w;
+  if (where != RPD_DEVICE) {
+    if ((e = s->weights.ensure(sizeof(float) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc weights");
+    if ((e = cudaMemcpyAsync(s->weights.ptr, w, sizeof(float) * n, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return map_cuda(ctx, e, "copy weights");
+    src = s->weights.as<float>();
+  }
+  k_set_weights<<<(n + 255) / 256, 256, 0, st>>>(src, s->user_to_stored.as<int>(), n, s->user.as<float4>(),
+                                                 s->stored.as<float4>());
+  if ((e = cudaGetLastError()) != cudaSuccess) return map_cuda(ctx, e, "set weights");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "set weights");
+  s->have_results = false;
   return RPD_OK;
 }
 
@@ -361,10 +404,12 @@ int rpd_solver_knn(rpd_solver *s, int K, int *knn_user, rpd_mem where, float *de
   cudaEventCreate(&ev[0]);
   cudaEventCreate(&ev[1]);
   cudaEventRecord(ev[0], st);
+  s->knn_full_K = 0;
   e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, nullptr, s->n, K, s->ring_bound.as<float>(),
                  s->knn.as<unsigned>(), nullptr, st);
   cudaEventRecord(ev[1], st);
   if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
+  s->knn_full_K = K;
   int *dst = where == RPD_DEVICE ? knn_user : s->knn_user.as<int>();
   const int tb = 256;
   k_knn_to_user<<<int((nk + tb - 1) / tb), tb, 0, st>>>(s->knn.as<unsigned>(), s->perm.as<int>(),
@@ -596,7 +641,7 @@ int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *pp, doub
   const int n = s->n;
   if ((e = s->out.ensure(sizeof(double4) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc out");
   if ((e = s->status.ensure(sizeof(int) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc status");
-  if ((e = s->knn.ensure(sizeof(unsigned) * p.K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
+  if ((e = s->knn_part.ensure(sizeof(unsigned) * p.K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
   DevBuf tr, id;
   if ((e = tr.ensure(sizeof(double) * (1 + size_t(cap) * kTraceRecord))) != cudaSuccess)
     return map_cuda(ctx, e, "alloc trace");
@@ -607,12 +652,12 @@ int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *pp, doub
   cudaMemcpyAsync(id.ptr, &sid, sizeof(int), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(tr.ptr, 0, sizeof(double), st);
   e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, id.as<int>(), 1, p.K,
-                 s->ring_bound.as<float>(), s->knn.as<unsigned>(), nullptr, st);
+                 s->ring_bound.as<float>(), s->knn_part.as<unsigned>(), nullptr, st);
   if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
   CellLaunch a;
   a.stored = s->stored.as<float4>();
   a.n = n;
-  a.knn = s->knn.as<unsigned>();
+  a.knn = s->knn_part.as<unsigned>();
   a.K = p.K;
   a.ids = id.as<int>();
   a.num = 1;

@@ -58,10 +58,13 @@ struct rpd_solver {
   rpd::DevBuf stored;          // float4[n] stored (binned) order
   rpd::DevBuf perm;            // int[n] stored -> user
   rpd::DevBuf user_to_stored;  // int[n]
+  rpd::DevBuf weights;         // float[n]: staging for rpd_solver_set_weights
   rpd::DevBuf counters;        // int[dim^3+1]
   rpd::DevBuf bin_ws;
   rpd::DevBuf ring_bound;      // float[dim+2]
-  rpd::DevBuf knn;             // unsigned[n*K]
+  rpd::DevBuf knn;             // unsigned[n*K]: every cell's neighbours (stored ids)
+  int knn_full_K = 0;          // K of the table in knn for all n cells (0: none)
+  rpd::DevBuf knn_part;        // unsigned[num*K]: rows of a retry pass or a trace
   rpd::DevBuf knn_user;        // int[n*K]
   rpd::DevBuf counter64;       // unsigned long long[RPD_CTR_NUM + 1]
   // domain on the device

@@ -61,6 +61,7 @@ def lib():
         for name in ("rpd_solver_num_points", "rpd_solver_bin_dim"):
             getattr(L, name).argtypes = [C.c_void_p]
         L.rpd_solver_set_points.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.rpd_solver_set_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_get_permutation.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_knn.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_float)]
         L.rpd_grid_create.restype = C.c_void_p
@@ -202,6 +203,15 @@ class Solver:
     def set_points(self, xyzw):
         x = as_xyzw(xyzw)
         self.ctx.check(lib().rpd_solver_set_points(self.h, _ptr(x), len(x), RPD_HOST))
+        return self
+
+    def set_weights(self, w):
+        """Weight-only re-solve setup: new weights (user order) for the seeds
+        already set; bins and the last neighbour table (same K) are kept."""
+        w = np.ascontiguousarray(w, np.float32)
+        if w.shape != (self.n,):
+            raise ValueError(f"expected {self.n} weights, got shape {w.shape}")
+        self.ctx.check(lib().rpd_solver_set_weights(self.h, _ptr(w), RPD_HOST))
         return self
 
     @property

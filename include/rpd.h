@@ -87,6 +87,13 @@ int rpd_solver_num_points(const rpd_solver *s);
 int rpd_solver_bin_dim(const rpd_solver *s);
 /* KNearests::getPermutation: perm[stored index] = user index, n ints. */
 int rpd_solver_get_permutation(rpd_solver *s, int *perm, rpd_mem where);
+/* New weights (n floats, user order) for the seeds already set, without
+   re-binning: a weight-only re-solve (Lloyd / optimal-transport iterations).
+   The neighbour table of the last launch with the same K is reused, since
+   the reference's neighbours ignore weights (knearests.cl:36-78).  No
+   counterpart in the reference, which re-uploads all seeds
+   (voronoi.cpp:1088-1107). */
+int rpd_solver_set_weights(rpd_solver *s, const float *w, rpd_mem where);
 /* KNearests::buildKnearests for every seed (knearests.cpp:238-315): the K
  * nearest other seeds, ascending distance, ties by stored index, written as
  * USER indices (-1 where fewer than K exist), n*K ints in user order. */

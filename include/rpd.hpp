@@ -173,6 +173,10 @@ class VoroAlgo {
   void setInputPoints(std::vector<float> const &seeds) {
     rpd_solver_set_points(s_, seeds.data(), int(seeds.size() / 4), RPD_HOST);
   }
+  // Weight-only re-solve (no counterpart in the reference): new weights,
+  // one per seed in the order given to setInputPoints; bins and neighbours
+  // are kept.
+  void setWeights(std::vector<float> const &w) { rpd_solver_set_weights(s_, w.data(), RPD_HOST); }
   int getNumInputPoints() const { return rpd_solver_num_points(s_); }
   int getNumOutputPoints() const { return rpd_solver_num_points(s_); }
   std::vector<double> getBarycenters() const {
