@@ -3,11 +3,52 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "engine.cuh"
 
 namespace rpd {
+
+namespace {
+constexpr int kMaxDev = 64;
+std::mutex g_alloc_mu;
+cudaStream_t g_alloc_stream[kMaxDev] = {};
+
+cudaError_t alloc_stream(cudaStream_t *out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_alloc_mu);
+  if (!g_alloc_stream[dev]) {
+    // keep freed blocks in the pool instead of returning them at every
+    // synchronization
+    cudaMemPool_t pool;
+    if ((e = cudaDeviceGetDefaultMemPool(&pool, dev)) != cudaSuccess) return e;
+    unsigned long long keep = ~0ull;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    if ((e = cudaStreamCreateWithFlags(&g_alloc_stream[dev], cudaStreamNonBlocking)) != cudaSuccess) return e;
+  }
+  *out = g_alloc_stream[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t pool_alloc(void **p, size_t bytes) {
+  cudaStream_t st;
+  cudaError_t e = alloc_stream(&st);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMallocAsync(p, bytes, st)) != cudaSuccess) return e;
+  // usable from every stream once the allocation stream has reached it
+  return cudaStreamSynchronize(st);
+}
+
+void pool_free(void *p) {
+  cudaStream_t st;
+  if (alloc_stream(&st) == cudaSuccess) cudaFreeAsync(p, st);
+}
+
 
 namespace {
 thread_local std::string g_cuda_error;
@@ -691,3 +732,53 @@ int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st) {
 }
 
 }  // extern "C"
+
+namespace rpd {
+
+// Runs a solver on another context's stream (no work of the solver may be
+// pending).
+void solver_rebind(rpd_solver *s, rpd_context *ctx) { s->ctx = ctx; }
+
+// Uses another solver's device grid without a copy (that solver must
+// outlive this one).
+void solver_share_grid(rpd_solver *dst, const rpd_solver *src) {
+  dst->g_flags.release();
+  dst->g_points.release();
+  dst->g_tris.release();
+  dst->g_list.release();
+  dst->g_offsets.release();
+  dst->g_sat.release();
+  dst->grid = src->grid;
+}
+
+// Releases what only a call in progress needs (binning workspace,
+// failing-id lists, parked cells, staging); the seeds, bins, neighbour
+// table and results stay.
+void solver_trim(rpd_solver *s) {
+  s->bin_ws.release();
+  s->knn_part.release();
+  s->knn_user.release();
+  s->ids_a.release();
+  s->ids_b.release();
+  s->ids_c.release();
+  s->fail_ws.release();
+  s->gather.release();
+  s->weights.release();
+  s->defer_slots.release();
+  s->defer_part.release();
+  s->defer_fail.release();
+  s->defer_ctr.release();
+}
+
+size_t solver_device_bytes(const rpd_solver *s) {
+  const DevBuf *b[] = {&s->user, &s->stored, &s->perm, &s->user_to_stored, &s->weights, &s->counters, &s->bin_ws,
+                       &s->ring_bound, &s->knn, &s->knn_part, &s->knn_user, &s->counter64, &s->g_flags, &s->g_points,
+                       &s->g_tris, &s->g_list, &s->g_offsets, &s->g_sat, &s->out, &s->status, &s->ids_a, &s->ids_b,
+                       &s->ids_c, &s->fail_ws, &s->hist, &s->gather, &s->defer_slots, &s->defer_part, &s->defer_fail,
+                       &s->defer_ctr};
+  size_t t = 0;
+  for (const DevBuf *x : b) t += x->bytes;
+  return t;
+}
+
+}  // namespace rpd

@@ -12,6 +12,15 @@
 namespace rpd {
 
 // Owning device allocation that only grows.
+// Device memory comes from the stream-ordered pool of the current device,
+// through one allocation stream per device: allocating and freeing never
+// synchronize the device, so solvers on other streams keep running (the
+// serving loop depends on it).  A buffer is grown or released only when no
+// work that uses it is pending: every entry point of the engine ends with a
+// synchronization of its stream.
+cudaError_t pool_alloc(void **p, size_t bytes);
+void pool_free(void *p);
+
 struct DevBuf {
   void *ptr = nullptr;
   size_t bytes = 0;
@@ -20,15 +29,16 @@ struct DevBuf {
   DevBuf &operator=(const DevBuf &) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) pool_free(ptr);
     ptr = nullptr;
     bytes = 0;
   }
   cudaError_t ensure(size_t want) {
     if (want <= bytes && ptr) return cudaSuccess;
     release();
-    cudaError_t e = cudaMalloc(&ptr, want ? want : 16);
+    cudaError_t e = pool_alloc(&ptr, want ? want : 16);
     if (e == cudaSuccess) bytes = want ? want : 16;
+    else ptr = nullptr;
     return e;
   }
   template <class T>
@@ -83,3 +93,11 @@ struct rpd_solver {
   bool inner_apex = true;      // cone apex at a grid corner inside the cell
   rpd_stats stats{};
 };
+
+namespace rpd {
+// Hooks of the serving loop (csrc/server.cu).
+void solver_rebind(rpd_solver *s, rpd_context *ctx);
+void solver_share_grid(rpd_solver *dst, const rpd_solver *src);
+size_t solver_device_bytes(const rpd_solver *s);
+void solver_trim(rpd_solver *s);
+}  // namespace rpd

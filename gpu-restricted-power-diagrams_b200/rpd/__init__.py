@@ -61,6 +61,16 @@ def lib():
         for name in ("rpd_solver_num_points", "rpd_solver_bin_dim"):
             getattr(L, name).argtypes = [C.c_void_p]
         L.rpd_solver_set_points.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.rpd_server_create.restype = C.c_void_p
+        L.rpd_server_create.argtypes = [C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_int)]
+        L.rpd_server_destroy.argtypes = [C.c_void_p]
+        L.rpd_server_submit_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.POINTER(C.c_int)]
+        L.rpd_server_submit_reweight.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.rpd_server_wait.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.rpd_server_release.argtypes = [C.c_void_p, C.c_int]
+        L.rpd_server_bytes_in_use.restype = C.c_size_t
+        L.rpd_server_bytes_in_use.argtypes = [C.c_void_p]
         L.rpd_solver_set_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_get_permutation.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_knn.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_float)]
@@ -463,3 +473,88 @@ class VoroAlgo:
 
     def getStats(self) -> dict:
         return self._s.stats()
+
+
+class RequestInfo(C.Structure):
+    """rpd_request_info: outcome and timings of one served request."""
+    _fields_ = [("status", C.c_int), ("session", C.c_int), ("n", C.c_int), ("slot", C.c_int),
+                ("queue_ms", C.c_double), ("latency_ms", C.c_double), ("device_ms", C.c_double),
+                ("npasses", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Server:
+    """The serving loop of include/rpd.h (rpd_server_*): sessions kept on the
+    device, solved and re-solved (weights only) on `slots` concurrent streams,
+    admitted in arrival order within `mem_budget` bytes (0: 90% of the free
+    device memory).  solve()/reweight() return a ticket at once; wait(ticket)
+    returns (moments in user order, request info)."""
+
+    def __init__(self, device: int = 0, slots: int = 4, mem_budget: int = 0):
+        err = C.c_int(0)
+        self.h = lib().rpd_server_create(device, slots, mem_budget, C.byref(err))
+        if not self.h:
+            raise RpdError(err.value, "server create")
+        self._out = {}     # ticket -> moments buffer (kept alive until waited for)
+        self._grids = []   # grids used: they must outlive the server
+
+    def solve(self, xyzw, grid=None, params=None, **kw):
+        """Submits a new session's solve; returns (ticket, session)."""
+        x = as_xyzw(xyzw)
+        p = params if params is not None else Params.default(**kw)
+        out = np.zeros((len(x), 4), np.float64)
+        sess = C.c_int(-1)
+        if grid is not None:
+            self._grids.append(grid)
+        t = lib().rpd_server_submit_solve(self.h, _ptr(x), len(x), grid.h if grid is not None else None,
+                                          C.byref(p), _ptr(out), C.byref(sess))
+        if t < 0:
+            raise RpdError(t, "submit solve")
+        self._out[t] = out
+        return t, sess.value
+
+    def reweight(self, session: int, w, params=None, **kw) -> int:
+        """Submits a weight-only re-solve of a session; returns the ticket."""
+        w = np.ascontiguousarray(w, np.float32)
+        p = params if params is not None else Params.default(**kw)
+        out = np.zeros((len(w), 4), np.float64)
+        t = lib().rpd_server_submit_reweight(self.h, session, _ptr(w), C.byref(p), _ptr(out))
+        if t < 0:
+            raise RpdError(t, "submit reweight")
+        self._out[t] = out
+        return t
+
+    def wait(self, ticket: int):
+        info = RequestInfo()
+        rc = lib().rpd_server_wait(self.h, ticket, C.byref(info))
+        out = self._out.pop(ticket)
+        if rc != RPD_OK:
+            raise RpdError(rc, f"request {ticket}")
+        return out, info.as_dict()
+
+    def release(self, session: int):
+        rc = lib().rpd_server_release(self.h, session)
+        if rc != RPD_OK:
+            raise RpdError(rc, f"release session {session}")
+
+    def bytes_in_use(self) -> int:
+        return lib().rpd_server_bytes_in_use(self.h)
+
+    def close(self):
+        if self.h:
+            lib().rpd_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

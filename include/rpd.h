@@ -214,6 +214,50 @@ int rpd_solver_get_moments(rpd_solver *s, double *out4, rpd_mem where);
 int rpd_solver_get_status(rpd_solver *s, int *status, rpd_mem where);
 int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st);
 
+/* --------------------------------------------------------------- serving */
+
+/* A request loop on one GPU (no counterpart in the reference, which solves
+ * one diagram per process).  A session is one diagram kept on the device:
+ * seeds, bins, neighbour table, results, and a device copy of its grid shared
+ * by every session on the same rpd_grid (which must outlive the server).
+ * Requests -- a new session's solve, or a weight-only re-solve of a session --
+ * are admitted in arrival order as one of `slots` concurrent streams and
+ * device memory free up: resident sessions plus the requests in flight stay
+ * within mem_budget bytes (0: 90% of the free memory).  A session runs one
+ * request at a time; requests of different sessions overlap on the device.
+ * A request's result depends only on its own inputs. */
+typedef struct rpd_server rpd_server;
+typedef struct rpd_request_info {
+  int status;         /* RPD_OK or the request's error */
+  int session;
+  int n;              /* seeds */
+  int slot;           /* slot that ran it */
+  double queue_ms;    /* submitted -> admitted */
+  double latency_ms;  /* submitted -> done (moments written) */
+  double device_ms;   /* the solve on the device (rpd_stats.total_ms) */
+  int npasses;
+} rpd_request_info;
+
+rpd_server *rpd_server_create(int device, int slots, size_t mem_budget, int *err);
+/* Waits for every submitted request, then frees everything. */
+void rpd_server_destroy(rpd_server *sv);
+/* A new session: the seeds (xyzw, host memory) are copied; when the request
+ * is done its moments (4n doubles, user order) are in `moments`, which the
+ * caller keeps valid until then (may be NULL).  Returns a ticket >= 0 or an
+ * error < 0, and the session id in *session. */
+int rpd_server_submit_solve(rpd_server *sv, const float *xyzw, int n, const rpd_grid *grid, const rpd_params *p,
+                            double *moments, int *session);
+/* A weight-only re-solve of a session: n weights (host memory, user order),
+ * copied; runs after the session's earlier requests. */
+int rpd_server_submit_reweight(rpd_server *sv, int session, const float *w, const rpd_params *p, double *moments);
+/* Blocks until the ticket's request is done and returns its status; each
+ * ticket is waited for once. */
+int rpd_server_wait(rpd_server *sv, int ticket, rpd_request_info *info);
+/* Frees a session once its requests are done. */
+int rpd_server_release(rpd_server *sv, int session);
+/* Device bytes held by resident sessions, grids and admitted requests. */
+size_t rpd_server_bytes_in_use(rpd_server *sv);
+
 /* Debugging: re-runs one seed's cell (user id) with the caps of `p` and
  * records every clip and integration into `records` (cap records of 12
  * doubles: kind 0 seed, 1 plane test, 2 cavity, 3 vertex, 4 integration,

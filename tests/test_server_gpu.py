@@ -1,0 +1,116 @@
+"""The serving loop (rpd_server_*): requests admitted onto concurrent streams
+give the same results as alone, a session's requests run in order, and the
+memory budget serializes requests that do not fit together."""
+import numpy as np
+import pytest
+
+from seeds_util import jittered, uniform
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rpd():
+    import rpd as m
+
+    m.default_context()
+    return m
+
+
+def workload(rpd):
+    g1 = rpd.Grid.blob(48, 5, 2)
+    g2 = rpd.Grid.blob(32, 5, 9)
+    sets = [
+        (jittered(30, seed=1, weights=True), g1, dict(K=50, P=30, V=40, T=100)),
+        (uniform(20000, seed=2), g2, dict(K=70, P=30, V=40, T=100)),
+        (jittered(20, seed=3, weights=True), None, dict(K=20, P=25, V=30)),
+        (jittered(26, seed=4, weights=True), g1, dict(K=50, P=30, V=40, T=100)),
+    ]
+    rng = np.random.default_rng(5)
+    reweights = []
+    for i, (x, g, kw) in enumerate(sets):
+        h = 1000.0 / round(len(x) ** (1 / 3))
+        for _ in range(2):
+            w = np.clip(x[:, 3] + rng.normal(0, 0.05 * h * h, len(x)), 0, None).astype(np.float32)
+            reweights.append((i, w))
+    return (g1, g2), sets, reweights
+
+
+def run(rpd, slots, budget, sets, reweights, submit_all):
+    out = {}
+    with rpd.Server(slots=slots, mem_budget=budget) as sv:
+        tickets = []
+        sessions = []
+        for i, (x, g, kw) in enumerate(sets):
+            t, sess = sv.solve(x, grid=g, **kw)
+            sessions.append(sess)
+            tickets.append((("solve", i), t))
+            if not submit_all:
+                out[("solve", i)] = sv.wait(t)
+                tickets.pop()
+        for j, (i, w) in enumerate(reweights):
+            t = sv.reweight(sessions[i], w, **sets[i][2])
+            tickets.append((("reweight", j), t))
+            if not submit_all:
+                out[("reweight", j)] = sv.wait(t)
+                tickets.pop()
+        for key, t in tickets:
+            out[key] = sv.wait(t)
+        for s in sessions:
+            sv.release(s)
+    return out
+
+
+def test_results_same_alone_and_in_the_mix(rpd):
+    grids, sets, reweights = workload(rpd)
+    alone = run(rpd, 1, 0, sets, reweights, submit_all=False)
+    mix = run(rpd, 4, 0, sets, reweights, submit_all=True)
+    assert set(alone) == set(mix)
+    slots = set()
+    for key in alone:
+        a, ia = alone[key]
+        m, im = mix[key]
+        assert ia["status"] == 0 and im["status"] == 0
+        assert np.array_equal(a, m), key
+        slots.add(im["slot"])
+    assert len(slots) > 1  # the mix ran on several streams
+    # and a plain solver agrees with the served results
+    for i, (x, g, kw) in enumerate(sets):
+        s = rpd.Solver().set_points(x)
+        if g is not None:
+            s.set_grid(g)
+        s.launch(**kw)
+        assert np.array_equal(s.moments(), alone[("solve", i)][0])
+    # re-solves: the last weights of each session, solved from scratch
+    last = {}
+    for j, (i, w) in enumerate(reweights):
+        last[i] = (j, w)
+    for i, (j, w) in last.items():
+        x, g, kw = sets[i]
+        x2 = x.copy()
+        x2[:, 3] = w
+        s = rpd.Solver().set_points(x2)
+        if g is not None:
+            s.set_grid(g)
+        s.launch(**kw)
+        assert np.array_equal(s.moments(), mix[("reweight", j)][0])
+
+
+def test_tiny_budget_runs_one_request_at_a_time(rpd):
+    grids, sets, reweights = workload(rpd)
+    out = run(rpd, 4, 1, sets[:3], [], submit_all=True)
+    spans = sorted((i["queue_ms"], i["latency_ms"]) for _, i in out.values())
+    for (a0, d0), (a1, d1) in zip(spans, spans[1:]):
+        assert a1 >= d0 - 0.5  # admitted after the previous one finished (ms, submit-relative)
+
+
+def test_failed_request_reports_error(rpd):
+    with rpd.Server(slots=2) as sv:
+        t, sess = sv.solve(jittered(10, seed=1), K=0)
+        with pytest.raises(rpd.RpdError):
+            sv.wait(t)
+        with pytest.raises(rpd.RpdError):
+            sv.reweight(sess, np.zeros(1000, np.float32))
+        t2, s2 = sv.solve(jittered(10, seed=1), K=20)
+        m, info = sv.wait(t2)
+        assert info["status"] == 0 and abs(m[:, 3].sum() / 1e9 - 1) < 1e-6
