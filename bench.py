@@ -37,6 +37,15 @@ CONFIGS = {
     "voronoi-100k": dict(kind="uniform", n=100_000, weights=False, grid="blob", gsize=100, nell=5, gseed=2,
                          sseed=1, K=70, P=30, V=40, T=100,
                          desc="100K i.i.d. uniform seeds (weights 0), 5-ellipsoid blob at 100^3, K=70 P=30 V=40"),
+    # a serving loop (one GPU)
+    "serve-200rps": dict(kind="serve", rate=200.0, requests=600, nmin=10_000, nmax=2_000_000, reweight=0.3,
+                         grid="blob", gsizes=(48, 64, 96, 128, 160, 200), nell=5, gseed=2, sseed=5, K=50, P=30, V=40,
+                         T=100, slots=4, resident=24,
+                         desc="Poisson arrivals at 200/s, 600 requests: 70% new diagrams of N log-uniform in "
+                              "[10K, 2M] i.i.d. uniform seeds with weights U[0, 0.1h^2], 30% weight-only re-solves "
+                              "of a resident diagram (w += N(0, (0.01 h^2)^2)); the 5-ellipsoid blob voxelized at "
+                              "S^3, S in {48,64,96,128,160,200} nearest 2 N^(1/3) (cells about 2 voxels across, as "
+                              "in the 1M config), K=50 P=30 V=40 T=100, 4 slots, at most 24 resident diagrams"),
 }
 
 
@@ -330,6 +339,121 @@ def run_ours(args, cfg, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_serve(args, cfg, rank):
+    """Serving loop: requests arrive by a seeded Poisson process and are
+    submitted at their arrival times; the server's own clock gives each
+    request's latency (submitted -> moments on the host).  Sustained cells/s
+    = cells of all requests / (first arrival -> last completion)."""
+    import threading
+
+    import numpy as np
+
+    import rpd
+
+    if rank != 0:
+        return
+    rng = np.random.default_rng(cfg["sseed"])
+    grids = {S: rpd.Grid.blob(S, cfg["nell"], cfg["gseed"]) for S in cfg["gsizes"]}
+    vols = {S: g.getVolume() for S, g in grids.items()}
+
+    def grid_for(n):
+        S = min(cfg["gsizes"], key=lambda x: abs(x - 2.0 * n ** (1 / 3)))
+        return S, grids[S]
+    pool = np.zeros((cfg["nmax"], 4), np.float32)
+    pool[:, :3] = (rng.random((cfg["nmax"], 3)) * 1000.0).astype(np.float32)
+    nreq = cfg["requests"]
+    gaps = rng.exponential(1.0 / cfg["rate"], nreq)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    kw = dict(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"])
+    # warm-up: one solve and one re-solve (allocator pool, grid upload)
+    with rpd.Server(slots=cfg["slots"]) as sv:
+        t, sess = sv.solve(pool[:200_000], grid=grid_for(200_000)[1], **kw)
+        sv.wait(t)
+        sv.wait(sv.reweight(sess, pool[:200_000, 3], **kw))
+        resident = []  # (session, n, weights)
+        tickets = []
+        lock = threading.Lock()
+        done = []
+
+        def waiter():
+            k = 0
+            while True:
+                with lock:
+                    if k < len(tickets):
+                        item = tickets[k]
+                    elif k >= nreq:
+                        return
+                    else:
+                        item = None
+                if item is None:
+                    time.sleep(0.0005)
+                    continue
+                kind, t, n = item
+                try:
+                    out, info = sv.wait(t)
+                    err = abs(out[:, 3].sum() / vols[grid_for(n)[0]] - 1.0)
+                except rpd.RpdError as exc:
+                    info, err = {"latency_ms": float("nan"), "device_ms": float("nan"), "failed_cells": n,
+                                 "error": str(exc)}, float("nan")
+                done.append((kind, n, info, err, time.perf_counter()))
+                k += 1
+
+        th = threading.Thread(target=waiter)
+        t0 = time.perf_counter()
+        th.start()
+        for i in range(nreq):
+            now = time.perf_counter() - t0
+            if arrivals[i] > now:
+                time.sleep(arrivals[i] - now)
+            if resident and rng.random() < cfg["reweight"]:
+                sess, n, w = resident[rng.integers(len(resident))]
+                h2 = (1000.0 / n ** (1 / 3)) ** 2
+                w += rng.normal(0.0, 0.01 * h2, n).astype(np.float32)
+                np.maximum(w, 0.0, out=w)
+                t = sv.reweight(sess, w, **kw)
+                item = ("reweight", t, n)
+            else:
+                n = int(np.exp(rng.uniform(np.log(cfg["nmin"]), np.log(cfg["nmax"]))))
+                x = pool[:n].copy()
+                h2 = (1000.0 / n ** (1 / 3)) ** 2
+                x[:, 3] = rng.uniform(0.0, 0.1 * h2, n).astype(np.float32)
+                t, sess = sv.solve(x, grid=grid_for(n)[1], **kw)
+                resident.append((sess, n, x[:, 3].copy()))
+                if len(resident) > cfg["resident"]:
+                    old = resident.pop(0)
+                    sv.release(old[0])
+                item = ("solve", t, n)
+            with lock:
+                tickets.append(item)
+        th.join()
+        t_end = max(d[4] for d in done)
+        for sess, _, _ in resident:
+            sv.release(sess)
+    ok = [d for d in done if d[2]["latency_ms"] == d[2]["latency_ms"]]
+    failed = [d[2]["error"] for d in done if d not in ok]
+    lat = np.array([d[2]["latency_ms"] for d in ok])
+    dev = np.array([d[2]["device_ms"] for d in ok])
+    cells = sum(d[1] for d in ok)
+    span = t_end - t0
+    clean = [d[3] for d in ok if d[2]["failed_cells"] == 0]
+    errs = max(clean) if clean else None
+    rw = [d for d in ok if d[0] == "reweight"]
+    line = {
+        "metric": "served cells/s and p50/p99 latency (config 5)", "value": cells / span, "unit": "cells/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f64 geometry on f32 seeds", "data": "synthetic",
+        "config": {"workload": "serve-200rps", "description": cfg["desc"], "slots": cfg["slots"]},
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "p50_reweight_ms": float(np.percentile([d[2]["latency_ms"] for d in rw], 50)) if rw else None,
+        "p50_device_ms": float(np.percentile(dev, 50)), "requests": len(done), "reweights": len(rw),
+        "offered_cells_per_s": cells / max(arrivals[-1], 1e-9), "span_s": span,
+        "max_total_mass_rel_err_vs_grid_volume": errs,
+        "requests_failed": len(failed), "first_failure": failed[0] if failed else None,
+        "requests_with_failed_cells": sum(1 for d in ok if d[2]["failed_cells"] > 0),
+        "failed_cells": int(sum(d[2]["failed_cells"] for d in ok)),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -342,7 +466,13 @@ def main():
     args = ap.parse_args()
     rank, world, local = dist_env()
     cfg = CONFIGS[args.config]
-    if args.impl == "reference":
+    if cfg.get("kind") == "serve":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop"}))
+            return
+        run_serve(args, cfg, rank)
+    elif args.impl == "reference":
         run_reference(args, cfg, rank, world)
     else:
         run_ours(args, cfg, rank, world, local)

@@ -32,6 +32,10 @@
 // is reduced across the warp.
 #include <algorithm>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "cell.cuh"
 
 namespace rpd {
@@ -1841,6 +1845,27 @@ __global__ void k_cone_finish(CellLaunch a) {
                    : make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
+// Raises a kernel's dynamic shared memory limit to the device's opt-in
+// maximum, once per kernel and device.  The limit is process-wide: set per
+// launch to the launch's own size, a launch on another thread could lower it
+// between this thread's setting and its launch (the serving loop runs
+// launches from several threads).
+cudaError_t allow_smem(const void *fn, size_t smem) {
+  static std::mutex mu;
+  static std::set<std::pair<const void *, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int optin = 0;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+  if (smem > size_t(optin)) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({fn, dev})) return cudaSuccess;
+  if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) != cudaSuccess) return e;
+  done.insert({fn, dev});
+  return cudaSuccess;
+}
+
 template <int VS>
 cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int sm_count, int *launches) {
   const int warps_per_block = 4;
@@ -1849,21 +1874,21 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
   cudaError_t e;
   if (a.grid.size > 0 && a.defer.slots) {
     // every boundary cell parks; the chunked kernel does the triangles
-    e = cudaFuncSetAttribute(k_cell<VS, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, false>), smem);
     if (e != cudaSuccess) return e;
     k_cell<VS, true, false><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
-    e = cudaFuncSetAttribute(k_cone<VS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    e = allow_smem(reinterpret_cast<const void *>(k_cone<VS>), smem);
     if (e != cudaSuccess) return e;
     k_cone<VS><<<sm_count * 4, warps_per_block * 32, smem, st>>>(a, L);
     k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a);
     if (launches) *launches += 3;
   } else if (a.grid.size > 0) {
-    e = cudaFuncSetAttribute(k_cell<VS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, true>), smem);
     if (e != cudaSuccess) return e;
     k_cell<VS, true, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (launches) ++*launches;
   } else {
-    e = cudaFuncSetAttribute(k_cell<VS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, false, true>), smem);
     if (e != cudaSuccess) return e;
     k_cell<VS, false, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (launches) ++*launches;

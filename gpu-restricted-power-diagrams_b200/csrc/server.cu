@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -112,6 +113,7 @@ struct rpd_server {
   size_t inflight = 0;  // admitted requests
   int next_ticket = 0, next_session = 0;
   bool stop = false;
+  Clock::time_point created = Clock::now();
 
   // The first queued request that may run now, or null (mu held).  A new
   // session whose memory does not fit holds back the new sessions behind it
@@ -229,8 +231,15 @@ struct rpd_server {
         r->info.slot = slot;
         r->info.queue_ms = ms_between(r->submitted, r->admitted);
         r->info.latency_ms = ms_between(r->submitted, r->done);
+        r->info.admitted_at_ms = ms_between(created, r->admitted);
+        r->info.done_at_ms = ms_between(created, r->done);
         r->info.device_ms = st.total_ms;
         r->info.npasses = st.npasses;
+        r->info.failed_cells = rc == RPD_OK ? r->n - st.status_hist[RPD_SUCCESS] - st.status_hist[RPD_EMPTY_CELL] : r->n;
+        if (rc != RPD_OK) {
+          const char *msg = rpd_context_error(c);
+          std::snprintf(r->info.error, sizeof(r->info.error), "%s", msg ? msg : "");
+        }
         r->finished = true;
         std::vector<float>().swap(r->data);
         if (s->released && s->pending == 0) drop_session(s);

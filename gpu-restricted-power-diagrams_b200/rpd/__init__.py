@@ -479,10 +479,13 @@ class RequestInfo(C.Structure):
     """rpd_request_info: outcome and timings of one served request."""
     _fields_ = [("status", C.c_int), ("session", C.c_int), ("n", C.c_int), ("slot", C.c_int),
                 ("queue_ms", C.c_double), ("latency_ms", C.c_double), ("device_ms", C.c_double),
-                ("npasses", C.c_int)]
+                ("npasses", C.c_int), ("admitted_at_ms", C.c_double), ("done_at_ms", C.c_double),
+                ("failed_cells", C.c_int), ("error", C.c_char * 160)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["error"] = self.error.decode(errors="replace")
+        return d
 
 
 class Server:
@@ -531,7 +534,7 @@ class Server:
         rc = lib().rpd_server_wait(self.h, ticket, C.byref(info))
         out = self._out.pop(ticket)
         if rc != RPD_OK:
-            raise RpdError(rc, f"request {ticket}")
+            raise RpdError(rc, f"request {ticket}: {info.error.decode(errors='replace')}")
         return out, info.as_dict()
 
     def release(self, session: int):

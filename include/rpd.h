@@ -236,6 +236,10 @@ typedef struct rpd_request_info {
   double latency_ms;  /* submitted -> done (moments written) */
   double device_ms;   /* the solve on the device (rpd_stats.total_ms) */
   int npasses;
+  double admitted_at_ms;  /* since the server was created */
+  double done_at_ms;      /* since the server was created */
+  int failed_cells;   /* cells whose final status is neither success nor empty */
+  char error[160];    /* the context's error text when status != RPD_OK */
 } rpd_request_info;
 
 rpd_server *rpd_server_create(int device, int slots, size_t mem_budget, int *err);
