@@ -203,6 +203,21 @@ def run_reference(args, cfg, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def aggregate_over_ranks(ms, e2e_s, n, world, device):
+    """Whole-job numbers of one timed run: each rank solved its own n-seed
+    diagram; the job's step time is the slowest rank's (max over ranks), and
+    the throughput counts the cells of all ranks.  Returns (ms, e2e_s,
+    cells_per_s, e2e_cells_per_s)."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(t[0].item()), float(t[1].item())
+    return ms, e2e_s, n * world / (ms / 1e3), n * world / e2e_s
+
+
 def run_ours(args, cfg, rank, world, local):
     import torch
 
@@ -257,13 +272,6 @@ def run_ours(args, cfg, rank, world, local):
     solver.launch(rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_COUNTERS))
     work = solver.stats()["counters"]
     ms = sum(step_ms) / len(step_ms)
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n * world / (ms / 1e3)
 
     # end to end through the C ABI from pinned host memory: binning upload,
     # solve, moments download, every step
@@ -281,10 +289,7 @@ def run_ours(args, cfg, rank, world, local):
         ctx.check(rpd.lib().rpd_solver_get_moments(solver.h, rpd._ptr(oa), rpd.RPD_HOST))
         e2e_s.append(time.perf_counter() - t0)
     e2e_t = sum(e2e_s) / len(e2e_s)
-    if world > 1:
-        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda")
 
     # roofline of the dominant kernel (the cell kernel of the first pass):
     # minimal DRAM bytes per launch = the neighbour table and the seeds read
@@ -314,7 +319,7 @@ def run_ours(args, cfg, rank, world, local):
         "config": {"workload": args.config, "description": cfg["desc"], "n_seeds_per_gpu": n,
                    "parallelism": f"{world} independent diagrams, one per GPU",
                    "l2": "flushed between steps (256 MB write, untimed)"},
-        "e2e": {"value": n * world / e2e_t, "unit": "cells/s", "h2d_bytes_per_step": int(x.nbytes),
+        "e2e": {"value": e2e_value, "unit": "cells/s", "h2d_bytes_per_step": int(x.nbytes),
                 "d2h_bytes_per_step": int(n * 32),
                 "path": "rpd_solver_set_points(host) + rpd_solver_launch + rpd_solver_get_moments(host)"},
         "gpu_launches": int(sum(launches)),
