@@ -1877,6 +1877,7 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
     e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, false>), smem);
     if (e != cudaSuccess) return e;
     k_cell<VS, true, false><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    if (a.after_cell) cudaEventRecord(a.after_cell, st);
     e = allow_smem(reinterpret_cast<const void *>(k_cone<VS>), smem);
     if (e != cudaSuccess) return e;
     k_cone<VS><<<sm_count * 4, warps_per_block * 32, smem, st>>>(a, L);
@@ -1886,11 +1887,13 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
     e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, true>), smem);
     if (e != cudaSuccess) return e;
     k_cell<VS, true, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    if (a.after_cell) cudaEventRecord(a.after_cell, st);
     if (launches) ++*launches;
   } else {
     e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, false, true>), smem);
     if (e != cudaSuccess) return e;
     k_cell<VS, false, true><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    if (a.after_cell) cudaEventRecord(a.after_cell, st);
     if (launches) ++*launches;
   }
   return cudaGetLastError();

@@ -76,6 +76,7 @@ struct CellLaunch {
   int trace_cap = 0;  // records
   DeferQueue defer;   // slots == null: every boundary cell inline
   int only_status = -1;  // >= 0: process only the rows whose status equals it
+  cudaEvent_t after_cell = nullptr;  // recorded after the cell kernel, before the cone kernels
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
 constexpr int kTraceRecord = 12;

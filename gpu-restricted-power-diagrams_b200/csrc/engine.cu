@@ -185,9 +185,9 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   // all cells with this K is kept across weight-only re-solves
   const bool all_cells = ids == nullptr && num == s->n;
   rpd::DevBuf &kb = all_cells ? s->knn : s->knn_part;
-  const bool reuse = all_cells && s->knn_full_K == K && !counters;
+  const bool reuse = all_cells && s->knn_full_K == K && !counters && !s->fresh_knn;
   if ((e = kb.ensure(sizeof(unsigned) * size_t(num) * K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
-  cudaEvent_t ev[3];
+  cudaEvent_t ev[4];
   for (auto &x : ev) cudaEventCreate(&x);
   unsigned long long *ctr = counters ? s->counter64.as<unsigned long long>() : nullptr;
   cudaEventRecord(ev[0], st);
@@ -218,6 +218,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.status = s->status.as<int>();
   a.out = s->out.as<double4>();
   a.counters = ctr;
+  a.after_cell = ev[3];
   if (s->grid.size > 0 && s->use_defer) {
     // boundary cells with many triangles are parked and their triangles
     // spread over all warps; cells past the capacity stay inline
@@ -249,6 +250,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
       CellLaunch b = a;
       b.defer = DeferQueue();
       b.only_status = kParkOverflow;
+      b.after_cell = nullptr;
       if ((e = cell_launch(b, st, ctx->sm_count, &launches)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
     }
   }
@@ -263,6 +265,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
     S.pass_T[pi] = T;
     cudaEventElapsedTime(&S.pass_knn_ms[pi], ev[0], ev[1]);
     cudaEventElapsedTime(&S.pass_cell_ms[pi], ev[1], ev[2]);
+    if (num > 0) cudaEventElapsedTime(&S.pass_cell_kernel_ms[pi], ev[1], ev[3]);
   }
   for (auto &x : ev) cudaEventDestroy(x);
   S.npasses++;
@@ -590,6 +593,7 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   const bool early = !(p.flags & RPD_FLAG_NO_EARLY_OUT);
   s->use_defer = !(p.flags & RPD_FLAG_NO_DEFER);
   s->inner_apex = !(p.flags & RPD_FLAG_REFERENCE_APEX);
+  s->fresh_knn = (p.flags & RPD_FLAG_FRESH_NEIGHBOURS) != 0;
   int rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
   if (rc != RPD_OK) return rc;
   if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {

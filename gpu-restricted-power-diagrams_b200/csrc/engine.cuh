@@ -91,6 +91,7 @@ struct rpd_solver {
   bool have_results = false;
   bool use_defer = true;       // park heavy boundary cells for the chunked kernel
   bool inner_apex = true;      // cone apex at a grid corner inside the cell
+  bool fresh_knn = false;      // recompute the neighbour table at this launch
   rpd_stats stats{};
 };
 

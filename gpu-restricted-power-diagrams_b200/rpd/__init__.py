@@ -111,6 +111,7 @@ FLAG_COUNTERS = 2
 FLAG_NO_EARLY_OUT = 4
 FLAG_NO_DEFER = 8
 FLAG_REFERENCE_APEX = 16
+FLAG_FRESH_NEIGHBOURS = 32
 COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
                  "exports", "export_vertices", "outside_early", "cone_empty", "cones_skipped"]
 
@@ -135,14 +136,15 @@ class Stats(C.Structure):
                 ("pass_P", C.c_int * 8), ("pass_V", C.c_int * 8), ("pass_T", C.c_int * 8),
                 ("pass_knn_ms", C.c_float * 8), ("pass_cell_ms", C.c_float * 8), ("status_hist", C.c_int * 11),
                 ("counters", C.c_ulonglong * 11), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
-                ("kernel_launches", C.c_int)]
+                ("kernel_launches", C.c_int), ("pass_cell_kernel_ms", C.c_float * 8)]
 
     def as_dict(self):
         n = self.npasses
         return {
             "npasses": n,
             "passes": [{"cells": self.pass_cells[i], "K": self.pass_K[i], "P": self.pass_P[i], "V": self.pass_V[i],
-                        "T": self.pass_T[i], "knn_ms": self.pass_knn_ms[i], "cell_ms": self.pass_cell_ms[i]}
+                        "T": self.pass_T[i], "knn_ms": self.pass_knn_ms[i], "cell_ms": self.pass_cell_ms[i],
+                        "cell_kernel_ms": self.pass_cell_kernel_ms[i]}
                        for i in range(min(n, 8))],
             "status": {STATUS_NAMES[i]: v for i, v in enumerate(self.status_hist) if v},
             "counters": {COUNTER_NAMES[i]: int(v) for i, v in enumerate(self.counters)},

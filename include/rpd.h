@@ -149,6 +149,9 @@ rpd_grid *rpd_grid_make_cube(int size, int *err);
 #define RPD_FLAG_REFERENCE_APEX 16u /* cone apex at the reference's start corner for
                                        every cell, with all triangles of its voxels
                                        (same results up to rounding, slower) */
+#define RPD_FLAG_FRESH_NEIGHBOURS 32u /* recompute the neighbour table even when the
+                                         seeds' positions and K are unchanged since
+                                         the last launch (same results) */
 
 /* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
 typedef struct rpd_params {
@@ -194,6 +197,7 @@ typedef struct rpd_stats {
   unsigned long long knn_candidates;
   float total_ms;                  /* device time of the whole launch */
   int kernel_launches;             /* device kernels this launch ran */
+  float pass_cell_kernel_ms[8];    /* of pass_cell_ms: the cell kernel alone (no cone kernels) */
 } rpd_stats;
 
 /* VoroAlgo::setGrid (voronoi.cpp:1079-1082): uploads the domain; null

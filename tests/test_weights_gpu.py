@@ -71,3 +71,16 @@ def test_set_weights_rejects_wrong_length(rpd):
     s = rpd.Solver().set_points(jittered(8, seed=1))
     with pytest.raises(ValueError):
         s.set_weights(np.zeros(7, np.float32))
+
+
+def test_fresh_neighbours_flag_recomputes_the_table(rpd):
+    x = jittered(20, seed=4, weights=True)
+    s = rpd.Solver().set_points(x)
+    s.launch(K=30, P=30, V=40)
+    m0 = s.moments()
+    s.launch(K=30, P=30, V=40)
+    reused = s.stats()["passes"][0]["knn_ms"]
+    s.launch(K=30, P=30, V=40, flags=rpd.FLAG_FRESH_NEIGHBOURS)
+    fresh = s.stats()["passes"][0]["knn_ms"]
+    assert fresh > reused
+    assert np.array_equal(s.moments(), m0)
