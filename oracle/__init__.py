@@ -41,6 +41,7 @@ class OracleParams(C.Structure):
         ("vhs0", C.c_int), ("vhs1", C.c_int), ("use_double", C.c_int), ("kernels", C.c_int),
         ("knn_mode", C.c_int), ("max_extra_passes", C.c_int), ("first_pass_only", C.c_int),
         ("cube_eps", C.c_double), ("nthreads", C.c_int), ("sample_stride", C.c_int),
+        ("used_cells", C.c_int), ("keep_distance", C.c_int), ("keep_volume", C.c_double),
     ]
 
 
@@ -134,6 +135,37 @@ def solve(xyzw, grid=None, K=20, P=25, V=30, T=100, vhs0=2, vhs1=2, use_double=F
     if rc != 0:
         raise RuntimeError(f"oracle_solve failed: {rc}")
     return (bary, status, st.as_dict()) if return_stats else (bary, status)
+
+
+def solve_used(xyzw, grid, keep_distance=0, keep_volume=0.001, K=20, P=25, V=30, T=100, use_double=True, kernels=0,
+               knn_mode=1, max_extra_passes=5, nthreads=0):
+    """oracle solve with the reference's used cells (voronoi.cpp:1286-1393):
+    returns (bary, status, used), used = per seed (user order) 0 unused, else
+    its ring distance (1: used, or a face neighbour of a used cell)."""
+    x = np.ascontiguousarray(np.asarray(xyzw, dtype=np.float64).reshape(-1, 4))
+    n = len(x)
+    bary = np.zeros((n, 4), np.float64)
+    status = np.zeros(n, np.int32)
+    used = np.zeros(n, np.uint8)
+    prm = OracleParams(K, P, V, T, 2, 2, int(use_double), kernels, knn_mode, max_extra_passes, 0, 0.1, nthreads, 1,
+                       1, keep_distance, keep_volume)
+    gv = grid.view()
+    rc = lib().oracle_solve_used(_ptr(x), n, C.byref(gv), C.byref(prm), _ptr(bary), _ptr(status), _ptr(used), None)
+    if rc != 0:
+        raise RuntimeError(f"oracle_solve_used failed: {rc}")
+    return bary, status, used
+
+
+def compact(bary, used, keep_distance, keep_volume, no_cell_limits=-100000.0):
+    """compact_result (voronoi.cpp:583-625) in ascending user order (the
+    reference's order comes from an atomic counter): the used seeds' rows, with
+    w = NO_CELL_LIMITS for outer-ring cells below keep_volume.  Returns
+    (rows (m,4), perm_to_user (m,))."""
+    keep = np.nonzero(used)[0]
+    rows = bary[keep].copy()
+    border = (rows[:, 3] < keep_volume) & (used[keep] == keep_distance)
+    rows[border, 3] = no_cell_limits
+    return rows, keep.astype(np.int32)
 
 
 def knn(xyzw, K, use_double=False, kernels=0, knn_mode=1, nthreads=0):

@@ -150,6 +150,7 @@ struct Cell {
   Status *status = nullptr;
   std::vector<std::array<uint8_t, 4>> vert;
   std::vector<Vec4<R>> plane;
+  std::vector<int> pnb;  // neighbour seed of each plane, -1 for box and cone planes (ConvexCell.cl:284-330)
   std::vector<uint8_t> next;
   int nb_vertex = 0, nb_plane = 0;
   Counters *cnt = nullptr;
@@ -157,6 +158,7 @@ struct Cell {
   void resize() {
     vert.assign(256, {0, 0, 0, 0});
     plane.assign(std::max(capP, 1) + 4, Vec4<R>{0, 0, 0, 0});
+    pnb.assign(std::max(capP, 1) + 4, -1);
     next.assign(std::max(capP, 1) + 4, 0);
   }
 
@@ -175,6 +177,7 @@ struct Cell {
     plane[3] = mk<R>(R(0.0), R(-1.0), R(0.0), vmax);
     plane[4] = mk<R>(R(0.0), R(0.0), R(1.0), -vmin);
     plane[5] = mk<R>(R(0.0), R(0.0), R(-1.0), vmax);
+    for (int i = 0; i < 6; ++i) pnb[i] = -1;
     nb_plane = 6;
     static const uint8_t cube[8][3] = {{2, 5, 0}, {5, 3, 0}, {1, 5, 2}, {5, 1, 3},
                                        {4, 2, 0}, {4, 0, 3}, {2, 4, 1}, {4, 3, 1}};
@@ -196,6 +199,7 @@ struct Cell {
     if (B.w <= kNoCellLimits) dot = 2 * dot3(B, dir);
     const R dir_norm = std::sqrt(dot3(dir, dir));
     plane[nb_plane] = mk<R>(dir.x / dir_norm, dir.y / dir_norm, dir.z / dir_norm, -dot / 2 / dir_norm);
+    pnb[nb_plane] = int(vid);
     return nb_plane++;
   }
 
@@ -389,6 +393,7 @@ struct Cell {
         *status = plane_overflow;
         return;
       }
+      pnb[nb_plane] = -1;
       plane[nb_plane++] = plane_from_points(faces[f][0], faces[f][1], faces[f][2]);
       clip(nb_plane - 1);
       if (*status != success) return;
@@ -459,10 +464,31 @@ inline bool merge_lists(const int *l1, int n1, const int *l2, int n2, int *res, 
   return true;
 }
 
+// Used cells (ConvexCell.cl:1118-1126, 680-690): relaxed byte accesses, as
+// the reference's concurrent work-items race on the same flags.
+struct UsedCells {
+  uint8_t *flags = nullptr;  // stored order, null: off
+  double eps = 0;            // USED_CELL_EPSILON (keepVolume)
+  int dist = 0;              // CUSED_CELL_DIST of the main passes (0 or 1)
+};
+
+// CCUpdateUsedCell: every plane neighbour of the cell's vertices gets d
+// when it has no mark yet.
+template <class R>
+void mark_neighbours(const Cell<R> &cc, uint8_t *flags, int d) {
+  for (int ve = 0; ve < cc.nb_vertex; ++ve)
+    for (int i = 0; i < 3; ++i) {
+      const int nb = cc.pnb[cc.ith(ve, i)];
+      if (nb >= 0 && __atomic_load_n(&flags[nb], __ATOMIC_RELAXED) == 0)
+        __atomic_store_n(&flags[nb], uint8_t(d), __ATOMIC_RELAXED);
+    }
+}
+
 // compute_voro_cell (ConvexCell.cl:812-1116) for one stored seed.
 template <class R>
 void voro_cell(Cell<R> &cc, int seed_id, const unsigned *neigs, int K, const GridView<R> *grid, bool out_domain,
-               Status *st_all, Vec4<R> *out_all, double vol_eps2, std::vector<int> &tr0, std::vector<int> &tr1) {
+               Status *st_all, Vec4<R> *out_all, double vol_eps2, std::vector<int> &tr0, std::vector<int> &tr1,
+               const UsedCells &used) {
   Status *st = st_all + seed_id;
   *st = success;
   const Vec4<R> *pts = cc.pts;
@@ -635,6 +661,33 @@ void voro_cell(Cell<R> &cc, int seed_id, const unsigned *neigs, int K, const Gri
       restore();
     }
   }
+  if (used.flags && out_all[seed_id].w >= R(used.eps)) {
+    __atomic_store_n(&used.flags[seed_id], uint8_t(1), __ATOMIC_RELAXED);
+    if (used.dist >= 1) mark_neighbours(cc, used.flags, 1);
+  }
+}
+
+// compute_bordering (ConvexCell.cl:756-809): the clipped cell only, then its
+// plane neighbours get the mark d.
+template <class R>
+void border_cell(Cell<R> &cc, int seed_id, const unsigned *neigs, int K, Status *st_all, uint8_t *flags, int d) {
+  Status *st = st_all + seed_id;
+  *st = success;
+  const Vec4<R> *pts = cc.pts;
+  if (pts[seed_id].w <= kNoCellLimits) return;
+  cc.init(seed_id, st);
+  for (int i = 0; i < K; ++i) {
+    const unsigned z = neigs[i];
+    const int cur = cc.new_plane(z);
+    cc.clip(cur);
+    if (*st != success) return;
+    if (cc.radius_reached(pts[z])) break;
+  }
+  if (!cc.radius_reached(pts[neigs[K - 1]])) {
+    *st = security_radius_not_reached;
+    return;
+  }
+  mark_neighbours(cc, flags, d);
 }
 
 // ---------------------------------------------------------------------------
@@ -865,6 +918,8 @@ struct Solver {
   Bins<R> bins;
   std::vector<Status> status;
   std::vector<Vec4<R>> out;
+  std::vector<uint8_t> used;  // used-cell marks (stored order) when keep_distance >= 0 with a grid
+  UsedCells uc;
   OracleStats *stats;
   Counters total;
   // VOLUME_EPSILON2 is a double literal in both builds (voronoi.cpp:919,922).
@@ -918,15 +973,26 @@ struct Solver {
     return true;
   }
 
+  // bordering_d > 0: the bordering kernel (mark d), on a scratch status
   bool cells(const std::vector<int> &ids, const std::vector<unsigned> &nn, int K, int P, int V, int T, int vhs,
-             bool out_domain) {
+             bool out_domain, int bordering_d = 0) {
     const int num = int(ids.size());
     if (!num) return true;
     const double t0 = now_s();
+    std::vector<Status> scratch;
+    Status *st_out = status.data();
+    if (bordering_d > 0) {
+      scratch.assign(status.size(), success);
+      st_out = scratch.data();
+    }
     if (prm.kernels == 1) {
       std::string name = "ref_cell_";
       name += std::is_same<R, double>::value ? std::string("d") : "f" + std::to_string(vhs);
-      name += grid ? (out_domain ? "_gridout" : "_grid") : "_nogrid";
+      if (bordering_d > 0)
+        name += "_border" + std::to_string(bordering_d);
+      else
+        name += grid ? (out_domain ? "_gridout" : "_grid") : "_nogrid";
+      if (bordering_d == 0 && uc.flags) name += "_used" + std::to_string(uc.dist);
       RefCellFn fn = (RefCellFn)ref_sym(name.c_str());
       if (!fn) return false;
       std::vector<unsigned> uids(ids.begin(), ids.end());
@@ -945,14 +1011,16 @@ struct Solver {
         a.grid_size = grid->size;
         a.voxel_size = double(grid->voxel);
       }
-      a.cube_eps = prm.cube_eps;
-      a.status = (int *)status.data();
+      a.cube_eps = bordering_d > 0 ? 0.0 : prm.cube_eps;
+      a.status = (int *)st_out;
       a.out = out.data();
       a.k = K;
       a.p = P;
       a.v = V;
       a.t = T;
       a.nthreads = nthreads();
+      a.used = uc.flags;
+      a.used_eps = uc.eps;
       fn(&a);
     } else {
       const int nth = nthreads();
@@ -971,9 +1039,13 @@ struct Solver {
         cc.resize();
         std::vector<int> tr0(std::max(T, 1) + 1), tr1(std::max(T, 1) + 1);
 #pragma omp for schedule(dynamic, 256)
-        for (int g = 0; g < num; ++g)
-          voro_cell<R>(cc, ids[g], nn.data() + size_t(g) * K, K, grid, out_domain, status.data(), out.data(),
-                       vol_eps2, tr0, tr1);
+        for (int g = 0; g < num; ++g) {
+          if (bordering_d > 0)
+            border_cell<R>(cc, ids[g], nn.data() + size_t(g) * K, K, st_out, uc.flags, bordering_d);
+          else
+            voro_cell<R>(cc, ids[g], nn.data() + size_t(g) * K, K, grid, out_domain, status.data(), out.data(),
+                         vol_eps2, tr0, tr1, uc);
+        }
       }
       for (auto &c : cs) {
         total.hs += c.hs;
@@ -989,7 +1061,7 @@ struct Solver {
 
   // VoroAlgoComputeData::launch (voronoi.cpp:861-1036): one pass = kNN of the
   // ids with this pass's K, then the cell kernel.
-  bool pass(const std::vector<int> &ids, int K, int P, int V, int T, int vhs, bool out_domain) {
+  bool pass(const std::vector<int> &ids, int K, int P, int V, int T, int vhs, bool out_domain, int bordering_d = 0) {
     if (stats && stats->npasses < 8) {
       stats->pass_cells[stats->npasses] = int(ids.size());
     }
@@ -998,7 +1070,7 @@ struct Solver {
     if (P >= 256) return false;  // voronoi.cpp:867-870
     std::vector<unsigned> nn;
     if (!knn(ids, K, nn)) return false;
-    const bool ok = cells(ids, nn, K, P, V, T, vhs, out_domain);
+    const bool ok = cells(ids, nn, K, P, V, T, vhs, out_domain, bordering_d);
     if (stats && stats->npasses < 8) stats->pass_seconds[stats->npasses] = now_s() - t0;
     return ok;
   }
@@ -1029,6 +1101,34 @@ struct Solver {
     status.assign(n, success);
     out.assign(n, Vec4<R>{0, 0, 0, 0});
     const bool dbl = std::is_same<R, double>::value;
+    // used cells only with a grid (voronoi.cpp:1291); the main passes mark at
+    // distance 0 or 1 (voronoi.cpp:1286)
+    if (grid && prm.used_cells && prm.keep_distance >= 0) {
+      used.assign(n, 0);
+      uc.flags = used.data();
+      uc.eps = prm.keep_volume;
+      uc.dist = std::min(prm.keep_distance, 1);
+    }
+    int K = prm.K, P = prm.P, V = prm.V, T = prm.T;
+    const int rc = passes(K, P, V, T, dbl);
+    if (rc < 0) return rc;
+    // bordering passes (voronoi.cpp:1381-1393) with the last caps: the cells
+    // marked d-1 that are not used themselves mark their neighbours d
+    if (uc.flags) {
+      for (int d = 2; d <= prm.keep_distance; ++d) {
+        std::vector<int> bids;
+        for (int i = 0; i < n; ++i)
+          if (used[i] + 1 == d && out[i].w < R(prm.keep_volume)) bids.push_back(i);
+        if (bids.empty()) break;
+        if (!pass(bids, K, P, V, T, dbl ? 2 : prm.vhs1, false, d)) return -3;
+        count_pass();
+      }
+    }
+    return 0;
+  }
+
+  int passes(int &K, int &P, int &V, int &T, bool dbl) {
+    const int n = int(status.size());
     std::vector<int> ids0, ids1;
     const int stride = prm.sample_stride > 1 ? prm.sample_stride : 1;
     for (int i = 0; i < n; i += stride) ids0.push_back(i);
@@ -1046,7 +1146,6 @@ struct Solver {
     }
     if (!ids0.empty()) {
       // extra passes with growing caps (voronoi.cpp:1311-1376)
-      int K = prm.K, P = prm.P, V = prm.V, T = prm.T;
       const int vhs = dbl ? 2 : prm.vhs1;
       const bool out_domain = grid && grid->has_border_corners;
       recompute(ids0, ids1, hist, [](Status) { return true; });
@@ -1090,7 +1189,7 @@ GridView<R> make_grid_view(const OracleGrid *g) {
 
 template <class R>
 int solve_t(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p, double *bary, int *status,
-            OracleStats *stats) {
+            OracleStats *stats, unsigned char *used_out = nullptr) {
   std::vector<Vec4<R>> user(n);
   for (int i = 0; i < n; ++i)
     user[i] = mk<R>(R(xyzw[4 * i]), R(xyzw[4 * i + 1]), R(xyzw[4 * i + 2]), R(xyzw[4 * i + 3]));
@@ -1107,6 +1206,7 @@ int solve_t(const double *xyzw, int n, const OracleGrid *grid, const OracleParam
     bary[4 * u + 2] = double(o.z);
     bary[4 * u + 3] = double(o.w);
     if (status) status[u] = int(s.status[st]);
+    if (used_out) used_out[u] = s.used.empty() ? 0 : s.used[st];
     if (stats && s.status[st] >= 0 && s.status[st] < kStatusNum) stats->final_status[s.status[st]]++;
   }
   if (stats) {
@@ -1155,6 +1255,14 @@ int oracle_solve(const double *xyzw, int n, const OracleGrid *grid, const Oracle
   if (stats) std::memset(stats, 0, sizeof(*stats));
   if (p->use_double) return solve_t<double>(xyzw, n, grid, p, bary, status, stats);
   return solve_t<float>(xyzw, n, grid, p, bary, status, stats);
+}
+
+int oracle_solve_used(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p, double *bary,
+                      int *status, unsigned char *used, OracleStats *stats) {
+  if (n <= 0 || !xyzw || !p || !bary || !used) return -1;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (p->use_double) return solve_t<double>(xyzw, n, grid, p, bary, status, stats, used);
+  return solve_t<float>(xyzw, n, grid, p, bary, status, stats, used);
 }
 
 int oracle_knn(const double *xyzw, int n, int K, int use_double, int kernels, int knn_mode, int *knn, int nthreads) {

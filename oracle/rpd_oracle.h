@@ -43,6 +43,9 @@ typedef struct OracleParams {
   double cube_eps;          // CUBE_EPSILON: 0.1 with a grid, 0 without
   int nthreads;             // 0: all host threads
   int sample_stride;        // >1: only every stride-th stored seed is solved (timing samples)
+  int used_cells;           // 1: mark used cells (needs a grid; voronoi.cpp:1291)
+  int keep_distance;        // VoroAlgo::m_keepDistance (>= 0)
+  double keep_volume;       // VoroAlgo::m_keepVolume
 } OracleParams;
 
 typedef struct OracleStats {
@@ -64,6 +67,11 @@ typedef struct OracleStats {
 // NO_CELL_LIMITS seeds), status n.  Returns 0 on success, <0 on error.
 int oracle_solve(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p,
                  double *bary, int *status, OracleStats *stats);
+
+// As oracle_solve, with the used-cell marks (user order, one byte per seed:
+// 0 unused, else the ring distance, 1 for used cells) when p->used_cells.
+int oracle_solve_used(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p, double *bary,
+                      int *status, unsigned char *used, OracleStats *stats);
 
 // K nearest neighbours of every seed, in user ids, ascending distance, -1 when
 // fewer exist.  knn_mode as in OracleParams.

@@ -25,6 +25,8 @@ typedef struct RefCellArgs {
   void *out;                  // real4[n]: (m*x, m*y, m*z, m)
   int k, p, v, t;             // caps of this pass
   int nthreads;               // 0 = all
+  unsigned char *used;        // CUSED_CELL builds: usedCells[n] (stored order)
+  double used_eps;            // USED_CELL_EPSILON
 } RefCellArgs;
 
 typedef struct RefKnnArgs {
