@@ -49,6 +49,7 @@ void usage(const char *argv0) {
             << "\t--output=xyz|mg|volume (repeatable)\n"
             << "\t--points4D: the seed file has a weight column\n"
             << "\t--keepVolume=v: cells with volume below v are empty (default 1)\n"
+            << "\t--keepDist2=d: with --grid, keep the used cells and d rings around them (default 0; -1 all)\n"
             << "\t--printInvariants --checkGrid --debug\n";
 }
 
@@ -60,6 +61,7 @@ int main(int argc, char **argv) {
   std::vector<std::string> outputs;
   bool points4d = false, invariants = false, check_grid = false, debug = false;
   double keep_volume = 1;
+  int keep_dist2 = 0;  // test_voronoi's final keep distance (Options.cpp:42, test_voronoi.cpp:38)
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i], val;
     const size_t eq = a.find('=');
@@ -80,6 +82,8 @@ int main(int argc, char **argv) {
     else if (a == "--grid") grid_file = need();
     else if (a == "--output") outputs.push_back(need());
     else if (a == "--keepVolume") keep_volume = std::atof(need().c_str());
+    else if (a == "--keepDist2") keep_dist2 = std::atoi(need().c_str());
+    else if (a == "--keepDist") (void)need();  // distance of the passes before the last: no effect here
     else if (a == "--points4D") points4d = true;
     else if (a == "--printInvariants") invariants = true;
     else if (a == "--checkGrid") check_grid = true;
@@ -115,13 +119,21 @@ int main(int argc, char **argv) {
   algo.m_P = P;
   algo.m_V = V;
   algo.m_T = T;
+  algo.m_keepDistance = keep_dist2;
+  algo.m_keepVolume = keep_volume;
   algo.setInputPoints(pts);
   if (has_grid) algo.setGrid(grid);
   std::vector<double> bary;
   std::vector<rpd::VoroAlgoStat> stats;
   const bool ok = algo.launch(
       [&](rpd::VoroAlgo const &a) {
-        bary = a.getBarycenters();
+        // back to one row per user seed (zeros for the unused ones), as
+        // test_voronoi.cpp:186-211 places them with getPermutationToUser
+        const std::vector<double> b = a.getBarycenters();
+        const std::vector<int> perm = a.getPermutationToUser();
+        bary.assign(4 * (pts.size() / 4), 0.0);
+        for (size_t i = 0; i < perm.size(); ++i)
+          for (int d = 0; d < 4; ++d) bary[4 * size_t(perm[i]) + d] = b[4 * i + d];
         return true;
       },
       stats);

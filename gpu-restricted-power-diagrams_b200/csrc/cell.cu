@@ -50,7 +50,7 @@ constexpr int kDeferred = 100;      // internal status: cell parked for k_cone
 struct Layout {
   int Pc, Vc, G, Mw;  // Mw: 32-bit words of one plane's edge mask
   unsigned o_plane, o_cx, o_cy, o_cz, o_cw, o_d2, o_tri, o_next, o_emask, o_rem, o_hole, o_edge;
-  unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist, o_pts, o_fstart, o_fv;
+  unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist, o_pts, o_fstart, o_fv, o_pnb;
   unsigned total;
 };
 
@@ -92,8 +92,10 @@ __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
     L.o_pts = o; o = align16(o + 8u * 12);
     L.o_fstart = o; o = align16(o + 4u * (L.Pc + 1));
     L.o_fv = o; o = align16(o + 3u * L.Vc);
+    L.o_pnb = o; o = align16(o + 4u * L.Pc);
   } else {
     L.o_bcx = L.o_bcy = L.o_bcz = L.o_bcw = L.o_bd2 = L.o_btri = L.o_tlist = L.o_pts = L.o_fstart = L.o_fv = 0;
+    L.o_pnb = 0;
   }
   L.total = o;
   return L;
@@ -114,6 +116,7 @@ struct WarpCell {
   double *pts;  // start corner and the current boundary triangle, local frame
   int *fstart;         // per plane: first entry of its face in fv (np + 1 entries)
   unsigned char *fv;   // vertex ids of every face, in cyclic order
+  int *pnb;            // per plane: its neighbour seed (stored id), -1 for box planes (used cells only)
   int nv, np;  // vertex and plane counts (warp-uniform)
   int vc, mw;  // capacity of the vertex arrays, words per edge mask
 };
@@ -142,6 +145,7 @@ __device__ __forceinline__ WarpCell bind(unsigned char *base, const Layout &L) {
   w.pts = reinterpret_cast<double *>(base + L.o_pts);
   w.fstart = reinterpret_cast<int *>(base + L.o_fstart);
   w.fv = base + L.o_fv;
+  w.pnb = reinterpret_cast<int *>(base + L.o_pnb);
   w.nv = w.np = 0;
   w.vc = L.Vc;
   w.mw = L.Mw;
@@ -1434,7 +1438,7 @@ struct DeferHeader {
 static_assert(sizeof(DeferHeader) == 144, "defer header size");
 
 __host__ __device__ inline size_t slot_bytes_for(const Layout &L, int T) {
-  return size_t(align16(unsigned(sizeof(DeferHeader) + 32u * L.Pc + 44u * L.Vc + 4u * ((T + 3) & ~3))));
+  return size_t(align16(unsigned(sizeof(DeferHeader) + 32u * L.Pc + 44u * L.Vc + 4u * ((T + 3) & ~3) + 4u * L.Pc)));
 }
 
 __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, const Layout &L, int T, int sid,
@@ -1465,7 +1469,10 @@ __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, con
     vt[v] = w.tri[v];
   }
   for (int i = lane; i < nuniq; i += 32) tl[i] = w.tlist[i];
-  (void)T;
+  if (w.pnb) {
+    int *nb = tl + ((T + 3) & ~3);
+    for (int i = lane; i < w.np; i += 32) nb[i] = w.pnb[i];
+  }
 }
 
 // Domain restriction of the clipped cell (ConvexCell.cl:918-1116): start
@@ -1634,6 +1641,21 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   }
 }
 
+// CCUpdateUsedCell (ConvexCell.cl:680-690): the plane neighbours of the
+// cell's vertices get mark d where they have none.  Concurrent cells write
+// the same flags: relaxed byte accesses, as in the reference.
+__device__ __forceinline__ void mark_neighbours(unsigned char *used, const unsigned *tri, int nv, const int *pnb, int d,
+                                                int lane, int nlanes) {
+  for (int v = lane; v < nv; v += nlanes) {
+    const unsigned t = tri[v];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int nb = pnb[(t >> (8 * i)) & 0xff];
+      if (nb >= 0 && *(volatile unsigned char *)&used[nb] == 0) *(volatile unsigned char *)&used[nb] = (unsigned char)d;
+    }
+  }
+}
+
 template <int VS, bool GRID, bool INL>
 __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1660,11 +1682,13 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   }
   init_box(w, s, a.cube_eps, lane);
   double R2 = cell_radius2<VS>(w, lane);
+  const bool track_nb = GRID && a.used != nullptr;  // plane neighbours for the used cells
+  if (track_nb && lane < 6) w.pnb[lane] = -1;
 
   // ---- power clipping by the K nearest, in order ----
   const unsigned *nrow = a.knn + size_t(row) * a.K;
   bool reached = false, exhausted = false, outside = false;
-  const bool early = GRID && a.early_out && a.grid.sat != nullptr;
+  const bool early = GRID && a.early_out && a.grid.sat != nullptr && a.border_d == 0;
   const double plain2 = early ? plain_radius2(a.grid, s, lane) : -1.0;
   for (int i0 = 0; i0 < a.K && status == kSuccess && !reached && !exhausted && !outside; i0 += 32) {
     // every lane builds the bisector of one neighbour, in double
@@ -1672,8 +1696,10 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
     Plane pl{0.0, 0.0, 0.0, 0.0};
     double nd2 = 0.0;
     bool valid = false;
+    unsigned zl = kNone;
     if (i < a.K) {
       const unsigned z = __ldg(&nrow[i]);
+      zl = z;
       if (z != kNone) {
         const float4 b = __ldg(&a.stored[z]);
         const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
@@ -1702,6 +1728,10 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
         break;
       }
       const int r = clip<VS>(w, e, a.V, status, lane, ctr, tr, trcap);
+      if (track_nb) {
+        const unsigned zj = __shfl_sync(kFull, zl, j);
+        if (r > 0 && lane == 0) w.pnb[w.np - 1] = int(zj);
+      }
       if (r < 0) break;
       if (r > 0) {
         R2 = cell_radius2<VS>(w, lane);
@@ -1717,6 +1747,13 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
     }
   }
   if (status == kSuccess && !reached && !exhausted && !outside) status = kSecurityRadiusNotReached;
+  if (a.border_d > 0) {
+    // bordering pass (ConvexCell.cl:756-809): the clipped cell marks its
+    // neighbours; statuses and moments stay those of the main passes
+    __syncwarp();
+    if (status == kSuccess) mark_neighbours(a.used, w.tri, w.nv, w.pnb, a.border_d, lane, 32);
+    return;
+  }
   if (outside) count(ctr, kCtrOutside, 1, lane);
   if (status == kSuccess && !outside) {
     if (GRID)
@@ -1737,6 +1774,12 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
       a.out[sid] = make_double4(acc[0] + m * double(s.x), acc[1] + m * double(s.y), acc[2] + m * double(s.z), m);
     else
       a.out[sid] = make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  if (track_nb && status == kSuccess && acc[3] >= a.keep_volume) {
+    // a used cell (ConvexCell.cl:1118-1126)
+    if (lane == 0) *(volatile unsigned char *)&a.used[sid] = 1;
+    __syncwarp();
+    if (a.mark_dist >= 1) mark_neighbours(a.used, w.tri, w.nv, w.pnb, 1, lane, 32);
   }
 }
 
@@ -1818,7 +1861,7 @@ __global__ void __launch_bounds__(128, 4) k_cone(CellLaunch a, Layout L) {
 // Per parked cell: its in-domain part plus the chunk partials in order; the
 // first failing chunk decides the status (the reference stops at the first
 // failing triangle, ConvexCell.cl:1104-1107).
-__global__ void k_cone_finish(CellLaunch a) {
+__global__ void k_cone_finish(CellLaunch a, Layout L) {
   const DeferQueue &dq = a.defer;
   const int parked = min(dq.counters[0], dq.capacity);
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1843,6 +1886,18 @@ __global__ void k_cone_finish(CellLaunch a) {
   a.out[sid] = status == kSuccess
                    ? make_double4(acc[0] + m * double(s.x), acc[1] + m * double(s.y), acc[2] + m * double(s.z), m)
                    : make_double4(0.0, 0.0, 0.0, 0.0);
+  if (a.used && status == kSuccess && m >= a.keep_volume) {
+    // a used cell (ConvexCell.cl:1118-1126), marked from the parked copy
+    *(volatile unsigned char *)&a.used[sid] = 1;
+    if (a.mark_dist >= 1) {
+      const unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
+      const double *vx = reinterpret_cast<const double *>(base + sizeof(DeferHeader) + 32u * L.Pc);
+      const unsigned *vt = reinterpret_cast<const unsigned *>(vx + 5 * size_t(L.Vc));
+      const int *tl = reinterpret_cast<const int *>(vt + L.Vc);
+      const int *nb = tl + ((a.T + 3) & ~3);
+      mark_neighbours(a.used, vt, h->nv, nb, 1, 0, 1);
+    }
+  }
 }
 
 // Raises a kernel's dynamic shared memory limit to the device's opt-in
@@ -1881,7 +1936,7 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
     e = allow_smem(reinterpret_cast<const void *>(k_cone<VS>), smem);
     if (e != cudaSuccess) return e;
     k_cone<VS><<<sm_count * 4, warps_per_block * 32, smem, st>>>(a, L);
-    k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a);
+    k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a, L);
     if (launches) *launches += 3;
   } else if (a.grid.size > 0) {
     e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, true>), smem);

@@ -77,6 +77,13 @@ struct CellLaunch {
   DeferQueue defer;   // slots == null: every boundary cell inline
   int only_status = -1;  // >= 0: process only the rows whose status equals it
   cudaEvent_t after_cell = nullptr;  // recorded after the cell kernel, before the cone kernels
+  // used cells (a domain only): a successful cell with mass >= keep_volume
+  // sets used[sid] = 1 and, with mark_dist >= 1, marks its face neighbours;
+  // border_d > 0: bordering pass, clip only and mark the neighbours border_d
+  unsigned char *used = nullptr;
+  double keep_volume = 0.0;
+  int mark_dist = 0;
+  int border_d = 0;
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
 constexpr int kTraceRecord = 12;

@@ -10,7 +10,7 @@
 
 namespace rpd {
 
-namespace {
+namespace pool_detail {
 constexpr int kMaxDev = 64;
 std::mutex g_alloc_mu;
 cudaStream_t g_alloc_stream[kMaxDev] = {};
@@ -33,11 +33,11 @@ cudaError_t alloc_stream(cudaStream_t *out) {
   *out = g_alloc_stream[dev];
   return cudaSuccess;
 }
-}  // namespace
+}  // namespace pool_detail
 
 cudaError_t pool_alloc(void **p, size_t bytes) {
   cudaStream_t st;
-  cudaError_t e = alloc_stream(&st);
+  cudaError_t e = pool_detail::alloc_stream(&st);
   if (e != cudaSuccess) return e;
   if ((e = cudaMallocAsync(p, bytes, st)) != cudaSuccess) return e;
   // usable from every stream once the allocation stream has reached it
@@ -46,7 +46,7 @@ cudaError_t pool_alloc(void **p, size_t bytes) {
 
 void pool_free(void *p) {
   cudaStream_t st;
-  if (alloc_stream(&st) == cudaSuccess) cudaFreeAsync(p, st);
+  if (pool_detail::alloc_stream(&st) == cudaSuccess) cudaFreeAsync(p, st);
 }
 
 
@@ -133,6 +133,41 @@ __global__ void k_status_hist(const int *__restrict__ status, int n, int *__rest
   if (threadIdx.x < kStatusNum && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
+// Stored ids of the bordering cells of distance d: marked d-1, not used
+// themselves (find_bordering, voronoi.cpp:711-719), ascending.
+__global__ void k_border_flags(const unsigned char *__restrict__ used, const double4 *__restrict__ out, int n, int d,
+                               double eps, int *__restrict__ f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  f[i] = i < n && int(used[i]) + 1 == d && out[i].w < eps;
+}
+__global__ void k_scatter_flagged(const int *__restrict__ f, const int *__restrict__ pos, int n, int *__restrict__ out,
+                                  int *__restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == n) *count = pos[n];
+  if (i < n && f[i]) out[pos[i]] = i;
+}
+// User-order flags of the used cells.
+__global__ void k_used_flags(const unsigned char *__restrict__ used, const int *__restrict__ user_to_stored, int n,
+                             int *__restrict__ f) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u > n) return;
+  f[u] = u < n && used[user_to_stored[u]] != 0;
+}
+// compact_result (voronoi.cpp:590-625): rows in ascending user order.
+__global__ void k_used_compact(const int *__restrict__ f, const int *__restrict__ pos, int n,
+                               const int *__restrict__ user_to_stored, const double4 *__restrict__ out,
+                               const unsigned char *__restrict__ used, int keep_distance, double eps,
+                               double4 *__restrict__ rows, int *__restrict__ user_ids) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n || !f[u]) return;
+  const int sid = user_to_stored[u];
+  double4 r = out[sid];
+  if (r.w < eps && int(used[sid]) == keep_distance) r.w = double(kNoCellLimits);
+  rows[pos[u]] = r;
+  user_ids[pos[u]] = u;
+}
+
 }  // namespace rpd
 
 using namespace rpd;
@@ -170,12 +205,62 @@ int recompute_ids(rpd_solver *s, const int *ids_in, int num, int cond, int *out0
   return RPD_OK;
 }
 
+int select_bordering(rpd_solver *s, int d, int &count) {
+  rpd_context *ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const int n = s->n;
+  const size_t nsc = scan_workspace_ints(n + 1);
+  if ((e = s->fail_ws.ensure(sizeof(int) * (2 * size_t(n + 1) + nsc + 1))) != cudaSuccess)
+    return map_cuda(ctx, e, "alloc bordering ws");
+  int *f = s->fail_ws.as<int>(), *pos = f + (n + 1), *tiles = pos + (n + 1), *cnt = tiles + nsc;
+  const int tb = 256;
+  k_border_flags<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(s->used.as<unsigned char>(), s->out.as<double4>(), n, d,
+                                                        s->keep_volume, f);
+  if ((e = exclusive_scan(f, pos, n + 1, tiles, st)) != cudaSuccess) return map_cuda(ctx, e, "scan");
+  k_scatter_flagged<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(f, pos, n, s->ids_c.as<int>(), cnt);
+  s->stats.kernel_launches += 5;
+  if ((e = cudaMemcpyAsync(&count, cnt, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return map_cuda(ctx, e, "copy count");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "bordering ids");
+  return RPD_OK;
+}
+
+// User-order flags and positions of the used cells in fail_ws; their count.
+int used_positions(rpd_solver *s, int **f_out, int **pos_out, int &count) {
+  rpd_context *ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const int n = s->n;
+  const size_t nsc = scan_workspace_ints(n + 1);
+  if ((e = s->fail_ws.ensure(sizeof(int) * (2 * size_t(n + 1) + nsc))) != cudaSuccess)
+    return map_cuda(ctx, e, "alloc used ws");
+  int *f = s->fail_ws.as<int>(), *pos = f + (n + 1), *tiles = pos + (n + 1);
+  const int tb = 256;
+  k_used_flags<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(s->used.as<unsigned char>(), s->user_to_stored.as<int>(), n, f);
+  if ((e = exclusive_scan(f, pos, n + 1, tiles, st)) != cudaSuccess) return map_cuda(ctx, e, "scan");
+  if ((e = cudaMemcpyAsync(&count, pos + n, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return map_cuda(ctx, e, "copy count");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "used cells");
+  *f_out = f;
+  *pos_out = pos;
+  return RPD_OK;
+}
+
+int count_used(rpd_solver *s) {
+  int *f = nullptr, *pos = nullptr, c = 0;
+  const int rc = used_positions(s, &f, &pos, c);
+  if (rc == RPD_OK) s->used_count = c;
+  s->stats.kernel_launches += 4;
+  return rc;
+}
+
 // One pass (VoroAlgoComputeData::launch, voronoi.cpp:861-1036): the K
 // nearest of the listed seeds, then their cells with this pass's caps.
 static_assert(int(RPD_CTR_NUM) == int(kCtrNum), "counter enums out of sync");
 
 int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T, float eps, int out_domain,
-             bool counters, bool early_out) {
+             bool counters, bool early_out, int border_d = 0) {
   rpd_context *ctx = s->ctx;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
@@ -214,12 +299,18 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.out_domain = out_domain;
   a.early_out = early_out ? 1 : 0;
   a.inner_apex = s->inner_apex ? 1 : 0;
+  if (s->used_on) {
+    a.used = s->used.as<unsigned char>();
+    a.keep_volume = s->keep_volume;
+    a.mark_dist = std::min(s->keep_distance, 1);
+    a.border_d = border_d;
+  }
   a.grid = s->grid;
   a.status = s->status.as<int>();
   a.out = s->out.as<double4>();
   a.counters = ctr;
   a.after_cell = ev[3];
-  if (s->grid.size > 0 && s->use_defer) {
+  if (s->grid.size > 0 && s->use_defer && border_d == 0) {
     // boundary cells with many triangles are parked and their triangles
     // spread over all warps; cells past the capacity stay inline
     DeferQueue &dq = a.defer;
@@ -484,6 +575,8 @@ void rpd_params_default(rpd_params *p) {
   p->cube_eps = -1.f;
   p->out_domain = -1;
   p->flags = 0;
+  p->keep_distance = -1;
+  p->keep_volume = 0.001;
 }
 
 int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
@@ -594,15 +687,24 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   s->use_defer = !(p.flags & RPD_FLAG_NO_DEFER);
   s->inner_apex = !(p.flags & RPD_FLAG_REFERENCE_APEX);
   s->fresh_knn = (p.flags & RPD_FLAG_FRESH_NEIGHBOURS) != 0;
+  // used cells only with a domain (voronoi.cpp:1291)
+  s->used_on = grid && p.keep_distance >= 0;
+  s->keep_distance = p.keep_distance;
+  s->keep_volume = p.keep_volume;
+  s->used_count = -1;
+  if (s->used_on) {
+    if ((e = s->used.ensure(size_t(n))) != cudaSuccess) return map_cuda(ctx, e, "alloc used");
+    cudaMemsetAsync(s->used.ptr, 0, size_t(n), st);
+  }
   int rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
   if (rc != RPD_OK) return rc;
+  int K = p.K, P = p.P, V = p.V, T = p.T;
   if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {
     int hist[kStatusNum];
     int n0 = 0, n1 = 0;
     int *A = s->ids_a.as<int>(), *B = s->ids_b.as<int>(), *Cc = s->ids_c.as<int>();
     // extra passes (voronoi.cpp:1311-1376): caps grow x1.5 by failing status
     if ((rc = recompute_ids(s, nullptr, n, 0, A, Cc, n0, n1, hist)) != RPD_OK) return rc;
-    int K = p.K, P = p.P, V = p.V, T = p.T;
     const int out_domain = p.out_domain >= 0 ? p.out_domain : (grid && s->grid.has_border_corners ? 1 : 0);
     for (int step = 0; step < p.max_extra_passes && n0 > 0; ++step) {
       bool relaunch = false;
@@ -618,6 +720,17 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
       if ((rc = recompute_ids(s, A, n0, 1, B, Cc, n0, n1, hist)) != RPD_OK) return rc;
       std::swap(A, B);
     }
+  }
+  if (s->used_on) {
+    // bordering passes (voronoi.cpp:1381-1393) with the last caps: the cells
+    // of ring d-1 that are not used themselves mark their neighbours d
+    for (int d = 2; d <= p.keep_distance; ++d) {
+      int nb = 0;
+      if ((rc = select_bordering(s, d, nb)) != RPD_OK) return rc;
+      if (nb == 0) break;
+      if ((rc = run_pass(s, s->ids_c.as<int>(), nb, K, P, V, T, eps, 0, false, false, d)) != RPD_OK) return rc;
+    }
+    if ((rc = count_used(s)) != RPD_OK) return rc;
   }
   cudaEventRecord(t1, st);
   int *h = s->hist.as<int>();
@@ -735,6 +848,41 @@ int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st) {
   return RPD_OK;
 }
 
+int rpd_solver_used_count(const rpd_solver *s) {
+  if (!s || !s->have_results || s->used_count < 0) return RPD_ERR_INVALID;
+  return s->used_count;
+}
+
+int rpd_solver_get_used(rpd_solver *s, double *rows4, int *user_ids, rpd_mem where) {
+  if (!s || !rows4 || !user_ids || !s->have_results || s->used_count < 0) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  int *f = nullptr, *pos = nullptr, c = 0;
+  int rc = used_positions(s, &f, &pos, c);
+  if (rc != RPD_OK) return rc;
+  double4 *rows = reinterpret_cast<double4 *>(rows4);
+  int *ids = user_ids;
+  if (where != RPD_DEVICE) {
+    if ((e = s->gather.ensure((sizeof(double4) + sizeof(int)) * size_t(std::max(c, 1)))) != cudaSuccess)
+      return map_cuda(ctx, e, "alloc gather");
+    rows = s->gather.as<double4>();
+    ids = reinterpret_cast<int *>(rows + std::max(c, 1));
+  }
+  const int n = s->n, tb = 256;
+  k_used_compact<<<(n + tb - 1) / tb, tb, 0, st>>>(f, pos, n, s->user_to_stored.as<int>(), s->out.as<double4>(),
+                                                   s->used.as<unsigned char>(), s->keep_distance, s->keep_volume,
+                                                   rows, ids);
+  if (where != RPD_DEVICE && c > 0) {
+    cudaMemcpyAsync(rows4, rows, sizeof(double4) * size_t(c), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(user_ids, ids, sizeof(int) * size_t(c), cudaMemcpyDeviceToHost, st);
+  }
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return map_cuda(ctx, e, "get used");
+  return c;
+}
+
 }  // extern "C"
 
 namespace rpd {
@@ -786,3 +934,4 @@ size_t solver_device_bytes(const rpd_solver *s) {
 }
 
 }  // namespace rpd
+

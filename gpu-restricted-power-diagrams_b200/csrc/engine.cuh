@@ -92,6 +92,12 @@ struct rpd_solver {
   bool use_defer = true;       // park heavy boundary cells for the chunked kernel
   bool inner_apex = true;      // cone apex at a grid corner inside the cell
   bool fresh_knn = false;      // recompute the neighbour table at this launch
+  // used cells (keep_distance >= 0 with a domain)
+  rpd::DevBuf used;            // unsigned char[n], stored order: 0 or the ring distance
+  bool used_on = false;
+  int keep_distance = -1;
+  double keep_volume = 0.0;
+  int used_count = -1;         // of the last launch, -1: none
   rpd_stats stats{};
 };
 

@@ -72,6 +72,8 @@ def lib():
         L.rpd_server_bytes_in_use.restype = C.c_size_t
         L.rpd_server_bytes_in_use.argtypes = [C.c_void_p]
         L.rpd_solver_set_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.rpd_solver_used_count.argtypes = [C.c_void_p]
+        L.rpd_solver_get_used.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_get_permutation.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_knn.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_float)]
         L.rpd_grid_create.restype = C.c_void_p
@@ -120,7 +122,8 @@ class Params(C.Structure):
     """rpd_params: the VoroAlgo knobs (voronoi.h:199-246)."""
 
     _fields_ = [("K", C.c_int), ("P", C.c_int), ("V", C.c_int), ("T", C.c_int), ("max_extra_passes", C.c_int),
-                ("cube_eps", C.c_float), ("out_domain", C.c_int), ("flags", C.c_uint)]
+                ("cube_eps", C.c_float), ("out_domain", C.c_int), ("flags", C.c_uint),
+                ("keep_distance", C.c_int), ("keep_volume", C.c_double)]
 
     @classmethod
     def default(cls, **kw):
@@ -216,6 +219,20 @@ class Solver:
         x = as_xyzw(xyzw)
         self.ctx.check(lib().rpd_solver_set_points(self.h, _ptr(x), len(x), RPD_HOST))
         return self
+
+    def used(self):
+        """Used cells of the last launch with keep_distance >= 0 and a grid:
+        (rows (m,4) in ascending user order, user ids (m,)), the reference's
+        compressed output (getBarycenters + getPermutationToUser)."""
+        m = lib().rpd_solver_used_count(self.h)
+        if m < 0:
+            raise RpdError(m, "no used cells: launch with keep_distance >= 0 and a grid")
+        rows = np.zeros((max(m, 1), 4), np.float64)
+        ids = np.zeros(max(m, 1), np.int32)
+        rc = lib().rpd_solver_get_used(self.h, _ptr(rows), _ptr(ids), RPD_HOST)
+        if rc < 0:
+            self.ctx.check(rc)
+        return rows[:m], ids[:m]
 
     def set_weights(self, w):
         """Weight-only re-solve setup: new weights (user order) for the seeds

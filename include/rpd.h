@@ -165,6 +165,11 @@ typedef struct rpd_params {
                            retry passes: -1 auto (when the grid has border
                            corners, voronoi.cpp:1320), 0 never, 1 always */
   unsigned flags;       /* RPD_FLAG_* */
+  int keep_distance;    /* used cells, with a domain only (--keepDist2; voronoi.cpp:1286-1393):
+                           -1 off (the default), 0 the cells of mass >= keep_volume,
+                           d >= 1 also the cells up to d face rings around them */
+  double keep_volume;   /* --keepVolume: the mass that makes a cell used (default 0.001,
+                           the FP64 build's, Options.cpp:40) */
 } rpd_params;
 
 void rpd_params_default(rpd_params *p);
@@ -217,6 +222,15 @@ int rpd_solver_get_moments(rpd_solver *s, double *out4, rpd_mem where);
 /* Per seed in user order: rpd_cell_status. */
 int rpd_solver_get_status(rpd_solver *s, int *status, rpd_mem where);
 int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st);
+/* Used cells of the last launch with keep_distance >= 0 and a domain
+ * (VoroAlgoComputeData::compressResult, voronoi.cpp:513-691): how many, and
+ * their rows in ascending user order -- (m*x, m*y, m*z, m), with m =
+ * RPD_NO_CELL_LIMITS for the outermost ring's cells below keep_volume (the
+ * reference's border seeds, voronoi.cpp:604-611) -- with each row's user id
+ * (getPermutationToUser).  The reference's order is that of an atomic
+ * counter; here it is deterministic.  Returns the count or an error < 0. */
+int rpd_solver_used_count(const rpd_solver *s);
+int rpd_solver_get_used(rpd_solver *s, double *rows4, int *user_ids, rpd_mem where);
 
 /* --------------------------------------------------------------- serving */
 

@@ -153,6 +153,8 @@ class VoroAlgo {
     p.P = m_P;
     p.V = m_V;
     p.T = m_T;
+    p.keep_distance = m_keepDistance;
+    p.keep_volume = m_keepVolume;
     if (rpd_solver_launch(s_, &p) != RPD_OK) {
       if (m_debug) fprintf(stderr, "VoroAlgo::launch: %s\n", ctx_->error().c_str());
       return false;
@@ -178,15 +180,33 @@ class VoroAlgo {
   // are kept.
   void setWeights(std::vector<float> const &w) { rpd_solver_set_weights(s_, w.data(), RPD_HOST); }
   int getNumInputPoints() const { return rpd_solver_num_points(s_); }
-  int getNumOutputPoints() const { return rpd_solver_num_points(s_); }
+  // With m_keepDistance >= 0 and a grid the outputs are the used cells
+  // (VoroAlgoComputeData::compressResult, voronoi.cpp:513-691), in
+  // ascending user order; otherwise every seed, in user order.
+  int getNumOutputPoints() const {
+    const int u = rpd_solver_used_count(s_);
+    return u >= 0 ? u : rpd_solver_num_points(s_);
+  }
   std::vector<double> getBarycenters() const {
+    const int u = rpd_solver_used_count(s_);
     std::vector<double> r(4 * size_t(getNumOutputPoints()));
-    rpd_solver_get_moments(s_, r.data(), RPD_HOST);
+    if (u >= 0) {
+      std::vector<int> ids(size_t(u) + 1);
+      rpd_solver_get_used(s_, r.data(), ids.data(), RPD_HOST);
+    } else {
+      rpd_solver_get_moments(s_, r.data(), RPD_HOST);
+    }
     return r;
   }
   std::vector<int> getPermutationToUser() const {
+    const int u = rpd_solver_used_count(s_);
     std::vector<int> r(getNumOutputPoints());
-    for (size_t i = 0; i < r.size(); ++i) r[i] = int(i);
+    if (u >= 0) {
+      std::vector<double> rows(4 * size_t(u) + 4);
+      rpd_solver_get_used(s_, rows.data(), r.data(), RPD_HOST);
+    } else {
+      for (size_t i = 0; i < r.size(); ++i) r[i] = int(i);
+    }
     return r;
   }
   std::vector<int> getStatus() const {
@@ -199,6 +219,8 @@ class VoroAlgo {
   int m_P = 35;
   int m_T = 100;
   int m_V = 40;
+  // used cells with a grid (voronoi.cpp:1052-1053 defaults): -1 every seed,
+  // else the kept ring distance; the mass that makes a cell used
   float m_keepVolume = 1;
   int m_keepDistance = 1;
 

@@ -1011,7 +1011,7 @@ struct Solver {
         a.grid_size = grid->size;
         a.voxel_size = double(grid->voxel);
       }
-      a.cube_eps = bordering_d > 0 ? 0.0 : prm.cube_eps;
+      a.cube_eps = prm.cube_eps;  // the bordering program keeps CUBE_EPSILON (voronoi.cpp:929)
       a.status = (int *)st_out;
       a.out = out.data();
       a.k = K;
