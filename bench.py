@@ -37,6 +37,12 @@ CONFIGS = {
     "voronoi-100k": dict(kind="uniform", n=100_000, weights=False, grid="blob", gsize=100, nell=5, gseed=2,
                          sseed=1, K=70, P=30, V=40, T=100,
                          desc="100K i.i.d. uniform seeds (weights 0), 5-ellipsoid blob at 100^3, K=70 P=30 V=40"),
+    # blue noise at 5M seeds, unit cube domain
+    "poisson-5m": dict(kind="poisson", n=5_000_000, rfac=0.7, weights=False, grid="cube", gsize=128, sseed=3,
+                       K=20, P=25, V=30, T=100,
+                       desc="5M seeds by seeded Poisson-disk dart throwing in [0,1]^3 (min distance 0.7 N^(-1/3)), "
+                            "weights 0, unit cube domain at 128^3 (faces inset half a voxel, 2 triangles per face "
+                            "cell), K=20 P=25 V=30 T=100; every predicate in FP64 (escalated fraction 1.0)"),
     # a serving loop (one GPU)
     "serve-200rps": dict(kind="serve", rate=200.0, requests=600, nmin=10_000, nmax=2_000_000, reweight=0.3,
                          grid="blob", gsizes=(48, 64, 96, 128, 160, 200), nell=5, gseed=2, sseed=5, K=50, P=30, V=40,
@@ -62,6 +68,8 @@ def make_seeds(cfg, rank):
     s = cfg["sseed"] + 1000 * rank
     if cfg["kind"] == "jittered":
         return synth.jittered_lattice(cfg["m"], seed=s, weights=cfg["weights"])
+    if cfg["kind"] == "poisson":
+        return synth.poisson_disk(cfg["n"], seed=s, rfac=cfg["rfac"])
     return synth.uniform(cfg["n"], seed=s)
 
 

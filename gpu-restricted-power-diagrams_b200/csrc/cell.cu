@@ -875,17 +875,25 @@ __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const 
 }
 
 // Apex inside the cell.  The signed cone decomposition holds for any apex on
-// a known side of the surface.  From a grid corner with flag 0 or 2 that lies
-// inside the convex cell, the segment to any point of the cell stays in the
-// cell, so a triangle that misses the cell crosses none of them and its cone
-// holds no part of the cell.  Picks the corner of the voxel range deepest in
-// the cell (lowest corner id on ties); returns its flag, or -1 when no corner
-// lies at least kApexDepth voxels inside.
-constexpr double kApexDepth = 1e-3;   // voxels
-constexpr double kSeparation = 1e-9;  // reference-frame units
+// a known side of the surface.  From a point inside the convex cell, the
+// segment to any point of the cell stays in the cell, so a triangle that
+// misses the cell crosses none of them and its cone holds no part of the
+// cell.  The apex is the grid corner with flag 0 or 2 of the voxel range
+// deepest in the cell (at least kApexDepth voxels; ties to the lowest corner
+// id), moved by kApexShift voxels along kApexDir: grid triangles have
+// vertices on lattice lines and planes through the corners, so cone planes
+// through the corner itself can contain face edges of the cell exactly, and
+// a facet's boundary then depends on rounding.  No triangle comes within
+// 4 kApexShift of the corner (else -1: the caller keeps the reference's
+// start corner), so the moved apex keeps the corner's side.  Returns the
+// flag, or -1.
+constexpr double kApexDepth = 4e-3;    // voxels
+constexpr double kApexShift = 1e-3;    // voxels
+constexpr double kSeparation = 1e-9;   // reference-frame units
+__device__ __constant__ double kApexDir[3] = {0.5317 / 1.0001074492, 0.3229 / 1.0001074492, 0.7831 / 1.0001074492};
 
 __device__ int inner_apex(const WarpCell &w, const DevGrid &g, float4 s, const int vmin[3], const int vmax[3],
-                          double apex[3], int lane) {
+                          const int *tids, int ntri, double apex[3], int lane) {
   const int S = g.size;
   int lo[3], n[3];
 #pragma unroll
@@ -923,9 +931,38 @@ __device__ int inner_apex(const WarpCell &w, const DevGrid &g, float4 s, const i
   }
   if (best_id == 0x7fffffff) return -1;
   const int x = best_id % S, y = (best_id / S) % S, z = best_id / (S * S);
-  apex[0] = x * h - s.x;
-  apex[1] = y * h - s.y;
-  apex[2] = z * h - s.z;
+  const double c[3] = {x * h - s.x, y * h - s.y, z * h - s.z};
+  // no triangle near the corner: the shifted apex is on the corner's side
+  const double near = 4.0 * kApexShift * h;
+  bool close = false;
+  for (int i = lane; i < ntri && !close; i += 32) {
+    const int tri = tids[i];
+    double P[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 q = __ldg(&g.points[__ldg(&g.tris[3 * tri + k])]);
+      P[k][0] = double(q.x) - s.x;
+      P[k][1] = double(q.y) - s.y;
+      P[k][2] = double(q.z) - s.z;
+    }
+    double lo3[3], hi3[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo3[d] = fmin(P[0][d], fmin(P[1][d], P[2][d])) - near;
+      hi3[d] = fmax(P[0][d], fmax(P[1][d], P[2][d])) + near;
+    }
+    if (c[0] < lo3[0] || c[0] > hi3[0] || c[1] < lo3[1] || c[1] > hi3[1] || c[2] < lo3[2] || c[2] > hi3[2])
+      continue;
+    const double e1[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
+    const double e2[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
+    const double nn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    const double len = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+    const double dist = fabs(nn[0] * (c[0] - P[0][0]) + nn[1] * (c[1] - P[0][1]) + nn[2] * (c[2] - P[0][2]));
+    close = !(dist > near * len);
+  }
+  if (__any_sync(kFull, close)) return -1;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) apex[d] = c[d] + kApexShift * h * kApexDir[d];
   return g.flags[best_id];
 }
 
@@ -1599,7 +1636,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   bool inner = false;
   if (nuniq > 0 && a.inner_apex) {
     double ap[3];
-    const int f = inner_apex(w, g, s, vmin, vmax, ap, lane);
+    const int f = inner_apex(w, g, s, vmin, vmax, w.tlist, nuniq, ap, lane);
     if (f >= 0) {
       inner = true;
       in_domain = f;

@@ -136,6 +136,14 @@ rpd_grid *rpd_grid_make_blob(int size, int nellipsoids, uint64_t seed, int *err)
   return r;
 }
 
+int rpd_synth_poisson_disk(int n, uint64_t seed, double rfac, float *xyzw) {
+  if (n <= 0 || !xyzw || !(rfac > 0)) return RPD_ERR_INVALID;
+  std::vector<float> v;
+  const int k = rpd::poisson_disk(n, seed, rfac, 200, v);
+  std::memcpy(xyzw, v.data(), sizeof(float) * v.size());
+  return k;
+}
+
 rpd_grid *rpd_grid_make_cube(int size, int *err) {
   if (size < 2 || size > 1024) {
     if (err) *err = RPD_ERR_INVALID;

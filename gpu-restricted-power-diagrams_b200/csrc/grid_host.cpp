@@ -409,4 +409,76 @@ void make_cube_domain(int size, HostGrid &g) {
   if (g.volume() < 0) g.swap_orientation();
 }
 
+
+// Seeded Poisson-disk sample of [0,1]^3 by dart throwing (random sequential
+// adsorption): a uniform candidate is kept when no kept point lies closer
+// than r = rfac * n^(-1/3).  Candidates come in seeded batches; a batch is
+// tried in the order of its candidates' background cells (side r, at most 8
+// points each) for locality, every candidate against every point kept
+// before it.  Stops at n points or after max_batches batches.  Output in the
+// reference frame: xyz * 1000, w = 0.  Returns the number of points.
+int poisson_disk(int n, uint64_t seed, double rfac, int max_batches, std::vector<float> &xyzw) {
+  xyzw.clear();
+  if (n <= 0) return 0;
+  const double r = rfac * std::pow(double(n), -1.0 / 3.0), r2 = r * r;
+  const int G = std::max(1, int(1.0 / r));
+  const double cell = 1.0 / G;  // >= r: neighbours lie in the 27 cells around
+  constexpr int kSlots = 8;     // a cube of side r holds at most 8 points r apart
+  std::vector<uint8_t> cnt(size_t(G) * G * G, 0);
+  std::vector<int> slot(size_t(G) * G * G * kSlots, -1);
+  std::vector<double> pts;
+  pts.reserve(size_t(n) * 3);
+  SplitMix rng(seed);
+  const size_t batch = std::max<size_t>(1 << 16, size_t(n) / 4);
+  std::vector<std::pair<uint64_t, std::array<double, 3>>> cand(batch);
+  int kept = 0;
+  for (int b = 0; b < max_batches && kept < n; ++b) {
+    for (auto &c : cand) {
+      c.second = {rng.uniform(), rng.uniform(), rng.uniform()};
+      const int ix = std::min(G - 1, int(c.second[0] / cell)), iy = std::min(G - 1, int(c.second[1] / cell)),
+                iz = std::min(G - 1, int(c.second[2] / cell));
+      c.first = (uint64_t(iz) * G + iy) * G + ix;
+    }
+    std::stable_sort(cand.begin(), cand.end(),
+                     [](const auto &a, const auto &c) { return a.first < c.first; });
+    for (const auto &c : cand) {
+      if (kept >= n) break;
+      const double x = c.second[0], y = c.second[1], z = c.second[2];
+      const int ix = int(c.first % G), iy = int((c.first / G) % G), iz = int(c.first / (uint64_t(G) * G));
+      bool ok = cnt[c.first] < kSlots;
+      for (int dz = -1; dz <= 1 && ok; ++dz) {
+        const int zz = iz + dz;
+        if (zz < 0 || zz >= G) continue;
+        for (int dy = -1; dy <= 1 && ok; ++dy) {
+          const int yy = iy + dy;
+          if (yy < 0 || yy >= G) continue;
+          for (int dx = -1; dx <= 1 && ok; ++dx) {
+            const int xx = ix + dx;
+            if (xx < 0 || xx >= G) continue;
+            const size_t id = (size_t(zz) * G + yy) * G + xx;
+            for (int k = 0; k < cnt[id]; ++k) {
+              const double *q = &pts[3 * size_t(slot[id * kSlots + k])];
+              const double ex = q[0] - x, ey = q[1] - y, ez = q[2] - z;
+              if (ex * ex + ey * ey + ez * ez < r2) {
+                ok = false;
+                break;
+              }
+            }
+          }
+        }
+      }
+      if (!ok) continue;
+      slot[c.first * kSlots + cnt[c.first]++] = kept;
+      pts.insert(pts.end(), {x, y, z});
+      ++kept;
+    }
+  }
+  xyzw.resize(size_t(kept) * 4);
+  for (int i = 0; i < kept; ++i) {
+    for (int d = 0; d < 3; ++d) xyzw[4 * size_t(i) + d] = float(pts[3 * size_t(i) + d] * 1000.0);
+    xyzw[4 * size_t(i) + 3] = 0.f;
+  }
+  return kept;
+}
+
 }  // namespace rpd

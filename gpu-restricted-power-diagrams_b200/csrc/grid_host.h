@@ -49,4 +49,7 @@ void make_random_blob(int size, int nell, uint64_t seed, HostGrid &g);
 // 2 triangles per rectangle, listed in their voxel.
 void make_cube_domain(int size, HostGrid &g);
 
+// Seeded Poisson-disk sample of the unit cube (reference frame x1000).
+int poisson_disk(int n, uint64_t seed, double rfac, int max_batches, std::vector<float> &xyzw);
+
 }  // namespace rpd

@@ -35,62 +35,20 @@ def jittered_lattice(m: int, seed: int = 2, jitter: float = 0.25, weights: bool 
     return x
 
 
-def poisson_disk(n: int, seed: int = 3, rfac: float = 0.7, max_tries: int = 60) -> np.ndarray:
-    """Dart throwing in [0,1]^3 with minimum distance r = rfac * n^(-1/3),
-    accelerated by a background grid of cell r/sqrt(3) (one dart per cell).
-    Returns up to n seeds (fewer when the darts saturate)."""
-    rng = np.random.default_rng(seed)
-    r = rfac * n ** (-1.0 / 3.0)
-    cell = r / np.sqrt(3.0)
-    G = int(np.ceil(1.0 / cell))
-    occ = -np.ones((G, G, G), np.int64)
-    pts = np.zeros((n, 3), np.float64)
-    count = 0
-    r2 = r * r
-    batch = max(4096, n // 8)
-    tries = 0
-    while count < n and tries < max_tries:
-        tries += 1
-        cand = rng.random((batch, 3))
-        ci = np.minimum((cand / cell).astype(np.int64), G - 1)
-        # greedy, in order: a candidate is kept if no kept dart lies within r
-        for k in range(batch):
-            if count >= n:
-                break
-            i, j, l = ci[k]
-            if occ[i, j, l] >= 0:
-                continue
-            p = cand[k]
-            ok = True
-            for di in (-2, -1, 0, 1, 2):
-                ii = i + di
-                if ii < 0 or ii >= G:
-                    continue
-                for dj in (-2, -1, 0, 1, 2):
-                    jj = j + dj
-                    if jj < 0 or jj >= G:
-                        continue
-                    for dl in (-2, -1, 0, 1, 2):
-                        ll = l + dl
-                        if ll < 0 or ll >= G:
-                            continue
-                        q = occ[ii, jj, ll]
-                        if q >= 0:
-                            d = pts[q] - p
-                            if d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < r2:
-                                ok = False
-                                break
-                    if not ok:
-                        break
-                if not ok:
-                    break
-            if ok:
-                occ[i, j, l] = count
-                pts[count] = p
-                count += 1
-    x = np.zeros((count, 4), np.float32)
-    x[:, :3] = (pts[:count] * SCALE).astype(np.float32)
-    return x
+def poisson_disk(n: int, seed: int = 3, rfac: float = 0.7) -> np.ndarray:
+    """Up to n seeds of [0,1]^3 (x1000) by seeded dart throwing with minimum
+    distance r = rfac * n^(-1/3) (rpd_synth_poisson_disk, weights 0)."""
+    import ctypes as C
+
+    from . import lib
+
+    L = lib()
+    L.rpd_synth_poisson_disk.argtypes = [C.c_int, C.c_uint64, C.c_double, C.c_void_p]
+    out = np.zeros((n, 4), np.float32)
+    k = L.rpd_synth_poisson_disk(n, seed, rfac, C.c_void_p(out.ctypes.data))
+    if k < 0:
+        raise ValueError(f"rpd_synth_poisson_disk failed: {k}")
+    return out[:k]
 
 
 def to_unit(xyzw: np.ndarray) -> np.ndarray:

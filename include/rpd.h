@@ -136,6 +136,11 @@ void rpd_grid_destroy(rpd_grid *g);
  * triangulated along the voxel columns. */
 rpd_grid *rpd_grid_make_blob(int size, int nellipsoids, uint64_t seed, int *err);
 rpd_grid *rpd_grid_make_cube(int size, int *err);
+/* Synthetic seeds of the blue-noise configuration (no counterpart in the
+ * reference): up to n points of [0,1000]^3 by seeded dart throwing with
+ * minimum distance rfac * n^(-1/3) * 1000, weights 0, into xyzw (4n floats).
+ * Returns the number of points (n unless the darts saturate). */
+int rpd_synth_poisson_disk(int n, uint64_t seed, double rfac, float *xyzw);
 
 /* --------------------------------------------------------------- solve */
 

@@ -131,3 +131,30 @@ def test_early_out_and_parking_do_not_change_results(rpd):
         assert err.max() < 1e-12, name
     assert np.array_equal(res["no_defer"][0], res["inline"][0]), "the early exit must not change any bit"
     assert np.array_equal(res["ref_apex_no_defer"][0], m0), "the early exit must not change any bit"
+
+
+def test_blue_noise_cube_domain(rpd):
+    # BASELINE config 3 in small: Poisson-disk seeds, unit cube domain
+    from rpd import synth
+
+    x = synth.poisson_disk(30_000, seed=3)
+    g = rpd.Grid.cube(48)
+    met, got, gst, ref, rst, _ = run_case(rpd, x, grid=g, K=20, P=25, V=30, T=100)
+    assert_parity(met)
+    assert abs(got[:, 3].sum() / g.getVolume() - 1) < 1e-9
+
+
+@pytest.mark.parametrize("workload", ["weighted-1m", "voronoi-100k"])
+def test_bench_workloads_full_size(rpd, workload):
+    # the benchmark's own inputs at full size against the FP64 oracle
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    cfg = bench.CONFIGS[workload]
+    x = bench.make_seeds(cfg, 0)
+    g = bench.make_grid(cfg)
+    met, got, gst, *_ = run_case(rpd, x, grid=g, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"])
+    assert_parity(met)

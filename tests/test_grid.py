@@ -66,3 +66,17 @@ def test_oracle_fp64_volume_on_blob(rpd):
     b, s = oracle.solve(jittered(16, seed=1).astype(np.float64), grid=ga, K=40, P=40, V=60, use_double=True)
     assert (s == oracle.SUCCESS).all()
     assert abs(b[:, 3].sum() / g.getVolume() - 1) < 1e-12
+
+
+def test_poisson_disk_generator(rpd):
+    from rpd import synth
+
+    x = synth.poisson_disk(50_000, seed=3)
+    y = synth.poisson_disk(50_000, seed=3)
+    assert len(x) == 50_000 and np.array_equal(x, y)  # seeded
+    assert (x[:, :3] >= 0).all() and (x[:, :3] <= 1000).all() and (x[:, 3] == 0).all()
+    from scipy.spatial import cKDTree
+
+    d, _ = cKDTree(x[:, :3].astype(np.float64)).query(x[:, :3].astype(np.float64), k=2)
+    r = 0.7 * 50_000 ** (-1 / 3) * 1000
+    assert d[:, 1].min() >= r * (1 - 1e-6)
