@@ -43,6 +43,13 @@ CONFIGS = {
                        desc="5M seeds by seeded Poisson-disk dart throwing in [0,1]^3 (min distance 0.7 N^(-1/3)), "
                             "weights 0, unit cube domain at 128^3 (faces inset half a voxel, 2 triangles per face "
                             "cell), K=20 P=25 V=30 T=100; every predicate in FP64 (escalated fraction 1.0)"),
+    # batched uneven diagrams in one graph (one GPU, or one batch per GPU)
+    "batch-256": dict(kind="batch", count=256, nmin=1000, nmax=200_000, gmin=64, gmax=160, ks=(20, 50, 70),
+                      nell=5, sseed=4, P=30, V=40, T=100,
+                      desc="256 independent diagrams in one batched solve (one CUDA graph replay): N log-uniform "
+                           "in [1K, 200K], uniform or jittered-lattice seeds (alternating), weights U[0, 0.1h^2], "
+                           "each with its own seeded 5-ellipsoid blob domain at 64^3..160^3 voxels, K drawn from "
+                           "{20, 50, 70}, P=30 V=40 T=100; compared with the same 256 solved one after another"),
     # a serving loop (one GPU)
     "serve-200rps": dict(kind="serve", rate=200.0, requests=600, nmin=10_000, nmax=2_000_000, reweight=0.3,
                          grid="blob", gsizes=(48, 64, 96, 128, 160, 200), nell=5, gseed=2, sseed=5, K=50, P=30, V=40,
@@ -354,6 +361,238 @@ def run_ours(args, cfg, rank, world, local):
         dist.destroy_process_group()
 
 
+def batch_specs(cfg, rank):
+    from rpd import synth
+
+    return synth.uneven_batch(cfg["count"], seed=cfg["sseed"] + 1000 * rank, nmin=cfg["nmin"], nmax=cfg["nmax"],
+                              gmin=cfg["gmin"], gmax=cfg["gmax"], ks=cfg["ks"])
+
+
+def batch_grids(rpd, cfg, specs):
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        return list(ex.map(lambda s: rpd.Grid.blob(s["grid_size"], cfg["nell"], s["grid_seed"]), specs))
+
+
+def run_batch(args, cfg, rank, world, local):
+    """Batched uneven diagrams: one step = one replay of the batch's graph
+    (every pass of all diagrams, neighbours included); the same diagrams
+    solved one after another with rpd_solver_launch are timed beside it."""
+    import torch
+
+    import rpd
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    ctx = rpd.Context(local)
+    specs = batch_specs(cfg, rank)
+    grids = batch_grids(rpd, cfg, specs)
+    solvers = []
+    for s, g in zip(specs, grids):
+        v = rpd.Solver(ctx).set_points(s["xyzw"])
+        v.set_grid(g)
+        solvers.append(v)
+    params = [rpd.Params.default(K=s["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"]) for s in specs]
+    n = sum(len(s["xyzw"]) for s in specs)
+    batch = rpd.Batch(solvers, params, ctx)
+    for _ in range(args.warmup):
+        batch.launch()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    clocks = ClockSampler(local)
+    step_ms, knn_ms, cell_ms = [], [], []
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        batch.launch()
+        st = batch.stats()
+        step_ms.append(st["graph_ms"])
+        knn_ms.append(st["pass0_knn_ms"])
+        cell_ms.append(st["pass0_cell_kernel_ms"])
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    bstats = batch.stats()
+    got = [(v.status().copy(), v.moments().copy()) for v in solvers]
+    # the same diagrams one after another (fresh neighbours, as in the batch)
+    seq_params = [rpd.Params.default(K=s["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"],
+                                     flags=rpd.FLAG_FRESH_NEIGHBOURS) for s in specs]
+    for v, p in zip(solvers[:8], seq_params):
+        v.launch(p)
+    seq_wall, seq_dev = [], []
+    seq_pass = {}
+    for _ in range(2):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev = 0.0
+        for v, p in zip(solvers, seq_params):
+            v.launch(p)
+            st = v.stats()
+            dev += st["total_ms"]
+            for i, q in enumerate(st["passes"]):
+                e = seq_pass.setdefault(i, {"cells": 0, "knn_ms": 0.0, "cell_ms": 0.0})
+                e["cells"] += q["cells"]
+                e["knn_ms"] += q["knn_ms"]
+                e["cell_ms"] += q["cell_ms"]
+        seq_wall.append(time.perf_counter() - t0)
+        seq_dev.append(dev)
+    seq_pass = [{k: (v / 2 if k != "cells" else v // 2) for k, v in seq_pass[i].items()} for i in sorted(seq_pass)]
+    same = sum(int(np.array_equal(v.status(), a) and np.array_equal(v.moments(), b)) for v, (a, b) in zip(solvers, got))
+    ms = sum(step_ms) / len(step_ms)
+
+    # end to end through the C ABI: every diagram's seeds from pinned host
+    # memory (upload + binning), the batch, every diagram's moments back
+    pins = [torch.from_numpy(s["xyzw"]).pin_memory() for s in specs]
+    outs = [torch.empty((len(s["xyzw"]), 4), dtype=torch.float64).pin_memory() for s in specs]
+    e2e_s = []
+    for _ in range(max(3, min(args.steps, 5))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for v, xp in zip(solvers, pins):
+            ctx.check(rpd.lib().rpd_solver_set_points(v.h, rpd._ptr(xp.numpy()), xp.shape[0], rpd.RPD_HOST))
+        batch.launch()
+        for v, op in zip(solvers, outs):
+            ctx.check(rpd.lib().rpd_solver_get_moments(v.h, rpd._ptr(op.numpy()), rpd.RPD_HOST))
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_t = sum(e2e_s) / len(e2e_s)
+    recaptured = batch.stats()["captures"] - bstats["captures"]
+    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda")
+    seq_rate = n / min(seq_wall)
+    seq_dev_rate = n / (min(seq_dev) / 1e3)
+
+    # roofline of the first pass's batched cell kernel: every diagram's
+    # neighbour table and seeds read once, moments and statuses written once,
+    # every grid read once
+    grid_bytes = 0
+    for g in grids:
+        a = g.arrays()
+        grid_bytes += int(a["in_domain"].nbytes + a["offsets"].nbytes + a["tri_list"].nbytes +
+                          a["triangles"].nbytes + len(a["points"]) * 16)
+    alg_bytes = sum(len(s["xyzw"]) * (4 * s["K"] + 16 + 32 + 4) for s in specs) + grid_bytes
+    cell_avg_ms = sum(cell_ms) / len(cell_ms)
+    achieved = alg_bytes / (cell_avg_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"k_cell_{args.config}_traffic.txt")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            for ln in f:
+                if ln.startswith("bytes_per_launch"):
+                    traffic = int(ln.split("=")[1].strip())
+    sizes = [len(s["xyzw"]) for s in specs]
+    line = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 geometry on f32 seeds (FP64 cofactor predicates and integration)",
+        "data": "synthetic",
+        "config": {"workload": args.config, "description": cfg["desc"], "diagrams": len(specs),
+                   "n_seeds_per_gpu": n, "n_min": min(sizes), "n_max": max(sizes),
+                   "parallelism": f"{world} independent batches, one per GPU",
+                   "l2": "flushed between steps (256 MB write, untimed)"},
+        "e2e": {"value": e2e_value, "unit": "cells/s", "h2d_bytes_per_step": int(sum(s["xyzw"].nbytes for s in specs)),
+                "d2h_bytes_per_step": int(n * 32),
+                "path": "rpd_solver_set_points(host) x256 + rpd_batch_launch + rpd_solver_get_moments(host) x256",
+                "recaptures": recaptured},
+        "gpu_launches": int(bstats["kernel_launches"] * args.steps),
+        "roofline": {"kernel": "k_cell_batch (first pass, all diagrams)", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "launch_ms": cell_avg_ms,
+                     "note": "timed by event nodes inside the graph; an issue-bound FP64 clipping kernel"},
+        "clocks": clk,
+        "sequential": {"value": seq_rate, "unit": "cells/s", "device_only_value": seq_dev_rate,
+                       "path": "rpd_solver_launch per diagram, one after another (wall clock, host syncs "
+                               "included); device_only_value sums each solve's device time",
+                       "batch_speedup": value / seq_rate, "diagrams_bitwise_equal_to_batch": same,
+                       "passes": seq_pass},
+        "detail": {"graph_ms": step_ms, "pass0_knn_ms": sum(knn_ms) / len(knn_ms),
+                   "pass0_cell_kernel_ms": cell_avg_ms, "batch": bstats},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        mid = int(np.argsort(sizes)[len(sizes) // 2])
+        cb = cpu_baseline(specs[mid]["xyzw"], grids[mid], dict(K=specs[mid]["K"], P=cfg["P"], V=cfg["V"],
+                                                               T=cfg["T"]), target_s=args.cpu_seconds)
+        cb["sample"] = f"diagram {mid} (the median size, {sizes[mid]} seeds, K={specs[mid]['K']}): " + cb["sample"]
+        line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for v in solvers:
+        v.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_batch_reference(args, cfg, rank):
+    """--impl reference for the batch: the reference's CPU implementation over
+    a bounded sample of the same diagrams (every 16th), rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+    import rpd
+
+    specs = batch_specs(cfg, 0)
+    sub = [specs[i] for i in range(0, len(specs), 16)]
+    grids = batch_grids(rpd, cfg, sub)
+    kind = "reference" if oracle.has_reference_kernels() else "port"
+    jobs = []
+    for s, g in zip(sub, grids):
+        a = g.arrays()
+        ga = oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+        n = len(s["xyzw"])
+        jobs.append((s["xyzw"].astype(np.float64), ga, s["K"], max(1, n // 6000)))
+
+    def step():
+        t, cells = 0.0, 0
+        for xd, ga, K, stride in jobs:
+            _, _, st = oracle.solve(xd, grid=ga, K=K, P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2, vhs1=2,
+                                    use_double=False, kernels=1 if kind == "reference" else 0, knn_mode=0,
+                                    sample_stride=stride, return_stats=True)
+            t += st["knn_seconds"] + st["cell_seconds"]
+            cells += st["pass_cells"][0]
+        return t, cells
+
+    for _ in range(args.warmup):
+        step()
+    times, cells = [], 0
+    for _ in range(args.steps):
+        t, cells = step()
+        times.append(t)
+    t = sum(times) / len(times)
+    value = cells / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 half-space predicate, VHSAlgo 2)",
+        "data": "synthetic", "config": {"workload": args.config, "description": cfg["desc"]},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": os.cpu_count(), "kind": kind,
+                         "sample": f"{cells} cells per step: every 16th diagram ({len(jobs)}), each sampled to "
+                                   f"about 6000 binned seeds, all passes"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args, cfg, rank):
     """Serving loop: requests arrive by a seeded Poisson process and are
     submitted at their arrival times; the server's own clock gives each
@@ -487,6 +726,11 @@ def main():
                 print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop"}))
             return
         run_serve(args, cfg, rank)
+    elif cfg.get("kind") == "batch":
+        if args.impl == "reference":
+            run_batch_reference(args, cfg, rank)
+        else:
+            run_batch(args, cfg, rank, world, local)
     elif args.impl == "reference":
         run_reference(args, cfg, rank, world)
     else:

@@ -49,6 +49,7 @@ constexpr int kDeferred = 100;      // internal status: cell parked for k_cone
 
 struct Layout {
   int Pc, Vc, G, Mw;  // Mw: 32-bit words of one plane's edge mask
+  int T;              // triangle cap the layout holds (parked slots)
   unsigned o_plane, o_cx, o_cy, o_cz, o_cw, o_d2, o_tri, o_next, o_emask, o_rem, o_hole, o_edge;
   unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist, o_pts, o_fstart, o_fv, o_pnb;
   unsigned total;
@@ -68,6 +69,7 @@ __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
   L.Vc = (V + 31) & ~31;
   L.G = grid ? pow2_at_least(2 * T) : 0;
   L.Mw = (L.Pc + 31) / 32;
+  L.T = T;
   unsigned o = 0;
   L.o_plane = o; o = align16(o + 32u * L.Pc);
   L.o_cx = o; o = align16(o + 8u * L.Vc);
@@ -1469,7 +1471,7 @@ struct DeferHeader {
   int sid, nuniq, nv, np;
   double pt0[3];
   double acc[4];
-  int inner, pad_i;
+  int inner, diag;  // diag: index of the cell's diagram in a batched launch
   double pad[8];
 };
 static_assert(sizeof(DeferHeader) == 144, "defer header size");
@@ -1478,8 +1480,9 @@ __host__ __device__ inline size_t slot_bytes_for(const Layout &L, int T) {
   return size_t(align16(unsigned(sizeof(DeferHeader) + 32u * L.Pc + 44u * L.Vc + 4u * ((T + 3) & ~3) + 4u * L.Pc)));
 }
 
-__device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, const Layout &L, int T, int sid,
+__device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, const Layout &L, int diag, int sid,
                           int nuniq, bool inner, const double acc[4], int lane) {
+  const int T = L.T;
   unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
   DeferHeader *h = reinterpret_cast<DeferHeader *>(base);
   Plane *pl = reinterpret_cast<Plane *>(base + sizeof(DeferHeader));
@@ -1493,6 +1496,7 @@ __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, con
     h->nv = w.nv;
     h->np = w.np;
     h->inner = inner ? 1 : 0;
+    h->diag = diag;
     for (int d = 0; d < 3; ++d) h->pt0[d] = w.pts[d];
     for (int d = 0; d < 4; ++d) h->acc[d] = acc[d];
   }
@@ -1658,7 +1662,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     if (lane == 0) slot = atomicAdd(&dq.counters[0], 1);
     slot = __shfl_sync(kFull, slot, 0);
     if (slot < dq.capacity) {
-      park_cell(w, dq, slot, L, a.T, sid_of_cell, nuniq, inner, acc, lane);
+      park_cell(w, dq, slot, L, a.diag, sid_of_cell, nuniq, inner, acc, lane);
       return kDeferred;
     }
   }
@@ -1673,8 +1677,18 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     }
     const int bk_nv = w.nv, bk_np = w.np;
     backup<VS>(w, lane);
-    int fail_at = 0;
-    return cone_triangles<VS>(w, a, s, w.tlist, 0, nuniq, bk_nv, bk_np, inner, acc, fail_at, lane, ctr, tr, trcap);
+    // the triangles in chunks of 32, each summed on its own and then added,
+    // as k_cone sums a parked cell: a cell's result does not depend on
+    // whether it was parked
+    for (int c0 = 0; c0 < nuniq; c0 += 32) {
+      double part[4] = {0, 0, 0, 0};
+      int fail_at = 0;
+      const int st = cone_triangles<VS>(w, a, s, w.tlist, c0, min(nuniq, c0 + 32), bk_nv, bk_np, inner, part,
+                                        fail_at, lane, ctr, tr, trcap);
+      if (st != kSuccess) return st;
+      for (int d = 0; d < 4; ++d) acc[d] += part[d];
+    }
+    return kSuccess;
   }
 }
 
@@ -1693,17 +1707,25 @@ __device__ __forceinline__ void mark_neighbours(unsigned char *used, const unsig
   }
 }
 
+// The vertex capacity a cell of this launch works with.  A batched launch's
+// layout may hold more vertices than a diagram's cap (it is sized for every
+// diagram); capacity-dependent choices follow the diagram's own cap, so a
+// cell's result does not depend on the other diagrams of its batch.
+__device__ __forceinline__ int vertex_capacity(const CellLaunch &a, const Layout &L) {
+  return min(L.Vc, (a.V + 31) & ~31);
+}
+
+// One row of a cell launch (one warp): clip, restrict, integrate, write.
+// `only_status` >= 0: skip the row unless its cell has that status; vc:
+// the vertex capacity (vertex_capacity).
 template <int VS, bool GRID, bool INL>
-__global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (row >= a.num) return;
-  WarpCell w = bind(smem + size_t(wib) * L.total, L);
+__device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, unsigned char *wsmem, int row,
+                                         int only_status, int vc, int lane) {
+  WarpCell w = bind(wsmem, L);
+  w.vc = vc;
   unsigned long long *ctr = a.counters;
   const int sid = a.ids ? a.ids[row] : row;
-  if (a.only_status >= 0 && a.status[sid] != a.only_status) return;
+  if (only_status >= 0 && a.status[sid] != only_status) return;
   const float4 s = a.stored[sid];
   double *tr = (a.trace && sid == a.trace_seed) ? a.trace : nullptr;
   const int trcap = a.trace_cap;
@@ -1820,17 +1842,59 @@ __global__ void __launch_bounds__(128, 5) k_cell(CellLaunch a, Layout L) {
   }
 }
 
+template <int VS, bool GRID, bool INL>
+__global__ void __launch_bounds__(128, 5) k_cell(const __grid_constant__ CellLaunch a, const __grid_constant__ Layout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= a.num) return;
+  cell_row<VS, GRID, INL>(a, L, smem + size_t(threadIdx.x >> 5) * L.total, row, a.only_status, L.Vc, lane);
+}
+
+// Rows of many diagrams in one persistent launch (batched solves): diagram
+// d owns rows start[d] .. start[d+1] and its own launch record descs[d];
+// warps stride over the rows.  park_counter (optional): the re-run of the
+// cells that found the defer queue full, which exits unless the queue
+// overflowed.
+template <int VS, bool GRID, bool INL>
+__global__ void __launch_bounds__(128, 5)
+    k_cell_batch(const CellLaunch *__restrict__ descs, const int *__restrict__ start, int ndiag,
+                 const __grid_constant__ Layout L, int only_status, const int *__restrict__ park_counter,
+                 int park_capacity) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (park_counter && *park_counter <= park_capacity) return;
+  const int lane = threadIdx.x & 31;
+  unsigned char *wsmem = smem + size_t(threadIdx.x >> 5) * L.total;
+  const int total = start[ndiag];
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < total; r += nwarps) {
+    const int d = owner_of_row(start, ndiag, r);
+    const CellLaunch &a = descs[d];
+    cell_row<VS, GRID, INL>(a, L, wsmem, r - start[d], only_status, vertex_capacity(a, L), lane);
+    __syncwarp();  // the warp's shared memory is reused by its next row
+  }
+}
+
 // Triangles of the parked boundary cells, CH at a time: every warp takes
 // work items (cell, chunk) from a counter, loads the cell into its shared
 // memory and runs the chunk's cones.  Partial moments and the first failure
 // go to per-item slots; k_cone_finish reduces them in order.
-template <int VS>
-__global__ void __launch_bounds__(128, 4) k_cone(CellLaunch a, Layout L) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  WarpCell w = bind(smem + size_t(wib) * L.total, L);
-  const DeferQueue &dq = a.defer;
+// Launch-record accessors: desc(d) is the record of diagram d.
+struct SingleDesc {
+  static constexpr bool kBatch = false;
+  const CellLaunch *a;  // the one record of a single launch
+  __device__ __forceinline__ const CellLaunch &operator()(int) const { return *a; }
+};
+struct BatchDesc {
+  static constexpr bool kBatch = true;
+  const CellLaunch *descs;
+  __device__ __forceinline__ const CellLaunch &operator()(int d) const { return descs[d]; }
+};
+
+template <int VS, class Desc>
+__device__ __forceinline__ void cone_items(const DeferQueue &dq, const Layout &L, Desc desc, unsigned char *wsmem,
+                                           int lane) {
+  WarpCell w = bind(wsmem, L);
   const int parked = min(*(volatile int *)&dq.counters[0], dq.capacity);
   const int items = parked * dq.max_chunks;
   for (;;) {
@@ -1852,6 +1916,8 @@ __global__ void __launch_bounds__(128, 4) k_cone(CellLaunch a, Layout L) {
     const unsigned *vt = reinterpret_cast<const unsigned *>(vd + L.Vc);
     const int *tl = reinterpret_cast<const int *>(vt + L.Vc);
     const bool inner = h->inner != 0;
+    const CellLaunch &a = desc(h->diag);
+    if constexpr (Desc::kBatch) w.vc = vertex_capacity(a, L);
     for (int i = lane; i < np; i += 32) w.plane[i] = pl[i];
     for (int v = lane; v < nv; v += 32) {
       w.cx[v] = vx[v];
@@ -1895,15 +1961,27 @@ __global__ void __launch_bounds__(128, 4) k_cone(CellLaunch a, Layout L) {
   }
 }
 
+template <int VS>
+__global__ void __launch_bounds__(128, 4) k_cone(const __grid_constant__ CellLaunch a, const __grid_constant__ Layout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  cone_items<VS>(a.defer, L, SingleDesc{&a}, smem + size_t(threadIdx.x >> 5) * L.total, threadIdx.x & 31);
+}
+
+template <int VS>
+__global__ void __launch_bounds__(128, 4)
+    k_cone_batch(const CellLaunch *__restrict__ descs, const __grid_constant__ DeferQueue dq,
+                 const __grid_constant__ Layout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  cone_items<VS>(dq, L, BatchDesc{descs}, smem + size_t(threadIdx.x >> 5) * L.total, threadIdx.x & 31);
+}
+
 // Per parked cell: its in-domain part plus the chunk partials in order; the
 // first failing chunk decides the status (the reference stops at the first
 // failing triangle, ConvexCell.cl:1104-1107).
-__global__ void k_cone_finish(CellLaunch a, Layout L) {
-  const DeferQueue &dq = a.defer;
-  const int parked = min(dq.counters[0], dq.capacity);
-  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= parked) return;
+template <class Desc>
+__device__ __forceinline__ void finish_slot(const DeferQueue &dq, const Layout &L, Desc desc, int slot) {
   const DeferHeader *h = reinterpret_cast<const DeferHeader *>(dq.slots + size_t(slot) * dq.slot_bytes);
+  const CellLaunch &a = desc(h->diag);
   const int sid = h->sid, nch = (h->nuniq + dq.chunk - 1) / dq.chunk;
   double acc[4] = {h->acc[0], h->acc[1], h->acc[2], h->acc[3]};
   int status = kSuccess;
@@ -1931,10 +2009,23 @@ __global__ void k_cone_finish(CellLaunch a, Layout L) {
       const double *vx = reinterpret_cast<const double *>(base + sizeof(DeferHeader) + 32u * L.Pc);
       const unsigned *vt = reinterpret_cast<const unsigned *>(vx + 5 * size_t(L.Vc));
       const int *tl = reinterpret_cast<const int *>(vt + L.Vc);
-      const int *nb = tl + ((a.T + 3) & ~3);
+      const int *nb = tl + ((L.T + 3) & ~3);
       mark_neighbours(a.used, vt, h->nv, nb, 1, 0, 1);
     }
   }
+}
+
+__global__ void k_cone_finish(const __grid_constant__ CellLaunch a, const __grid_constant__ Layout L) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= min(a.defer.counters[0], a.defer.capacity)) return;
+  finish_slot(a.defer, L, SingleDesc{&a}, slot);
+}
+
+__global__ void k_cone_finish_batch(const CellLaunch *__restrict__ descs, const __grid_constant__ DeferQueue dq,
+                                    const __grid_constant__ Layout L) {
+  const int parked = min(dq.counters[0], dq.capacity);
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < parked; slot += gridDim.x * blockDim.x)
+    finish_slot(dq, L, BatchDesc{descs}, slot);
 }
 
 // Raises a kernel's dynamic shared memory limit to the device's opt-in
@@ -1958,9 +2049,21 @@ cudaError_t allow_smem(const void *fn, size_t smem) {
   return cudaSuccess;
 }
 
+// Warps per block for a per-warp layout: 4 where they fit the shared memory
+// of one block, else fewer (large caps); 0 when one warp does not fit.
+int warps_per_block_for(const Layout &L) {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  int w = 4;
+  while (w > 0 && size_t(L.total) * w > size_t(optin)) w >>= 1;
+  return w;
+}
+
 template <int VS>
 cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int sm_count, int *launches) {
-  const int warps_per_block = 4;
+  const int warps_per_block = warps_per_block_for(L);
+  if (warps_per_block == 0) return cudaErrorInvalidValue;
   const size_t smem = size_t(L.total) * warps_per_block;
   const int blocks = (a.num + warps_per_block - 1) / warps_per_block;
   cudaError_t e;
@@ -1991,9 +2094,89 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
   return cudaGetLastError();
 }
 
+// Blocks of a persistent launch: as many as stay resident on every SM.
+template <class Kernel>
+int resident_blocks(Kernel k, int threads, size_t smem, int sm_count) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return per_sm * sm_count;
+}
+
+template <int VS, bool GRID, bool INL>
+cudaError_t batch_cells(const CellLaunch *descs, const int *start, int ndiag, const Layout &L, int only_status,
+                        const int *park_counter, int park_capacity, cudaStream_t st, int sm_count) {
+  const int wpb = warps_per_block_for(L);
+  if (wpb == 0) return cudaErrorInvalidValue;
+  const size_t smem = size_t(L.total) * wpb;
+  auto k = k_cell_batch<VS, GRID, INL>;
+  cudaError_t e = allow_smem(reinterpret_cast<const void *>(k), smem);
+  if (e != cudaSuccess) return e;
+  k<<<resident_blocks(k, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(descs, start, ndiag, L, only_status,
+                                                                         park_counter, park_capacity);
+  return cudaGetLastError();
+}
+
+cudaError_t record_after_cell(const CellBatch &b, cudaStream_t st) {
+  // an event node when the stream is being captured
+  return b.after_cell ? cudaEventRecordWithFlags(b.after_cell, st, cudaEventRecordExternal) : cudaSuccess;
+}
+
+template <int VS>
+cudaError_t launch_batch_vs(const CellBatch &b, const Layout &Lg, const Layout &Lp, cudaStream_t st, int sm_count,
+                            int *launches) {
+  cudaError_t e;
+  if (b.start_plain) {
+    if ((e = batch_cells<VS, false, true>(b.descs_inline, b.start_plain, b.ndiag, Lp, -1, nullptr, 0, st,
+                                          sm_count)) != cudaSuccess)
+      return e;
+    if (launches) ++*launches;
+  }
+  if (!b.start_grid) return record_after_cell(b, st);
+  if (!b.defer.slots) {
+    if ((e = batch_cells<VS, true, true>(b.descs_inline, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, st,
+                                         sm_count)) != cudaSuccess)
+      return e;
+    if (launches) ++*launches;
+    return record_after_cell(b, st);
+  }
+  // every boundary cell parks; the chunked kernel does the triangles, then
+  // the cells that found the queue full run again inline
+  if ((e = batch_cells<VS, true, false>(b.descs, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, st, sm_count)) !=
+      cudaSuccess)
+    return e;
+  if ((e = record_after_cell(b, st)) != cudaSuccess) return e;
+  const int wpb = warps_per_block_for(Lg);
+  const size_t smem = size_t(Lg.total) * wpb;
+  auto kc = k_cone_batch<VS>;
+  if ((e = allow_smem(reinterpret_cast<const void *>(kc), smem)) != cudaSuccess) return e;
+  kc<<<resident_blocks(kc, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(b.descs, b.defer, Lg);
+  k_cone_finish_batch<<<sm_count * 4, 128, 0, st>>>(b.descs, b.defer, Lg);
+  if ((e = batch_cells<VS, true, true>(b.descs_inline, b.start_grid, b.ndiag, Lg, kParkOverflow, b.defer.counters,
+                                       b.defer.capacity, st, sm_count)) != cudaSuccess)
+    return e;
+  if (launches) *launches += 4;
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 size_t cell_warp_smem(int P, int V, int T, bool grid) { return make_layout(P, V, T, grid).total; }
+
+bool cell_caps_fit(int P, int V, int T, bool grid) { return warps_per_block_for(make_layout(P, V, T, grid)) > 0; }
+
+cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches) {
+  if (b.ndiag <= 0) return cudaSuccess;
+  if (b.P > kMaxP || b.V > kMaxV || b.T > kMaxT || b.P < 7 || b.V < 8) return cudaErrorInvalidValue;
+  const Layout Lg = make_layout(b.P, b.V, b.T, true), Lp = make_layout(b.P, b.V, b.T, false);
+  if (b.defer.slots && b.defer.slot_bytes < slot_bytes_for(Lg, b.T)) return cudaErrorInvalidValue;
+  const int vs = Lg.Vc / 32;
+  if (vs <= 2) return launch_batch_vs<2>(b, Lg, Lp, st, sm_count, launches);
+  if (vs <= 3) return launch_batch_vs<3>(b, Lg, Lp, st, sm_count, launches);
+  if (vs <= 4) return launch_batch_vs<4>(b, Lg, Lp, st, sm_count, launches);
+  if (vs <= 6) return launch_batch_vs<6>(b, Lg, Lp, st, sm_count, launches);
+  return launch_batch_vs<8>(b, Lg, Lp, st, sm_count, launches);
+}
 
 size_t defer_slot_bytes(int P, int V, int T) { return slot_bytes_for(make_layout(P, V, T, true), T); }
 

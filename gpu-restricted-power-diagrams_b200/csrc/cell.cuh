@@ -84,6 +84,7 @@ struct CellLaunch {
   double keep_volume = 0.0;
   int mark_dist = 0;
   int border_d = 0;
+  int diag = 0;  // index of this diagram in a batched launch (parked cells record it)
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
 constexpr int kTraceRecord = 12;
@@ -101,5 +102,24 @@ size_t defer_slot_bytes(int P, int V, int T);
 // k_cell over the rows; with a domain and a defer queue, also the chunked
 // boundary-triangle kernel and the per-cell reduction (3 launches).
 cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count = 148, int *launches = nullptr);
+
+// Whether one warp's layout for these caps fits a block's shared memory.
+bool cell_caps_fit(int P, int V, int T, bool grid);
+
+// The cells of many diagrams in shared persistent launches (batched
+// solves).  Row prefixes and launch records live on the device, written by
+// earlier kernels of the same stream, so the launches can be captured in a
+// graph before their row counts are known.
+struct CellBatch {
+  const CellLaunch *descs = nullptr;         // ndiag records; defer = the shared queue
+  const CellLaunch *descs_inline = nullptr;  // the same records without the queue
+  const int *start_grid = nullptr;   // ndiag+1 row prefixes of the diagrams with a domain (null: none)
+  const int *start_plain = nullptr;  // ndiag+1 row prefixes of the diagrams without one (null: none)
+  int ndiag = 0;
+  DeferQueue defer;                  // slots == null: every boundary cell inline
+  int P = 0, V = 0, T = 0;           // layout caps: at least every diagram's caps of this pass
+  cudaEvent_t after_cell = nullptr;  // recorded (as a graph node when capturing) after the cell kernel
+};
+cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches = nullptr);
 
 }  // namespace rpd

@@ -28,6 +28,19 @@ constexpr unsigned kFull = 0xffffffffu;
 // Bins per axis of the seed grid: round((n / 3.1)^(1/3)) (knearests.cpp:63).
 int bins_per_axis(int n);
 
+// Batched launches: diagram d owns rows start[d] .. start[d+1]; the owner of
+// row r (0 <= r < start[ndiag]) is the last d with start[d] <= r, which
+// skips diagrams without rows.
+__device__ __forceinline__ int owner_of_row(const int *__restrict__ start, int ndiag, int r) {
+  int lo = 0, hi = ndiag - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= r) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 }  // namespace rpd
 
 #define RPD_CUDA_TRY(expr)                                   \

@@ -116,17 +116,12 @@ struct ShellRows {
   }
 };
 
+// The K nearest of stored seed `pin` into row[0..K) (one warp).
 template <int S>
-__global__ void __launch_bounds__(256) k_knn(const float4 *__restrict__ stored, const int *__restrict__ counters,
-                                             int dim, const int *__restrict__ ids, int num, int K,
-                                             const float *__restrict__ ring_bound, unsigned *__restrict__ out,
-                                             unsigned long long *__restrict__ candidates) {
-  __shared__ unsigned long long stage_buf[kKnnThreads / 32][32];
-  const int lane = threadIdx.x & 31;
-  unsigned long long *stage = stage_buf[threadIdx.x >> 5];
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= num) return;  // warp-uniform
-  const int pin = ids ? ids[w] : w;
+__device__ __forceinline__ void knn_row(const float4 *__restrict__ stored, const int *__restrict__ counters, int dim,
+                                        int pin, int K, const float *__restrict__ ring_bound, unsigned *__restrict__ row,
+                                        unsigned long long *__restrict__ candidates, unsigned long long *stage,
+                                        int lane) {
   const float4 p = stored[pin];
   const int cin = bin_of(p, dim);
   ShellRows sh;
@@ -216,7 +211,6 @@ __global__ void __launch_bounds__(256) k_knn(const float4 *__restrict__ stored, 
       kth = key_at<S>(best, K - 1);
     }
   }
-  unsigned *row = out + size_t(w) * K;
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const int pos = s * 32 + lane;
@@ -226,6 +220,39 @@ __global__ void __launch_bounds__(256) k_knn(const float4 *__restrict__ stored, 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(kFull, ncand, o);
     if (lane == 0) atomicAdd(candidates, ncand);
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) k_knn(const float4 *__restrict__ stored, const int *__restrict__ counters,
+                                             int dim, const int *__restrict__ ids, int num, int K,
+                                             const float *__restrict__ ring_bound, unsigned *__restrict__ out,
+                                             unsigned long long *__restrict__ candidates) {
+  __shared__ unsigned long long stage_buf[kKnnThreads / 32][32];
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= num) return;  // warp-uniform
+  const int pin = ids ? ids[w] : w;
+  knn_row<S>(stored, counters, dim, pin, K, ring_bound, out + size_t(w) * K, candidates, stage_buf[threadIdx.x >> 5],
+             lane);
+}
+
+// Rows of many diagrams (batched solves): the diagrams of slot class S own
+// rows start[d] .. start[d+1] of this launch; warps stride over them.
+template <int S>
+__global__ void __launch_bounds__(256) k_knn_batch(const KnnDiag *__restrict__ diags, const int *__restrict__ start,
+                                                   int ndiag) {
+  __shared__ unsigned long long stage_buf[kKnnThreads / 32][32];
+  const int lane = threadIdx.x & 31;
+  const int total = start[ndiag];
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < total; r += nwarps) {
+    const int d = owner_of_row(start, ndiag, r);
+    const KnnDiag &g = diags[d];
+    const int i = r - start[d];
+    const int pin = g.ids ? g.ids[i] : i;
+    knn_row<S>(g.stored, g.counters, g.dim, pin, g.K, g.ring_bound, g.out + size_t(i) * g.K, nullptr,
+               stage_buf[threadIdx.x >> 5], lane);
   }
 }
 
@@ -252,6 +279,19 @@ void ring_bounds(int dim, float *bound) {
     const float d = 1000.f * float(ring - 1) / float(dim);
     bound[ring] = d * d;
   }
+}
+
+cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st) {
+  switch (S) {
+    case 1: k_knn_batch<1><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;
+    case 2: k_knn_batch<2><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;
+    case 3: k_knn_batch<3><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;
+    case 4: k_knn_batch<4><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;
+    case 6: k_knn_batch<6><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;
+    case 8: k_knn_batch<8><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t knn_launch(const float4 *stored, const int *counters, int dim, const int *ids, int num, int K,

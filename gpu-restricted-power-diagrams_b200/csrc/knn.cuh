@@ -21,4 +21,23 @@ void ring_bounds(int dim, float *bound);
 cudaError_t knn_launch(const float4 *stored, const int *counters, int dim, const int *ids, int num, int K,
                        const float *ring_bound, unsigned *out, unsigned long long *candidates, cudaStream_t st);
 
+// One diagram of a batched neighbour launch: rows are ids[0..) (null: the
+// seeds 0..), row i written to out + i*K.
+struct KnnDiag {
+  const float4 *stored;
+  const int *counters;
+  int dim;
+  int K;
+  const int *ids;
+  const float *ring_bound;
+  unsigned *out;
+};
+// Slot classes of knn_slots, in order.
+constexpr int kKnnClasses = 6;
+constexpr int kKnnClassSlots[kKnnClasses] = {1, 2, 3, 4, 6, 8};
+// Persistent launch over the rows of every diagram of slot class S:
+// start[0..ndiag] (device) are the row prefixes of the diagrams in this
+// class (empty for the others); `blocks` fixed, the rows read on the device.
+cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st);
+
 }  // namespace rpd

@@ -100,6 +100,11 @@ def lib():
         L.rpd_solver_get_status.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_get_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.rpd_solver_trace_cell.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.rpd_batch_create.restype = C.c_void_p
+        L.rpd_batch_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+        L.rpd_batch_launch.argtypes = [C.c_void_p]
+        L.rpd_batch_get_stats.argtypes = [C.c_void_p, C.c_void_p]
+        L.rpd_batch_destroy.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -301,6 +306,63 @@ class Solver:
     def close(self):
         if self.h:
             lib().rpd_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("diagrams", C.c_int), ("cells", C.c_longlong), ("graph_ms", C.c_float),
+                ("passes_captured", C.c_int), ("max_passes", C.c_int), ("kernel_launches", C.c_int),
+                ("captures", C.c_int), ("solved_alone", C.c_int), ("pass0_knn_ms", C.c_float),
+                ("pass0_cell_kernel_ms", C.c_float), ("pass_ms", C.c_float * 8), ("pass_cells", C.c_longlong * 8)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pass_ms", "pass_cells")}
+        n = min(self.passes_captured, 8)
+        d["passes"] = [{"cells": int(self.pass_cells[i]), "ms": self.pass_ms[i]} for i in range(n)]
+        return d
+
+
+class Batch:
+    """Many independent diagrams solved together (rpd_batch_*): every pass of
+    every solver in shared launches, the whole solve one CUDA graph replayed
+    at each launch.  Each solver afterwards holds the results its own
+    launch(params) would give."""
+
+    def __init__(self, solvers, params=None, ctx: Context | None = None):
+        self.solvers = list(solvers)
+        self.ctx = ctx or self.solvers[0].ctx
+        n = len(self.solvers)
+        hs = (C.c_void_p * n)(*[s.h for s in self.solvers])
+        if params is None:
+            pa = None
+        else:
+            if isinstance(params, Params):
+                params = [params] * n
+            pa = (Params * n)(*params)
+        err = C.c_int(0)
+        self.h = lib().rpd_batch_create(self.ctx.h, hs, pa, n, C.byref(err))
+        if not self.h:
+            raise RpdError(err.value, self.ctx.error())
+        self._keep = (hs, pa)
+
+    def launch(self):
+        self.ctx.check(lib().rpd_batch_launch(self.h))
+        return self
+
+    def stats(self) -> dict:
+        st = BatchStats()
+        self.ctx.check(lib().rpd_batch_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self.h:
+            lib().rpd_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

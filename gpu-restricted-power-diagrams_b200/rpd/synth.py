@@ -57,3 +57,28 @@ def to_unit(xyzw: np.ndarray) -> np.ndarray:
     out[..., :3] *= 1.0 / SCALE ** 4
     out[..., 3] *= 1.0 / SCALE ** 3
     return out
+
+
+def uneven_batch(count: int, seed: int = 4, nmin: int = 1000, nmax: int = 200_000, gmin: int = 64, gmax: int = 160,
+                 ks=(20, 50, 70)):
+    """`count` independent diagram specs of the batched workload: seed counts
+    log-uniform in [nmin, nmax]; positions uniform or jittered-lattice
+    (alternating), weights U[0, 0.1 h^2] with h the diagram's spacing
+    n^(-1/3); a seeded ellipsoid-blob domain of gmin..gmax voxels per axis; K
+    from `ks`.  Returns dicts {xyzw, grid_size, grid_seed, K}."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+        s = int(rng.integers(1 << 30))
+        if i % 2 == 0:
+            x = uniform(n, seed=s)
+        else:
+            m = max(2, int(round(n ** (1.0 / 3.0))))
+            x = jittered_lattice(m, seed=s, weights=False)
+        h = len(x) ** (-1.0 / 3.0)
+        w = np.random.default_rng(s + 1).uniform(0.0, 0.1 * h * h, size=len(x))
+        x[:, 3] = (w * SCALE * SCALE).astype(np.float32)
+        specs.append({"xyzw": x, "grid_size": int(rng.integers(gmin, gmax + 1)), "grid_seed": int(rng.integers(1 << 20)),
+                      "K": int(ks[int(rng.integers(len(ks)))])})
+    return specs

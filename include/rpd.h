@@ -285,6 +285,45 @@ int rpd_server_release(rpd_server *sv, int session);
 /* Device bytes held by resident sessions, grids and admitted requests. */
 size_t rpd_server_bytes_in_use(rpd_server *sv);
 
+/* -------------------------------------------------------- batched solves */
+
+/* Many independent diagrams solved together (no counterpart in the
+ * reference, which solves one diagram per VoroAlgo::launch).  The solvers
+ * belong to one context; each keeps its own seeds, domain and caps (params[i]
+ * for solvers[i]; NULL: defaults for all).  Every pass of every diagram runs
+ * in shared persistent launches -- one neighbour launch per K class, one cell
+ * launch, the cone kernels, the failing-cell compaction -- and the retry
+ * schedule (cap growth, failing-cell lists) is decided on the device, so the
+ * whole solve is one CUDA graph, captured at the first rpd_batch_launch and
+ * replayed after.  Each solver then holds exactly the results
+ * rpd_solver_launch would give it (statuses, moments, stats' passes and
+ * histogram), read with the solver's own getters.  Changing a solver's seeds
+ * or domain is allowed between launches (the graph is captured again);
+ * changing weights (rpd_solver_set_weights) is not a change.  Not supported:
+ * RPD_FLAG_COUNTERS and used cells (keep_distance >= 0 with a domain). */
+typedef struct rpd_batch rpd_batch;
+typedef struct rpd_batch_stats {
+  int diagrams;
+  long long cells;      /* seeds of all diagrams */
+  float graph_ms;       /* device time of the last replay */
+  int passes_captured;  /* passes in the graph */
+  int max_passes;       /* most passes a diagram ran */
+  int kernel_launches;  /* kernels per replay */
+  int captures;         /* graph captures so far */
+  int solved_alone;     /* diagrams whose retries outgrew the graph, solved after it on their own */
+  float pass0_knn_ms;   /* of graph_ms: the first pass's neighbour launches */
+  float pass0_cell_kernel_ms; /* of graph_ms: the first pass's cell kernel (no cone kernels) */
+  float pass_ms[8];     /* of graph_ms: each captured pass (plan, neighbours, cells, compaction) */
+  long long pass_cells[8]; /* cells of each pass, all diagrams */
+} rpd_batch_stats;
+
+rpd_batch *rpd_batch_create(rpd_context *ctx, rpd_solver *const *solvers, const rpd_params *params, int count,
+                            int *err);
+/* Solves every diagram; synchronous. */
+int rpd_batch_launch(rpd_batch *b);
+int rpd_batch_get_stats(const rpd_batch *b, rpd_batch_stats *st);
+void rpd_batch_destroy(rpd_batch *b);
+
 /* Debugging: re-runs one seed's cell (user id) with the caps of `p` and
  * records every clip and integration into `records` (cap records of 12
  * doubles: kind 0 seed, 1 plane test, 2 cavity, 3 vertex, 4 integration,
