@@ -42,6 +42,7 @@ class OracleParams(C.Structure):
         ("knn_mode", C.c_int), ("max_extra_passes", C.c_int), ("first_pass_only", C.c_int),
         ("cube_eps", C.c_double), ("nthreads", C.c_int), ("sample_stride", C.c_int),
         ("used_cells", C.c_int), ("keep_distance", C.c_int), ("keep_volume", C.c_double),
+        ("H", C.c_int), ("HC", C.c_int),
     ]
 
 
@@ -135,6 +136,30 @@ def solve(xyzw, grid=None, K=20, P=25, V=30, T=100, vhs0=2, vhs1=2, use_double=F
     if rc != 0:
         raise RuntimeError(f"oracle_solve failed: {rc}")
     return (bary, status, st.as_dict()) if return_stats else (bary, status)
+
+
+def solve_hessian(xyzw, grid=None, H=50, HC=1, K=20, P=25, V=30, T=100, use_double=True, kernels=0, knn_mode=1,
+                  max_extra_passes=5, cube_eps=None, nthreads=0):
+    """oracle solve with --hessian (ConvexCell.cl:621-678,1133-1150): returns
+    (bary, status, hess, ids) in user order; hess (n, H) areas for HC=1 or
+    (n, H, 4) area-weighted facet centroids and areas for HC=4; ids (n, H)
+    the facets' neighbours as user ids, -1 after a row's last facet."""
+    x = np.ascontiguousarray(np.asarray(xyzw, dtype=np.float64).reshape(-1, 4))
+    n = len(x)
+    bary = np.zeros((n, 4), np.float64)
+    status = np.zeros(n, np.int32)
+    hess = np.zeros((n, H, HC), np.float64)
+    ids = np.full((n, H), -1, np.int32)
+    if cube_eps is None:
+        cube_eps = 0.1 if grid is not None else 0.0
+    prm = OracleParams(K, P, V, T, 2, 2, int(use_double), kernels, knn_mode, max_extra_passes, 0, cube_eps, nthreads,
+                       1, 0, -1, 0.0, H, HC)
+    gv = grid.view() if grid is not None else None
+    rc = lib().oracle_solve_hessian(_ptr(x), n, C.byref(gv) if gv is not None else None, C.byref(prm), _ptr(bary),
+                                    _ptr(status), _ptr(hess), _ptr(ids), None)
+    if rc != 0:
+        raise RuntimeError(f"oracle_solve_hessian failed: {rc}")
+    return bary, status, (hess[:, :, 0] if HC == 1 else hess), ids
 
 
 def solve_used(xyzw, grid, keep_distance=0, keep_volume=0.001, K=20, P=25, V=30, T=100, use_double=True, kernels=0,

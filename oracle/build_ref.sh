@@ -23,13 +23,14 @@ CXX="${RPD_HOST_CXX:-/usr/bin/g++}"
 FLAGS=(-std=c++17 -O2 -fPIC -fopenmp -ffp-contract=off -fno-fast-math -w
        -D__OPENCL_VERSION__=120 -I"$HERE/shim" -I"$REF")
 
-cell() {  # name real vhs grid outdomain [used-cell distance]
-  local name=$1 real=$2 vhs=$3 grid=$4 outd=$5 used=${6:-}
+cell() {  # name real vhs grid outdomain [used-cell distance] [hessian components]
+  local name=$1 real=$2 vhs=$3 grid=$4 outd=$5 used=${6:-} hc=${7:-}
   local defs=(-DREF_REAL=$real -DVHSAlgo=$vhs -DREF_CELL_ENTRY=ref_cell_$name)
   [ "$real" = double ] && defs+=(-DREF_IS_DOUBLE=1)
   [ "$grid" = 1 ] && defs+=(-DUSE_GRID)
   [ "$outd" = 1 ] && defs+=(-DGRID_OUT_DOMAIN)
   [ -n "$used" ] && defs+=(-DCUSED_CELL -DCUSED_CELL_DIST=$used)
+  [ -n "$hc" ] && defs+=(-DCHESSIAN -DHC=$hc)
   { echo '#include "cl_prelude.h"'
     echo '#include "Status.h"'
     echo "namespace ref_cell_ns_$name {"
@@ -68,6 +69,12 @@ cell d_grid_used1 double 2 1 0 1 & pids+=($!)
 cell d_gridout_used1 double 2 1 1 1 & pids+=($!)
 cell d_border2 double 2 0 0 2 & pids+=($!)
 cell d_border3 double 2 0 0 3 & pids+=($!)
+# --hessian (voronoi.cpp:930-936): HC 1 and 4, with and without a grid
+for hc in 1 4; do
+  cell d_nogrid_h$hc double 2 0 0 "" $hc & pids+=($!)
+  cell d_grid_h$hc double 2 1 0 "" $hc & pids+=($!)
+  cell d_gridout_h$hc double 2 1 1 "" $hc & pids+=($!)
+done
 knn f float & pids+=($!)
 knn d double & pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done

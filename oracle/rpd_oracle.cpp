@@ -154,8 +154,13 @@ struct Cell {
   std::vector<uint8_t> next;
   int nb_vertex = 0, nb_plane = 0;
   Counters *cnt = nullptr;
+  // --hessian: facet integrals per plane, HC values each (neighb_intr,
+  // ConvexCell.cl:1059-1066); hc == 0: off
+  int hc = 0;
+  mutable std::vector<R> intr;
 
   void resize() {
+    if (hc > 0) intr.assign(size_t(hc) * (std::max(capP, 1) + 4), R(0));
     vert.assign(256, {0, 0, 0, 0});
     plane.assign(std::max(capP, 1) + 4, Vec4<R>{0, 0, 0, 0});
     pnb.assign(std::max(capP, 1) + 4, -1);
@@ -433,6 +438,22 @@ struct Cell {
           sum_b.x += w * (A.x + 0.25 * s.x);
           sum_b.y += w * (A.y + 0.25 * s.y);
           sum_b.z += w * (A.z + 0.25 * s.z);
+          if (hc > 0) {
+            // CCExportBaryVolumeAndArea (ConvexCell.cl:621-678): the same
+            // triangle (A, C's foot on plane i, C's foot on the edge line)
+            // in plane i, signed by the plane's normal
+            const R tri_area = (2 * st - 1) * factor * det3v(a_plane[i], a_line[j], pl[i]) / 2;
+            const int pid = ith(ve, i);
+            if (hc == 1) {
+              intr[pid] += tri_area;
+            } else {
+              const Vec4<R> m = add4(a_plane[i], a_line[j]);
+              intr[4 * pid + 0] += tri_area * (A.x + m.x / 3);
+              intr[4 * pid + 1] += tri_area * (A.y + m.y / 3);
+              intr[4 * pid + 2] += tri_area * (A.z + m.z / 3);
+              intr[4 * pid + 3] += tri_area;
+            }
+          }
         }
       }
     }
@@ -485,12 +506,21 @@ void mark_neighbours(const Cell<R> &cc, uint8_t *flags, int d) {
 }
 
 // compute_voro_cell (ConvexCell.cl:812-1116) for one stored seed.
+// Hessian rows of one pass's cells (stored order).
+template <class R>
+struct HessRows {
+  int H = 0, HC = 1;
+  R *vals = nullptr;  // n*H*HC
+  int *ids = nullptr; // n*H
+};
+
 template <class R>
 void voro_cell(Cell<R> &cc, int seed_id, const unsigned *neigs, int K, const GridView<R> *grid, bool out_domain,
                Status *st_all, Vec4<R> *out_all, double vol_eps2, std::vector<int> &tr0, std::vector<int> &tr1,
-               const UsedCells &used) {
+               const UsedCells &used, const HessRows<R> &hr) {
   Status *st = st_all + seed_id;
   *st = success;
+  if (hr.H > 0) hr.ids[size_t(seed_id) * hr.H] = -1;
   const Vec4<R> *pts = cc.pts;
   if (pts[seed_id].w <= kNoCellLimits) {
     out_all[seed_id] = pts[seed_id];
@@ -624,6 +654,7 @@ void voro_cell(Cell<R> &cc, int seed_id, const unsigned *neigs, int K, const Gri
     }
   }
 
+  if (cc.hc > 0) std::fill(cc.intr.begin(), cc.intr.end(), R(0));
   const bool add_volume = grid ? in_domain == 2 : true;
   if (add_volume) cc.export_bary(out_all + seed_id, R(1), vol_eps2);
 
@@ -664,6 +695,23 @@ void voro_cell(Cell<R> &cc, int seed_id, const unsigned *neigs, int K, const Gri
   if (used.flags && out_all[seed_id].w >= R(used.eps)) {
     __atomic_store_n(&used.flags[seed_id], uint8_t(1), __ATOMIC_RELAXED);
     if (used.dist >= 1) mark_neighbours(cc, used.flags, 1);
+  }
+  if (hr.H > 0) {
+    // the row: facets with a neighbour and an area above 0.2, in plane
+    // order; more than H is hessian_overflow (ConvexCell.cl:1133-1150)
+    const int HC = hr.HC;
+    int c = 0;
+    for (int p = 0; p < cc.nb_plane; ++p) {
+      if (cc.pnb[p] < 0 || cc.intr[size_t(HC) * p + HC - 1] <= R(0.2)) continue;
+      if (c >= hr.H) {
+        *st = hessian_overflow;
+        return;
+      }
+      for (int k = 0; k < HC; ++k) hr.vals[(size_t(seed_id) * hr.H + c) * HC + k] = cc.intr[size_t(HC) * p + k];
+      hr.ids[size_t(seed_id) * hr.H + c] = cc.pnb[p];
+      ++c;
+    }
+    if (c < hr.H) hr.ids[size_t(seed_id) * hr.H + c] = -1;
   }
 }
 
@@ -920,6 +968,8 @@ struct Solver {
   std::vector<Vec4<R>> out;
   std::vector<uint8_t> used;  // used-cell marks (stored order) when keep_distance >= 0 with a grid
   UsedCells uc;
+  std::vector<R> hess;        // Hessian rows (stored order) when prm.H > 0
+  std::vector<int> hess_ids;
   OracleStats *stats;
   Counters total;
   // VOLUME_EPSILON2 is a double literal in both builds (voronoi.cpp:919,922).
@@ -993,6 +1043,7 @@ struct Solver {
       else
         name += grid ? (out_domain ? "_gridout" : "_grid") : "_nogrid";
       if (bordering_d == 0 && uc.flags) name += "_used" + std::to_string(uc.dist);
+      if (bordering_d == 0 && prm.H > 0) name += "_h" + std::to_string(prm.HC);
       RefCellFn fn = (RefCellFn)ref_sym(name.c_str());
       if (!fn) return false;
       std::vector<unsigned> uids(ids.begin(), ids.end());
@@ -1021,6 +1072,11 @@ struct Solver {
       a.nthreads = nthreads();
       a.used = uc.flags;
       a.used_eps = uc.eps;
+      if (prm.H > 0) {
+        a.hessian = hess.data();
+        a.hessidx = hess_ids.data();
+        a.h = prm.H;
+      }
       fn(&a);
     } else {
       const int nth = nthreads();
@@ -1036,7 +1092,15 @@ struct Solver {
         cc.cube_eps = R(prm.cube_eps);
         cc.pts = bins.stored.data();
         cc.cnt = &cs[tid];
+        cc.hc = prm.H > 0 ? prm.HC : 0;
         cc.resize();
+        HessRows<R> hr;
+        if (prm.H > 0) {
+          hr.H = prm.H;
+          hr.HC = prm.HC;
+          hr.vals = hess.data();
+          hr.ids = hess_ids.data();
+        }
         std::vector<int> tr0(std::max(T, 1) + 1), tr1(std::max(T, 1) + 1);
 #pragma omp for schedule(dynamic, 256)
         for (int g = 0; g < num; ++g) {
@@ -1044,7 +1108,7 @@ struct Solver {
             border_cell<R>(cc, ids[g], nn.data() + size_t(g) * K, K, st_out, uc.flags, bordering_d);
           else
             voro_cell<R>(cc, ids[g], nn.data() + size_t(g) * K, K, grid, out_domain, status.data(), out.data(),
-                         vol_eps2, tr0, tr1, uc);
+                         vol_eps2, tr0, tr1, uc, hr);
         }
       }
       for (auto &c : cs) {
@@ -1100,6 +1164,10 @@ struct Solver {
     if (make_bins(user, bins, prm.kernels == 1 || prm.knn_mode == 0) < 0) return -2;
     status.assign(n, success);
     out.assign(n, Vec4<R>{0, 0, 0, 0});
+    if (prm.H > 0) {
+      hess.assign(size_t(n) * prm.H * prm.HC, R(0));
+      hess_ids.assign(size_t(n) * prm.H, -1);
+    }
     const bool dbl = std::is_same<R, double>::value;
     // used cells only with a grid (voronoi.cpp:1291); the main passes mark at
     // distance 0 or 1 (voronoi.cpp:1286)
@@ -1189,7 +1257,8 @@ GridView<R> make_grid_view(const OracleGrid *g) {
 
 template <class R>
 int solve_t(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p, double *bary, int *status,
-            OracleStats *stats, unsigned char *used_out = nullptr) {
+            OracleStats *stats, unsigned char *used_out = nullptr, double *hess_out = nullptr,
+            int *hess_ids_out = nullptr) {
   std::vector<Vec4<R>> user(n);
   for (int i = 0; i < n; ++i)
     user[i] = mk<R>(R(xyzw[4 * i]), R(xyzw[4 * i + 1]), R(xyzw[4 * i + 2]), R(xyzw[4 * i + 3]));
@@ -1207,6 +1276,14 @@ int solve_t(const double *xyzw, int n, const OracleGrid *grid, const OracleParam
     bary[4 * u + 3] = double(o.w);
     if (status) status[u] = int(s.status[st]);
     if (used_out) used_out[u] = s.used.empty() ? 0 : s.used[st];
+    if (hess_out && p->H > 0) {
+      const size_t H = size_t(p->H), HC = size_t(p->HC);
+      for (size_t k = 0; k < H * HC; ++k) hess_out[u * H * HC + k] = double(s.hess[st * H * HC + k]);
+      for (size_t k = 0; k < H; ++k) {
+        const int v = s.hess_ids[st * H + k];
+        hess_ids_out[u * H + k] = v < 0 ? -1 : s.bins.perm[v];
+      }
+    }
     if (stats && s.status[st] >= 0 && s.status[st] < kStatusNum) stats->final_status[s.status[st]]++;
   }
   if (stats) {
@@ -1263,6 +1340,14 @@ int oracle_solve_used(const double *xyzw, int n, const OracleGrid *grid, const O
   if (stats) std::memset(stats, 0, sizeof(*stats));
   if (p->use_double) return solve_t<double>(xyzw, n, grid, p, bary, status, stats, used);
   return solve_t<float>(xyzw, n, grid, p, bary, status, stats, used);
+}
+
+int oracle_solve_hessian(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p, double *bary,
+                         int *status, double *hess, int *hess_ids, OracleStats *stats) {
+  if (n <= 0 || !xyzw || !p || !bary || p->H <= 0 || (p->HC != 1 && p->HC != 4) || !hess || !hess_ids) return -1;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (p->use_double) return solve_t<double>(xyzw, n, grid, p, bary, status, stats, nullptr, hess, hess_ids);
+  return solve_t<float>(xyzw, n, grid, p, bary, status, stats, nullptr, hess, hess_ids);
 }
 
 int oracle_knn(const double *xyzw, int n, int K, int use_double, int kernels, int knn_mode, int *knn, int nthreads) {

@@ -46,6 +46,8 @@ typedef struct OracleParams {
   int used_cells;           // 1: mark used cells (needs a grid; voronoi.cpp:1291)
   int keep_distance;        // VoroAlgo::m_keepDistance (>= 0)
   double keep_volume;       // VoroAlgo::m_keepVolume
+  int H;                    // VoroAlgo::m_H: facets per Hessian row, 0 = off (voronoi.h:207)
+  int HC;                   // VoroAlgo::m_HC: 1 (area) or 4 (area-weighted centroid, area)
 } OracleParams;
 
 typedef struct OracleStats {
@@ -72,6 +74,13 @@ int oracle_solve(const double *xyzw, int n, const OracleGrid *grid, const Oracle
 // 0 unused, else the ring distance, 1 for used cells) when p->used_cells.
 int oracle_solve_used(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p, double *bary,
                       int *status, unsigned char *used, OracleStats *stats);
+
+// As oracle_solve, with the Hessian rows of --hessian (p->H > 0;
+// ConvexCell.cl:621-678,1133-1150) in user order: hess n*H*HC (per facet the
+// area, or with HC = 4 the area-weighted centroid and the area), ids n*H
+// (the facet's neighbour as a user id, -1 after the last facet of a row).
+int oracle_solve_hessian(const double *xyzw, int n, const OracleGrid *grid, const OracleParams *p, double *bary,
+                         int *status, double *hess, int *hess_ids, OracleStats *stats);
 
 // K nearest neighbours of every seed, in user ids, ascending distance, -1 when
 // fewer exist.  knn_mode as in OracleParams.

@@ -93,6 +93,7 @@ static thread_local int ref_grid_size;
 static thread_local REF_REAL ref_grid_voxel_size;
 static thread_local REF_REAL ref_cube_epsilon;
 static thread_local REF_REAL ref_used_eps;
+static thread_local int ref_H;  // CHESSIAN builds: the Hessian row length
 static const int ref_one = 1;
 
 struct RefVTag {
@@ -119,6 +120,7 @@ static constexpr RefVTag ref_V_tag{};
 #define GRID_VOXEL_SIZE ref_grid_voxel_size
 #define CUBE_EPSILON ref_cube_epsilon
 #define USED_CELL_EPSILON ref_used_eps
+#define H ref_H
 #define NO_CELL_LIMITS -100000
 #if REF_IS_DOUBLE
 #define VOLUME_EPSILON2 1.e-12

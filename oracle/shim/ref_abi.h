@@ -27,6 +27,9 @@ typedef struct RefCellArgs {
   int nthreads;               // 0 = all
   unsigned char *used;        // CUSED_CELL builds: usedCells[n] (stored order)
   double used_eps;            // USED_CELL_EPSILON
+  void *hessian;              // CHESSIAN builds: real[n*H*HC] (stored order)
+  int *hessidx;               // CHESSIAN builds: int[n*H]
+  int h;                      // H
 } RefCellArgs;
 
 typedef struct RefKnnArgs {
