@@ -50,6 +50,7 @@ void usage(const char *argv0) {
             << "\t--points4D: the seed file has a weight column\n"
             << "\t--keepVolume=v: cells with volume below v are empty (default 1)\n"
             << "\t--keepDist2=d: with --grid, keep the used cells and d rings around them (default 0; -1 all)\n"
+            << "\t--hessian: compute the facet-area rows (--H=h facets per row, default 50; --HC=1|4)\n"
             << "\t--printInvariants --checkGrid --debug\n";
 }
 
@@ -62,6 +63,8 @@ int main(int argc, char **argv) {
   bool points4d = false, invariants = false, check_grid = false, debug = false;
   double keep_volume = 1;
   int keep_dist2 = 0;  // test_voronoi's final keep distance (Options.cpp:42, test_voronoi.cpp:38)
+  bool hessian = false;
+  int H = 50, HC = 1;  // Options.cpp:22-23
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i], val;
     const size_t eq = a.find('=');
@@ -85,6 +88,9 @@ int main(int argc, char **argv) {
     else if (a == "--keepDist2") keep_dist2 = std::atoi(need().c_str());
     else if (a == "--keepDist") (void)need();  // distance of the passes before the last: no effect here
     else if (a == "--points4D") points4d = true;
+    else if (a == "--hessian") hessian = true;
+    else if (a == "--H") H = std::atoi(need().c_str());
+    else if (a == "--HC") HC = std::atoi(need().c_str());
     else if (a == "--printInvariants") invariants = true;
     else if (a == "--checkGrid") check_grid = true;
     else if (a == "--debug") debug = true;
@@ -121,6 +127,8 @@ int main(int argc, char **argv) {
   algo.m_T = T;
   algo.m_keepDistance = keep_dist2;
   algo.m_keepVolume = keep_volume;
+  algo.m_H = hessian ? H : 0;  // Options.cpp:269-270
+  algo.m_HC = HC;
   algo.setInputPoints(pts);
   if (has_grid) algo.setGrid(grid);
   std::vector<double> bary;

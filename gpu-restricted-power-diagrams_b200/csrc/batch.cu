@@ -394,6 +394,10 @@ int check_params(rpd_context *ctx, const rpd_params &p) {
     set_error(ctx, "batched solves collect no work counters (RPD_FLAG_COUNTERS)");
     return RPD_ERR_INVALID;
   }
+  if (p.hessian_h != 0) {
+    set_error(ctx, "batched solves return no Hessian rows (hessian_h > 0): use rpd_solver_launch");
+    return RPD_ERR_INVALID;
+  }
   return RPD_OK;
 }
 
@@ -769,6 +773,7 @@ int rpd_batch_launch(rpd_batch *b) {
     s->knn_full_K = b->params[d].K;
     s->used_on = false;
     s->used_count = -1;
+    s->hess_h = 0;
     s->have_results = true;
   }
   // diagrams whose schedule outgrew the capture: solved alone

@@ -50,6 +50,8 @@ constexpr int kDeferred = 100;      // internal status: cell parked for k_cone
 struct Layout {
   int Pc, Vc, G, Mw;  // Mw: 32-bit words of one plane's edge mask
   int T;              // triangle cap the layout holds (parked slots)
+  int HC;             // Hessian components per facet (0: no Hessian)
+  unsigned o_harea, o_hbuf, o_hstage;  // Hessian: per-plane sums, per-vertex terms, per-lane staging
   unsigned o_plane, o_cx, o_cy, o_cz, o_cw, o_d2, o_tri, o_next, o_emask, o_rem, o_hole, o_edge;
   unsigned o_bcx, o_bcy, o_bcz, o_bcw, o_bd2, o_btri, o_tlist, o_pts, o_fstart, o_fv, o_pnb;
   unsigned total;
@@ -63,8 +65,9 @@ __host__ __device__ inline int pow2_at_least(int x) {
   return g;
 }
 
-__host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
+__host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid, int hc = 0) {
   Layout L;
+  L.HC = hc;
   L.Pc = (P + 3) & ~3;
   L.Vc = (V + 31) & ~31;
   L.G = grid ? pow2_at_least(2 * T) : 0;
@@ -98,6 +101,16 @@ __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid) {
   } else {
     L.o_bcx = L.o_bcy = L.o_bcz = L.o_bcw = L.o_bd2 = L.o_btri = L.o_tlist = L.o_pts = L.o_fstart = L.o_fv = 0;
     L.o_pnb = 0;
+    if (hc > 0) {
+      L.o_pnb = o;
+      o = align16(o + 4u * L.Pc);
+    }
+  }
+  L.o_harea = L.o_hbuf = L.o_hstage = 0;
+  if (hc > 0) {
+    L.o_harea = o; o = align16(o + 8u * hc * (L.Pc + 4));
+    L.o_hbuf = o; o = align16(o + 8u * hc * 3 * L.Vc);
+    L.o_hstage = o; o = align16(o + (8u * hc + 4u) * 32);
   }
   L.total = o;
   return L;
@@ -118,7 +131,12 @@ struct WarpCell {
   double *pts;  // start corner and the current boundary triangle, local frame
   int *fstart;         // per plane: first entry of its face in fv (np + 1 entries)
   unsigned char *fv;   // vertex ids of every face, in cyclic order
-  int *pnb;            // per plane: its neighbour seed (stored id), -1 for box planes (used cells only)
+  int *pnb;            // per plane: its neighbour seed (stored id), -1 for box planes (used cells, Hessian)
+  // Hessian (null when off): per plane the facet sums (area, or moments and
+  // area), per vertex slot the terms of one integration, per lane a staged piece
+  double *harea, *hbuf, *hstage;
+  int *hstage_f;
+  int hc;
   int nv, np;  // vertex and plane counts (warp-uniform)
   int vc, mw;  // capacity of the vertex arrays, words per edge mask
 };
@@ -148,6 +166,11 @@ __device__ __forceinline__ WarpCell bind(unsigned char *base, const Layout &L) {
   w.fstart = reinterpret_cast<int *>(base + L.o_fstart);
   w.fv = base + L.o_fv;
   w.pnb = reinterpret_cast<int *>(base + L.o_pnb);
+  w.hc = L.HC;
+  w.harea = L.HC ? reinterpret_cast<double *>(base + L.o_harea) : nullptr;
+  w.hbuf = L.HC ? reinterpret_cast<double *>(base + L.o_hbuf) : nullptr;
+  w.hstage = L.HC ? reinterpret_cast<double *>(base + L.o_hstage) : nullptr;
+  w.hstage_f = L.HC ? reinterpret_cast<int *>(base + L.o_hstage + 8u * L.HC * 32) : nullptr;
   w.nv = w.np = 0;
   w.vc = L.Vc;
   w.mw = L.Mw;
@@ -518,12 +541,79 @@ __device__ int clip(WarpCell &w, const Plane &e, int V, int &status, int lane, u
   return 1;
 }
 
+// Facet integrals of one integration (CCExportBaryVolumeAndArea,
+// ConvexCell.cl:621-678) into w.harea: per vertex A and each pair (plane
+// p, edge line l) of the volume decomposition, the triangle (A, the seed's
+// foot on p, the seed's foot on l) in plane p, signed by p's normal, times
+// factor; with 4 components also its area times its centroid (local frame).
+// Each vertex slot's terms go to w.hbuf first, then one lane per plane adds
+// them in vertex order: the sums do not depend on the warp schedule.
+__device__ __noinline__ void hess_integrate(const WarpCell &w, double factor, int lane) {
+  const int hc = w.hc;
+  for (int v = lane; v < w.nv; v += 32) {
+    const double inv = 1.0 / w.cw[v];
+    const double Ax = w.cx[v] * inv, Ay = w.cy[v] * inv, Az = w.cz[v] * inv;
+    const unsigned t = w.tri[v];
+    double term[3][4] = {};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const Plane &pi = w.plane[(t >> (8 * i)) & 0xff];
+      const Plane &pj = w.plane[(t >> (8 * ((i + 1) % 3))) & 0xff];
+      const double cxv = pi.y * pj.z - pi.z * pj.y;
+      const double cyv = pi.z * pj.x - pi.x * pj.z;
+      const double czv = pi.x * pj.y - pi.y * pj.x;
+      const double c2 = cxv * cxv + cyv * cyv + czv * czv;
+      double Lx = 0, Ly = 0, Lz = 0;
+      if (c2 >= kVolEps2) {
+        const double k = -(Ax * cxv + Ay * cyv + Az * czv) / c2;
+        Lx = k * cxv;
+        Ly = k * cyv;
+        Lz = k * czv;
+      }
+      // line i pairs with plane i (sign -) and plane i+1 (sign +)
+#pragma unroll
+      for (int st = 0; st < 2; ++st) {
+        const Plane &pp = st ? pj : pi;
+        const double k = -(Ax * pp.x + Ay * pp.y + Az * pp.z);
+        const double Px = -Ax - k * pp.x, Py = -Ay - k * pp.y, Pz = -Az - k * pp.z;
+        // det(P, L, n) / 2 with the foot vectors taken from A
+        const double det = Px * (Ly * pp.z - Lz * pp.y) - Py * (Lx * pp.z - Lz * pp.x) + Pz * (Lx * pp.y - Ly * pp.x);
+        const double ar = (st ? 0.5 : -0.5) * det;
+        const int slot = st ? (i + 1) % 3 : i;
+        if (hc == 1) {
+          term[slot][0] += ar;
+        } else {
+          term[slot][0] += ar * (Ax + (Px + Lx) * (1.0 / 3.0));
+          term[slot][1] += ar * (Ay + (Py + Ly) * (1.0 / 3.0));
+          term[slot][2] += ar * (Az + (Pz + Lz) * (1.0 / 3.0));
+          term[slot][3] += ar;
+        }
+      }
+    }
+    for (int i = 0; i < 3; ++i)
+      for (int c = 0; c < hc; ++c) w.hbuf[(3 * v + i) * hc + c] = term[i][c];
+  }
+  __syncwarp();
+  for (int p = lane; p < w.np; p += 32) {
+    double sum[4] = {0, 0, 0, 0};
+    for (int v = 0; v < w.nv; ++v) {
+      const unsigned t = w.tri[v];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        if (int((t >> (8 * i)) & 0xff) == p)
+          for (int c = 0; c < hc; ++c) sum[c] += w.hbuf[(3 * v + i) * hc + c];
+    }
+    for (int c = 0; c < hc; ++c) w.harea[p * hc + c] += factor * sum[c];
+  }
+  __syncwarp();
+}
+
 // Signed-tet integration of the cell (ConvexCell.cl:577-619) in the local
 // frame: per vertex A and each of its planes i, the two tets (A, C, C
 // projected on plane i, C projected on the edge line of planes i, j), C the
 // seed at the origin.  Unit normals make the plane projection division-free.
 // Accumulates (sum w*centroid, sum w)/6 * factor into acc (warp-uniform).
-template <int VS>
+template <int VS, bool HESS = false>
 __device__ void integrate(const WarpCell &w, double factor, double acc[4], int lane, unsigned long long *ctr,
                           double *tr, int trcap) {
   double sx = 0, sy = 0, sz = 0, sw = 0;
@@ -580,6 +670,9 @@ __device__ void integrate(const WarpCell &w, double factor, double acc[4], int l
   acc[1] += f * sy;
   acc[2] += f * sz;
   acc[3] += f * sw;
+  if constexpr (HESS) {
+    if (w.harea) hess_integrate(w, factor, lane);
+  }
   count(ctr, kCtrExports, 1, lane);
   count(ctr, kCtrExportVertices, w.nv, lane);
 }
@@ -793,7 +886,8 @@ __device__ double plain_radius2(const DevGrid &g, float4 s, int lane) {
 // the status; on failure fail_at is the failing triangle's position.
 // With the apex inside the cell (inner), a cone rarely misses the cell: the
 // quick classification is skipped and the triangle's plane clips first.
-template <int VS>
+// HESS: the Hessian facet sums as well (when w.harea is set).
+template <int VS, bool HESS = false>
 __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const int *tids, int t0, int t1,
                               int bk_nv, int bk_np, bool inner, double acc[4], int &fail_at, int lane,
                               unsigned long long *ctr, double *tr, int trcap) {
@@ -870,7 +964,7 @@ __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const 
         return cstat;
       }
     }
-    integrate<VS>(w, go_out ? 1.0 : -1.0, acc, lane, ctr, tr, trcap);
+    integrate<VS, HESS>(w, go_out ? 1.0 : -1.0, acc, lane, ctr, tr, trcap);
     if (any_cut) restore<VS>(w, bk_nv, bk_np, lane);
   }
   return kSuccess;
@@ -1209,9 +1303,11 @@ __device__ __forceinline__ void clip_line(const double *n, const double x0[3], c
 
 // Face f's facet: its edges inside the cone, and the cone planes' lines
 // inside the face (bounded by the face's edge planes and the other cone
-// planes).
-__device__ void face_facet(ConePiece &q, const WarpCell &w, const double *px, const double *py, const double *pz,
-                           int f) {
+// planes), as boundary segments (U, V) of the facet; emit(c, U, V) for each,
+// c the face's first vertex.
+template <class Emit>
+__device__ __forceinline__ void face_segments(const ConePiece &q, const WarpCell &w, const double *px,
+                                              const double *py, const double *pz, int f, Emit emit) {
   const int f0 = w.fstart[f], k = w.fstart[f + 1] - f0;
   const int v0 = w.fv[f0];
   const double c[3] = {px[v0], py[v0], pz[v0]};
@@ -1224,7 +1320,7 @@ __device__ void face_facet(ConePiece &q, const WarpCell &w, const double *px, co
     if (lo < hi) {
       const double U[3] = {fma(lo, v[0] - u[0], u[0]), fma(lo, v[1] - u[1], u[1]), fma(lo, v[2] - u[2], u[2])};
       const double V[3] = {fma(hi, v[0] - u[0], u[0]), fma(hi, v[1] - u[1], u[1]), fma(hi, v[2] - u[2], u[2])};
-      edge_tet(q, c, U, V);
+      emit(c, U, V);
     }
   }
   const Plane pf = w.plane[f];
@@ -1249,9 +1345,60 @@ __device__ void face_facet(ConePiece &q, const WarpCell &w, const double *px, co
     if (lo < hi) {
       const double U[3] = {fma(lo, d[0], x0[0]), fma(lo, d[1], x0[1]), fma(lo, d[2], x0[2])};
       const double V[3] = {fma(hi, d[0], x0[0]), fma(hi, d[1], x0[1]), fma(hi, d[2], x0[2])};
-      edge_tet(q, c, U, V);
+      emit(c, U, V);
     }
   }
+}
+
+__device__ void face_facet(ConePiece &q, const WarpCell &w, const double *px, const double *py, const double *pz,
+                           int f) {
+  face_segments(q, w, px, py, pz, f,
+                [&](const double *c, const double *U, const double *V) { edge_tet(q, c, U, V); });
+}
+
+// The facet of face f inside the cone as Hessian terms: its area (the
+// boundary segments fanned from c, against the face's outward normal -n),
+// and with 4 components its area times its centroid (local frame).
+__device__ __noinline__ void face_piece(const ConePiece &q, const WarpCell &w, const double *px, const double *py,
+                                        const double *pz, int f, double out[4]) {
+  const Plane pf = w.plane[f];
+  double a = 0, mx = 0, my = 0, mz = 0;
+  face_segments(q, w, px, py, pz, f, [&](const double *c, const double *U, const double *V) {
+    const double ux = U[0] - c[0], uy = U[1] - c[1], uz = U[2] - c[2];
+    const double vx = V[0] - c[0], vy = V[1] - c[1], vz = V[2] - c[2];
+    const double t = -0.5 * ((uy * vz - uz * vy) * pf.x + (uz * vx - ux * vz) * pf.y + (ux * vy - uy * vx) * pf.z);
+    a += t;
+    mx += t * (c[0] + U[0] + V[0]) * (1.0 / 3.0);
+    my += t * (c[1] + U[1] + V[1]) * (1.0 / 3.0);
+    mz += t * (c[2] + U[2] + V[2]) * (1.0 / 3.0);
+  });
+  if (w.hc == 1) {
+    out[0] = a;
+  } else {
+    out[0] = mx;
+    out[1] = my;
+    out[2] = mz;
+    out[3] = a;
+  }
+}
+
+// One round of facet pieces (lane: face f >= 0 or none) into w.harea,
+// signed: each lane stages its piece, then lane c adds component c of
+// every staged piece in lane order.
+__device__ __noinline__ void hess_pieces(const ConePiece &q, const WarpCell &w, const double *px, const double *py,
+                                         const double *pz, int f, double sgn, int lane) {
+  const int hc = w.hc;
+  double out[4] = {0, 0, 0, 0};
+  if (f >= 0) face_piece(q, w, px, py, pz, f, out);
+  for (int c = 0; c < hc; ++c) w.hstage[lane * hc + c] = sgn * out[c];
+  w.hstage_f[lane] = f;
+  __syncwarp();
+  if (lane < hc)
+    for (int l = 0; l < 32; ++l) {
+      const int g = w.hstage_f[l];
+      if (g >= 0) w.harea[g * hc + lane] += w.hstage[l * hc + lane];
+    }
+  __syncwarp();
 }
 
 // Sets up the cone of triangle tri from apex a; false for a flat cone.
@@ -1308,6 +1455,7 @@ __device__ bool cone_setup(ConePiece &q, const DevGrid &g, float4 s, int tri, co
 
 // Cone pieces of triangles tids[t0, t1) (at most 32), one per lane, summed
 // over the warp into acc.  Needs build_faces.
+template <bool HESS = false>
 __device__ void facet_triangles(const WarpCell &w, const double *px, const double *py, const double *pz,
                                 const DevGrid &g, float4 s, const int *tids, int t0, int t1, const double a[3],
                                 double acc[4], int lane, unsigned long long *ctr) {
@@ -1449,10 +1597,14 @@ __device__ void facet_triangles(const WarpCell &w, const double *px, const doubl
       }
     }
     while (__any_sync(kFull, hit != 0)) {
+      int f = -1;
       if (hit) {
-        const int f = fb + __ffsll(hit) - 1;
+        f = fb + __ffsll(hit) - 1;
         hit &= hit - 1;
         face_facet(q, w, px, py, pz, f);
+      }
+      if constexpr (HESS) {
+        if (w.harea) hess_pieces(q, w, px, py, pz, f, sgn, lane);
       }
     }
   }
@@ -1651,7 +1803,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     }
   }
   trace_rec(tr, trcap, lane, 5, pt0[0], pt0[1], pt0[2], in_domain, nuniq);
-  if (in_domain == 2) integrate<VS>(w, 1.0, acc, lane, ctr, tr, trcap);
+  if (in_domain == 2) integrate<VS, INL>(w, 1.0, acc, lane, ctr, tr, trcap);
   if (nuniq == 0) return kSuccess;
   if (lane < 3) w.pts[lane] = pt0[lane];
   __syncwarp();
@@ -1672,7 +1824,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     if (inner) {
       build_faces(w, w.bcx, w.bcy, w.bcz, pt0, lane);
       for (int b0 = 0; b0 < nuniq; b0 += 32)
-        facet_triangles(w, w.bcx, w.bcy, w.bcz, g, s, w.tlist, b0, min(nuniq, b0 + 32), pt0, acc, lane, ctr);
+        facet_triangles<INL>(w, w.bcx, w.bcy, w.bcz, g, s, w.tlist, b0, min(nuniq, b0 + 32), pt0, acc, lane, ctr);
       return kSuccess;
     }
     const int bk_nv = w.nv, bk_np = w.np;
@@ -1683,7 +1835,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     for (int c0 = 0; c0 < nuniq; c0 += 32) {
       double part[4] = {0, 0, 0, 0};
       int fail_at = 0;
-      const int st = cone_triangles<VS>(w, a, s, w.tlist, c0, min(nuniq, c0 + 32), bk_nv, bk_np, inner, part,
+      const int st = cone_triangles<VS, INL>(w, a, s, w.tlist, c0, min(nuniq, c0 + 32), bk_nv, bk_np, inner, part,
                                         fail_at, lane, ctr, tr, trcap);
       if (st != kSuccess) return st;
       for (int d = 0; d < 4; ++d) acc[d] += part[d];
@@ -1726,6 +1878,10 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
   unsigned long long *ctr = a.counters;
   const int sid = a.ids ? a.ids[row] : row;
   if (only_status >= 0 && a.status[sid] != only_status) return;
+  // Hessian rows run inline only (no defer queue)
+  if constexpr (INL) {
+    if (a.hess && lane == 0) a.hessid[size_t(sid) * a.H] = -1;  // an empty row until the cell succeeds
+  }
   const float4 s = a.stored[sid];
   double *tr = (a.trace && sid == a.trace_seed) ? a.trace : nullptr;
   const int trcap = a.trace_cap;
@@ -1740,8 +1896,16 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
     return;
   }
   init_box(w, s, a.cube_eps, lane);
+  if constexpr (INL) {
+    if (w.harea) {
+      for (int i = lane; i < w.hc * (L.Pc + 4); i += 32) w.harea[i] = 0.0;
+      __syncwarp();
+    }
+  }
   double R2 = cell_radius2<VS>(w, lane);
-  const bool track_nb = GRID && a.used != nullptr;  // plane neighbours for the used cells
+  // plane neighbours for the used cells and the Hessian
+  const bool used_on = GRID && a.used != nullptr;
+  const bool track_nb = used_on || (INL && a.hess != nullptr);
   if (track_nb && lane < 6) w.pnb[lane] = -1;
 
   // ---- power clipping by the K nearest, in order ----
@@ -1806,6 +1970,7 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
     }
   }
   if (status == kSuccess && !reached && !exhausted && !outside) status = kSecurityRadiusNotReached;
+  const int np_cell = w.np;  // the clipped cell's planes (cone planes come after)
   if (a.border_d > 0) {
     // bordering pass (ConvexCell.cl:756-809): the clipped cell marks its
     // neighbours; statuses and moments stay those of the main passes
@@ -1818,23 +1983,55 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
     if (GRID)
       status = restrict_to_domain<VS, INL>(w, a, L, s, sid, acc, lane, ctr, tr, trcap);
     else
-      integrate<VS>(w, 1.0, acc, lane, ctr, tr, trcap);
+      integrate<VS, INL>(w, 1.0, acc, lane, ctr, tr, trcap);
   }
   if (status == kDeferred) return;  // k_cone_finish writes it
   if (status == kParkOverflow) {
     if (lane == 0) a.status[sid] = kParkOverflow;
     return;
   }
+  if (INL && a.hess && status == kSuccess) {
+    // the row (ConvexCell.cl:1133-1150): facets with a neighbour and an area
+    // above 0.2, in plane order; more than H is hessian_overflow, which
+    // keeps the moments
+    __syncwarp();
+    if (lane == 0) {
+      const int hc = a.HC, H = a.H;
+      double *hrow = a.hess + size_t(sid) * H * hc;
+      int *hids = a.hessid + size_t(sid) * H;
+      int cnt = 0;
+      for (int p = 0; p < np_cell; ++p) {
+        const double ar = w.harea[p * hc + hc - 1];
+        if (w.pnb[p] < 0 || ar <= 0.2) continue;
+        if (cnt >= H) {
+          status = kHessianOverflow;
+          break;
+        }
+        if (hc == 1) {
+          hrow[cnt] = ar;
+        } else {
+          hrow[4 * cnt + 0] = w.harea[4 * p + 0] + ar * double(s.x);
+          hrow[4 * cnt + 1] = w.harea[4 * p + 1] + ar * double(s.y);
+          hrow[4 * cnt + 2] = w.harea[4 * p + 2] + ar * double(s.z);
+          hrow[4 * cnt + 3] = ar;
+        }
+        hids[cnt] = w.pnb[p];
+        ++cnt;
+      }
+      if (status == kSuccess && cnt < H) hids[cnt] = -1;
+    }
+    status = __shfl_sync(kFull, status, 0);
+  }
   if (lane == 0) {
     a.status[sid] = status;
     // local moments -> global: sum w*(x_local + s) = m_local + m * s
     const double m = acc[3];
-    if (status == kSuccess)
+    if (status == kSuccess || status == kHessianOverflow)
       a.out[sid] = make_double4(acc[0] + m * double(s.x), acc[1] + m * double(s.y), acc[2] + m * double(s.z), m);
     else
       a.out[sid] = make_double4(0.0, 0.0, 0.0, 0.0);
   }
-  if (track_nb && status == kSuccess && acc[3] >= a.keep_volume) {
+  if (used_on && status == kSuccess && acc[3] >= a.keep_volume) {
     // a used cell (ConvexCell.cl:1118-1126)
     if (lane == 0) *(volatile unsigned char *)&a.used[sid] = 1;
     __syncwarp();
@@ -2183,7 +2380,8 @@ size_t defer_slot_bytes(int P, int V, int T) { return slot_bytes_for(make_layout
 cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count, int *launches) {
   if (a.num <= 0) return cudaSuccess;
   if (a.P > kMaxP || a.V > kMaxV || a.T > kMaxT || a.P < 7 || a.V < 8) return cudaErrorInvalidValue;
-  const Layout L = make_layout(a.P, a.V, a.T, a.grid.size > 0);
+  if (a.hess && (a.defer.slots || a.H < 1 || (a.HC != 1 && a.HC != 4))) return cudaErrorInvalidValue;
+  const Layout L = make_layout(a.P, a.V, a.T, a.grid.size > 0, a.hess ? a.HC : 0);
   if (a.defer.slots && a.defer.slot_bytes < slot_bytes_for(L, a.T)) return cudaErrorInvalidValue;
   const int vs = L.Vc / 32;
   if (vs <= 2) return launch_vs<2>(a, L, st, sm_count, launches);

@@ -85,6 +85,11 @@ struct CellLaunch {
   int mark_dist = 0;
   int border_d = 0;
   int diag = 0;  // index of this diagram in a batched launch (parked cells record it)
+  // --hessian (no defer queue): per cell a row of H facets, HC values each,
+  // and their neighbours (stored ids, -1 after the last), stored order
+  double *hess = nullptr;
+  int *hessid = nullptr;
+  int H = 0, HC = 1;
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
 constexpr int kTraceRecord = 12;

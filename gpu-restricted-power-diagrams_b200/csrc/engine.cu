@@ -133,6 +133,54 @@ __global__ void k_status_hist(const int *__restrict__ status, int n, int *__rest
   if (threadIdx.x < kStatusNum && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
+// Hessian rows in user order: values copied up to a row's terminator, the
+// neighbours as user ids; the rest of a row is zeros and -1.
+__global__ void k_hessian_user(const double *__restrict__ hess, const int *__restrict__ hessid,
+                               const int *__restrict__ user_to_stored, const int *__restrict__ perm, int n, int H,
+                               int HC, double *__restrict__ vals, int *__restrict__ ids) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const size_t sid = size_t(user_to_stored[u]);
+  bool live = true;
+  for (int k = 0; k < H; ++k) {
+    const int v = live ? hessid[sid * H + k] : -1;
+    live = v >= 0;
+    ids[size_t(u) * H + k] = live ? perm[v] : -1;
+    for (int c = 0; c < HC; ++c)
+      vals[(size_t(u) * H + k) * HC + c] = live ? hess[(sid * H + k) * HC + c] : 0.0;
+  }
+}
+
+// Hessian rows of the used cells (compact_result, voronoi.cpp:594-629): the
+// row of used user u goes to its compacted position pos[u]; a cell lighter
+// than eps has an empty row; a neighbour is kept when it is used and not
+// lighter than eps, as its compacted position.
+__global__ void k_hessian_used(const int *__restrict__ f, const int *__restrict__ pos, int n,
+                               const int *__restrict__ user_to_stored, const int *__restrict__ perm,
+                               const double4 *__restrict__ out, double eps, const double *__restrict__ hess,
+                               const int *__restrict__ hessid, int H, int HC, double *__restrict__ vals,
+                               int *__restrict__ ids) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n || !f[u]) return;
+  const size_t sid = size_t(user_to_stored[u]), row = size_t(pos[u]);
+  int w = 0;
+  if (out[sid].w >= eps) {
+    for (int k = 0; k < H; ++k) {
+      const int v = hessid[sid * H + k];
+      if (v < 0) break;
+      const int uv = perm[v];
+      if (!f[uv] || out[v].w < eps) continue;
+      ids[row * H + w] = pos[uv];
+      for (int c = 0; c < HC; ++c) vals[(row * H + w) * HC + c] = hess[(sid * H + k) * HC + c];
+      ++w;
+    }
+  }
+  for (int k = w; k < H; ++k) {
+    ids[row * H + k] = -1;
+    for (int c = 0; c < HC; ++c) vals[(row * H + k) * HC + c] = 0.0;
+  }
+}
+
 // Stored ids of the bordering cells of distance d: marked d-1, not used
 // themselves (find_bordering, voronoi.cpp:711-719), ascending.
 __global__ void k_border_flags(const unsigned char *__restrict__ used, const double4 *__restrict__ out, int n, int d,
@@ -310,7 +358,14 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.out = s->out.as<double4>();
   a.counters = ctr;
   a.after_cell = ev[3];
-  if (s->grid.size > 0 && s->use_defer && border_d == 0) {
+  if (s->hess_h > 0 && border_d == 0) {
+    a.hess = s->hess.as<double>();
+    a.hessid = s->hessid.as<int>();
+    a.H = s->hess_h;
+    a.HC = s->hess_hc;
+  }
+  // Hessian rows are summed in the cell's own warp (no defer queue)
+  if (s->grid.size > 0 && s->use_defer && border_d == 0 && s->hess_h == 0) {
     // boundary cells with many triangles are parked and their triangles
     // spread over all warps; cells past the capacity stay inline
     DeferQueue &dq = a.defer;
@@ -577,6 +632,8 @@ void rpd_params_default(rpd_params *p) {
   p->flags = 0;
   p->keep_distance = -1;
   p->keep_volume = 0.001;
+  p->hessian_h = 0;
+  p->hessian_hc = 1;
 }
 
 int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
@@ -689,6 +746,19 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   s->fresh_knn = (p.flags & RPD_FLAG_FRESH_NEIGHBOURS) != 0;
   // used cells only with a domain (voronoi.cpp:1291)
   s->used_on = grid && p.keep_distance >= 0;
+  if (p.hessian_h < 0 || (p.hessian_h > 0 && p.hessian_hc != 1 && p.hessian_hc != 4)) {
+    set_error(ctx, "hessian_h must be >= 0 and hessian_hc 1 or 4");
+    return RPD_ERR_INVALID;
+  }
+  s->hess_h = 0;
+  if (p.hessian_h > 0) {
+    if ((e = s->hess.ensure(sizeof(double) * size_t(n) * p.hessian_h * p.hessian_hc)) != cudaSuccess)
+      return map_cuda(ctx, e, "alloc hessian");
+    if ((e = s->hessid.ensure(sizeof(int) * size_t(n) * p.hessian_h)) != cudaSuccess)
+      return map_cuda(ctx, e, "alloc hessian");
+    s->hess_h = p.hessian_h;
+    s->hess_hc = p.hessian_hc;
+  }
   s->keep_distance = p.keep_distance;
   s->keep_volume = p.keep_volume;
   s->used_count = -1;
@@ -840,6 +910,43 @@ int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *pp, doub
   const int nrec = int(count);
   cudaMemcpy(records, tr.as<double>() + 1, sizeof(double) * size_t(nrec) * kTraceRecord, cudaMemcpyDeviceToHost);
   return nrec;
+}
+
+int rpd_solver_get_hessian(rpd_solver *s, double *values, int *ids, rpd_mem where) {
+  if (!s || !values || !ids || !s->have_results || s->hess_h <= 0) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const int n = s->n, H = s->hess_h, HC = s->hess_hc;
+  // with used cells, the rows of the used cells only (compacted)
+  int *f = nullptr, *pos = nullptr, rows = n, rc;
+  if (s->used_count >= 0 && (rc = used_positions(s, &f, &pos, rows)) != RPD_OK) return rc;
+  const size_t nv = size_t(rows) * H * HC, ni = size_t(rows) * H;
+  double *dv = values;
+  int *di = ids;
+  if (where == RPD_HOST) {
+    if ((e = s->gather.ensure(sizeof(double) * nv + sizeof(int) * ni + 16)) != cudaSuccess)
+      return map_cuda(ctx, e, "alloc gather");
+    dv = s->gather.as<double>();
+    di = reinterpret_cast<int *>(dv + nv);
+  }
+  const int tb = 256;
+  if (f)
+    k_hessian_used<<<(n + tb - 1) / tb, tb, 0, st>>>(f, pos, n, s->user_to_stored.as<int>(), s->perm.as<int>(),
+                                                     s->out.as<double4>(), s->keep_volume, s->hess.as<double>(),
+                                                     s->hessid.as<int>(), H, HC, dv, di);
+  else
+    k_hessian_user<<<(n + tb - 1) / tb, tb, 0, st>>>(s->hess.as<double>(), s->hessid.as<int>(),
+                                                     s->user_to_stored.as<int>(), s->perm.as<int>(), n, H, HC, dv, di);
+  if (where == RPD_HOST) {
+    if ((e = cudaMemcpyAsync(values, dv, sizeof(double) * nv, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return map_cuda(ctx, e, "copy hessian");
+    if ((e = cudaMemcpyAsync(ids, di, sizeof(int) * ni, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return map_cuda(ctx, e, "copy hessian");
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "hessian");
+  return RPD_OK;
 }
 
 int rpd_solver_get_stats(const rpd_solver *s, rpd_stats *st) {

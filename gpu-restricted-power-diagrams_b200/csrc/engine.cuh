@@ -98,6 +98,10 @@ struct rpd_solver {
   int keep_distance = -1;
   double keep_volume = 0.0;
   int used_count = -1;         // of the last launch, -1: none
+  // --hessian rows (stored order) of the last launch with hessian_h > 0
+  rpd::DevBuf hess;            // double[n*H*HC]
+  rpd::DevBuf hessid;          // int[n*H]: stored ids, -1 after a row's last facet
+  int hess_h = 0, hess_hc = 1; // of the last launch (0: no rows)
   rpd_stats stats{};
 };
 

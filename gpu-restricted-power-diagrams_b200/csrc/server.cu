@@ -334,6 +334,7 @@ int rpd_server_submit_solve(rpd_server *sv, const float *xyzw, int n, const rpd_
   r->grid = grid;
   if (p) r->params = *p;
   else rpd_params_default(&r->params);
+  if (r->params.hessian_h != 0) return RPD_ERR_INVALID;  // requests return moments only
   r->moments = moments;
   r->need = transient_bytes(n, r->params);
   r->new_resident = resident_bytes(n, r->params);
@@ -360,6 +361,7 @@ int rpd_server_submit_reweight(rpd_server *sv, int session, const float *w, cons
   r->session = session;
   if (p) r->params = *p;
   else rpd_params_default(&r->params);
+  if (r->params.hessian_h != 0) return RPD_ERR_INVALID;  // requests return moments only
   r->moments = moments;
   std::lock_guard<std::mutex> lock(sv->mu);
   if (sv->stop) return RPD_ERR_INVALID;

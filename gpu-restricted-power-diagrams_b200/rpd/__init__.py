@@ -100,6 +100,7 @@ def lib():
         L.rpd_solver_get_status.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_get_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.rpd_solver_trace_cell.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.rpd_solver_get_hessian.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_batch_create.restype = C.c_void_p
         L.rpd_batch_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.rpd_batch_launch.argtypes = [C.c_void_p]
@@ -128,7 +129,8 @@ class Params(C.Structure):
 
     _fields_ = [("K", C.c_int), ("P", C.c_int), ("V", C.c_int), ("T", C.c_int), ("max_extra_passes", C.c_int),
                 ("cube_eps", C.c_float), ("out_domain", C.c_int), ("flags", C.c_uint),
-                ("keep_distance", C.c_int), ("keep_volume", C.c_double)]
+                ("keep_distance", C.c_int), ("keep_volume", C.c_double), ("hessian_h", C.c_int),
+                ("hessian_hc", C.c_int)]
 
     @classmethod
     def default(cls, **kw):
@@ -285,6 +287,19 @@ class Solver:
         st = Stats()
         self.ctx.check(lib().rpd_solver_get_stats(self.h, C.byref(st)))
         return st.as_dict()
+
+    def hessian(self, H: int, HC: int = 1):
+        """Hessian rows of the last launch with hessian_h=H, hessian_hc=HC:
+        (values (n,H) areas for HC=1 or (n,H,4) area-weighted centroids and
+        areas, ids (n,H) neighbour user ids, -1 after a row's last facet).
+        With used cells: the used cells' rows, ids their compacted positions."""
+        m = lib().rpd_solver_used_count(self.h)
+        rows = m if m >= 0 else self.n
+        vals = np.zeros((max(rows, 1), H, HC), np.float64)
+        ids = np.zeros((max(rows, 1), H), np.int32)
+        self.ctx.check(lib().rpd_solver_get_hessian(self.h, _ptr(vals), _ptr(ids), RPD_HOST))
+        vals, ids = vals[:rows], ids[:rows]
+        return (vals[:, :, 0] if HC == 1 else vals), ids
 
     TRACE_KINDS = {0: "seed", 1: "plane", 2: "cavity", 3: "vertex", 4: "integrate", 5: "start", 6: "triangle"}
 

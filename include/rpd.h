@@ -175,6 +175,9 @@ typedef struct rpd_params {
                            d >= 1 also the cells up to d face rings around them */
   double keep_volume;   /* --keepVolume: the mass that makes a cell used (default 0.001,
                            the FP64 build's, Options.cpp:40) */
+  int hessian_h;        /* --hessian with --H: facets per Hessian row, 0 off (the default;
+                           Options.cpp:22,269) */
+  int hessian_hc;       /* --HC: 1 (facet area) or 4 (area-weighted facet centroid and area) */
 } rpd_params;
 
 void rpd_params_default(rpd_params *p);
@@ -284,6 +287,24 @@ int rpd_server_wait(rpd_server *sv, int ticket, rpd_request_info *info);
 int rpd_server_release(rpd_server *sv, int session);
 /* Device bytes held by resident sessions, grids and admitted requests. */
 size_t rpd_server_bytes_in_use(rpd_server *sv);
+
+/* --hessian output of the last launch with hessian_h > 0 (VoroAlgo::
+ * getHessians / getHessianIds, voronoi.h:161-180; CCExportBaryVolumeAndArea,
+ * ConvexCell.cl:621-678): per seed (user order) a row of hessian_h facets of
+ * its restricted cell -- one per neighbour whose shared facet inside the
+ * domain has an area above 0.2 (squared reference-frame units), in the order
+ * the neighbours' planes entered the cell -- with hessian_hc values each
+ * (the area; or the area-weighted centroid x, y, z and the area, reference
+ * frame).  values: n*hessian_h*hessian_hc doubles; ids: n*hessian_h ints,
+ * the neighbours' user ids, -1 after a row's last facet (rows of cells that
+ * did not succeed are empty).  A cell with more facets than hessian_h gets
+ * the status RPD_HESSIAN_OVERFLOW and its first hessian_h facets.  With used
+ * cells (keep_distance >= 0 and a domain) the rows are those of the used
+ * cells, in the order of rpd_solver_get_used, and a facet's id is its
+ * neighbour's position in that order (compact_result, voronoi.cpp:594-629):
+ * rows of cells lighter than keep_volume are empty, and neighbours that are
+ * not used or lighter than keep_volume are left out. */
+int rpd_solver_get_hessian(rpd_solver *s, double *values, int *ids, rpd_mem where);
 
 /* -------------------------------------------------------- batched solves */
 

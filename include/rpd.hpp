@@ -155,6 +155,8 @@ class VoroAlgo {
     p.T = m_T;
     p.keep_distance = m_keepDistance;
     p.keep_volume = m_keepVolume;
+    p.hessian_h = m_H;
+    p.hessian_hc = m_HC;
     if (rpd_solver_launch(s_, &p) != RPD_OK) {
       if (m_debug) fprintf(stderr, "VoroAlgo::launch: %s\n", ctx_->error().c_str());
       return false;
@@ -209,6 +211,25 @@ class VoroAlgo {
     }
     return r;
   }
+  // --hessian rows (m_H > 0): per output point m_H facets of m_HC values
+  // (the area, or the area-weighted centroid and the area), and their
+  // neighbours as output indices, -1 after a row's last facet.
+  std::vector<double> getHessians() const {
+    if (m_H <= 0) return {};
+    std::vector<double> v(size_t(getNumOutputPoints()) * m_H * m_HC + 1);
+    std::vector<int> ids(size_t(getNumOutputPoints()) * m_H + 1);
+    rpd_solver_get_hessian(s_, v.data(), ids.data(), RPD_HOST);
+    v.pop_back();
+    return v;
+  }
+  std::vector<int> getHessianIds() const {
+    if (m_H <= 0) return {};
+    std::vector<double> v(size_t(getNumOutputPoints()) * m_H * m_HC + 1);
+    std::vector<int> ids(size_t(getNumOutputPoints()) * m_H + 1);
+    rpd_solver_get_hessian(s_, v.data(), ids.data(), RPD_HOST);
+    ids.pop_back();
+    return ids;
+  }
   std::vector<int> getStatus() const {
     std::vector<int> r(getNumOutputPoints());
     rpd_solver_get_status(s_, r.data(), RPD_HOST);
@@ -223,6 +244,10 @@ class VoroAlgo {
   // else the kept ring distance; the mass that makes a cell used
   float m_keepVolume = 1;
   int m_keepDistance = 1;
+  // --hessian (voronoi.cpp:1048-1049 defaults): facets per row (0: off) and
+  // values per facet (1 or 4)
+  int m_H = 0;
+  int m_HC = 1;
 
  private:
   std::shared_ptr<Context> ctx_;
