@@ -361,11 +361,13 @@ def run_ours(args, cfg, rank, world, local):
         dist.destroy_process_group()
 
 
-def batch_specs(cfg, rank):
+def batch_specs(cfg, rank, count=None):
+    """The batch's diagrams; `count` < cfg["count"] keeps the first ones (the
+    same specs: the generator draws them in order)."""
     from rpd import synth
 
-    return synth.uneven_batch(cfg["count"], seed=cfg["sseed"] + 1000 * rank, nmin=cfg["nmin"], nmax=cfg["nmax"],
-                              gmin=cfg["gmin"], gmax=cfg["gmax"], ks=cfg["ks"])
+    return synth.uneven_batch(count or cfg["count"], seed=cfg["sseed"] + 1000 * rank, nmin=cfg["nmin"],
+                              nmax=cfg["nmax"], gmin=cfg["gmin"], gmax=cfg["gmax"], ks=cfg["ks"])
 
 
 def batch_grids(rpd, cfg, specs):
@@ -392,7 +394,7 @@ def run_batch(args, cfg, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     ctx = rpd.Context(local)
-    specs = batch_specs(cfg, rank)
+    specs = batch_specs(cfg, rank, args.diagrams)
     grids = batch_grids(rpd, cfg, specs)
     solvers = []
     for s, g in zip(specs, grids):
@@ -717,6 +719,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--diagrams", type=int, default=None,
+                    help="batch configs: solve only the first N diagrams (small cases for profiling)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     cfg = CONFIGS[args.config]
