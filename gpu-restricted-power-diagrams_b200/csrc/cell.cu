@@ -1704,6 +1704,22 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   const int S = g.size;
   const int ex = vmax[0] - vmin[0] + 1, ey = vmax[1] - vmin[1] + 1, ez = vmax[2] - vmin[2] + 1;
   const int nvox = (ex > 0 && ey > 0 && ez > 0) ? ex * ey * ez : 0;
+  if (g.tsat && nvox > 0) {
+    // disjoint lists: the range's triangle count from the summed counts
+    // (lane q < 8 reads corner q); more than T fails as the merge would,
+    // before any list is read
+    int part = 0;
+    if (lane < 8) {
+      const int S1 = S + 1;
+      const int x = (lane & 1) ? vmax[0] + 1 : vmin[0], y = (lane & 2) ? vmax[1] + 1 : vmin[1],
+                z = (lane & 4) ? vmax[2] + 1 : vmin[2];
+      const int sign = ((lane & 1) ^ ((lane >> 1) & 1) ^ ((lane >> 2) & 1)) ? 1 : -1;
+      part = sign * __ldg(&g.tsat[x + S1 * (y + S1 * z)]);  // + for an odd number of upper corners
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+    if (__shfl_sync(kFull, part, 0) > a.T) return kTriangleOverflow;
+  }
   // first corner with flag != 1 in (z, y, x) scan order, and the triangle ids
   // of every voxel in the range
   int in_domain = 1, c0 = -1;

@@ -20,6 +20,9 @@ struct DevGrid {
   // No triangle id appears in two voxel lists: the union of the lists of a
   // voxel range is their concatenation (no sort needed).
   int lists_disjoint = 0;
+  // With disjoint lists: summed triangle counts, (size+1)^3, so a voxel
+  // range's triangle count is 8 reads; null: unused.
+  const int *tsat = nullptr;
 };
 
 // Counters of one launch (optional): cells by outcome and work done.

@@ -672,6 +672,37 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
       }
   if ((e = s->g_sat.ensure(sizeof(int) * sat.size())) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
   cudaMemcpyAsync(s->g_sat.ptr, sat.data(), sizeof(int) * sat.size(), cudaMemcpyHostToDevice, st);
+  bool disjoint = true;
+  {
+    std::vector<unsigned char> seen(size_t(g->num_triangles()), 0);
+    for (int t : g->tri_list) {
+      if (seen[size_t(t)]) {
+        disjoint = false;
+        break;
+      }
+      seen[size_t(t)] = 1;
+    }
+  }
+  // with disjoint lists, the summed triangle counts: a cell whose voxel
+  // range holds more than T triangles fails without reading the lists (the
+  // union the reference merges has exactly that many ids)
+  std::vector<int> tsat;
+  if (disjoint) {
+    tsat.assign(size_t(S1) * S1 * S1, 0);
+    auto at = [&](int i, int j, int k) -> int & { return tsat[i + size_t(S1) * (j + size_t(S1) * k)]; };
+    for (int z = 0; z < S; ++z)
+      for (int y = 0; y < S; ++y)
+        for (int x = 0; x < S; ++x) {
+          const size_t v = x + size_t(S) * (y + size_t(S) * z);
+          const int f = g->offsets[v + 1] - g->offsets[v];
+          at(x + 1, y + 1, z + 1) = f + at(x, y + 1, z + 1) + at(x + 1, y, z + 1) + at(x + 1, y + 1, z) -
+                                    at(x, y, z + 1) - at(x, y + 1, z) - at(x + 1, y, z) + at(x, y, z);
+        }
+    if ((e = s->g_tsat.ensure(sizeof(int) * tsat.size())) != cudaSuccess) return map_cuda(ctx, e, "alloc grid");
+    cudaMemcpyAsync(s->g_tsat.ptr, tsat.data(), sizeof(int) * tsat.size(), cudaMemcpyHostToDevice, st);
+  } else {
+    s->g_tsat.release();
+  }
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "upload grid");
   DevGrid d;
   d.size = g->size;
@@ -682,17 +713,8 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
   d.list = s->g_list.as<const int>();
   d.offsets = s->g_offsets.as<const int>();
   d.sat = s->g_sat.as<const int>();
-  {
-    std::vector<unsigned char> seen(size_t(g->num_triangles()), 0);
-    d.lists_disjoint = 1;
-    for (int t : g->tri_list) {
-      if (seen[size_t(t)]) {
-        d.lists_disjoint = 0;
-        break;
-      }
-      seen[size_t(t)] = 1;
-    }
-  }
+  d.lists_disjoint = disjoint ? 1 : 0;
+  d.tsat = disjoint ? s->g_tsat.as<const int>() : nullptr;
   d.has_border_corners = 0;
   for (char c : g->in_domain)
     if (c == 1) {
@@ -1007,6 +1029,7 @@ void solver_share_grid(rpd_solver *dst, const rpd_solver *src) {
   dst->g_list.release();
   dst->g_offsets.release();
   dst->g_sat.release();
+  dst->g_tsat.release();
   dst->grid = src->grid;
 }
 
@@ -1032,7 +1055,7 @@ void solver_trim(rpd_solver *s) {
 size_t solver_device_bytes(const rpd_solver *s) {
   const DevBuf *b[] = {&s->user, &s->stored, &s->perm, &s->user_to_stored, &s->weights, &s->counters, &s->bin_ws,
                        &s->ring_bound, &s->knn, &s->knn_part, &s->knn_user, &s->counter64, &s->g_flags, &s->g_points,
-                       &s->g_tris, &s->g_list, &s->g_offsets, &s->g_sat, &s->out, &s->status, &s->ids_a, &s->ids_b,
+                       &s->g_tris, &s->g_list, &s->g_offsets, &s->g_sat, &s->g_tsat, &s->out, &s->status, &s->ids_a, &s->ids_b,
                        &s->ids_c, &s->fail_ws, &s->hist, &s->gather, &s->defer_slots, &s->defer_part, &s->defer_fail,
                        &s->defer_ctr};
   size_t t = 0;

@@ -78,7 +78,7 @@ struct rpd_solver {
   rpd::DevBuf knn_user;        // int[n*K]
   rpd::DevBuf counter64;       // unsigned long long[RPD_CTR_NUM + 1]
   // domain on the device
-  rpd::DevBuf g_flags, g_points, g_tris, g_list, g_offsets, g_sat;
+  rpd::DevBuf g_flags, g_points, g_tris, g_list, g_offsets, g_sat, g_tsat;
   rpd::DevGrid grid;           // grid.size == 0: no domain
   // results (stored order) and pass bookkeeping
   rpd::DevBuf out;             // double4[n]

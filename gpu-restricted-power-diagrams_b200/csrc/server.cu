@@ -72,8 +72,9 @@ size_t grid_bytes(const rpd_grid *g) {
   int size = 0, np = 0, nt = 0, nl = 0;
   if (!g || rpd_grid_info(g, &size, &np, &nt, &nl) != RPD_OK) return 0;
   const size_t S = size_t(size);
-  // flags, offsets, summed-volume table, points, triangles, lists
-  return S * S * S * (1 + 4) + (S + 1) * (S + 1) * (S + 1) * 4 + size_t(np) * 16 + size_t(nt) * 12 +
+  // flags, offsets, summed-volume and summed-triangle tables, points,
+  // triangles, lists
+  return S * S * S * (1 + 4) + (S + 1) * (S + 1) * (S + 1) * 8 + size_t(np) * 16 + size_t(nt) * 12 +
          size_t(nl) * 4 + 4096;
 }
 
