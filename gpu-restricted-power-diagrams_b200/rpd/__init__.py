@@ -101,6 +101,7 @@ def lib():
         L.rpd_solver_get_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.rpd_solver_trace_cell.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_get_hessian.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.rpd_compare_moments.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
         L.rpd_batch_create.restype = C.c_void_p
         L.rpd_batch_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.rpd_batch_launch.argtypes = [C.c_void_p]
@@ -328,6 +329,31 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+class MomentDiff(C.Structure):
+    _fields_ = [("cells", C.c_longlong), ("cells_both", C.c_longlong), ("sum_a", C.c_double * 4),
+                ("sum_b", C.c_double * 4), ("max_mass", C.c_double), ("max_bary", C.c_double * 3),
+                ("max_moment", C.c_double * 3), ("avg_mass", C.c_double), ("avg_bary", C.c_double * 3),
+                ("avg_moment", C.c_double * 3)]
+
+
+def compare_moments(a, b) -> dict:
+    """rpd_compare_moments: the reference diff tool's figures for two (n,4)
+    moment arrays (m*x, m*y, m*z, m)."""
+    a = np.ascontiguousarray(a, np.float64).reshape(-1, 4)
+    b = np.ascontiguousarray(b, np.float64).reshape(-1, 4)
+    if a.shape != b.shape:
+        raise ValueError("moment arrays differ in size")
+    d = MomentDiff()
+    rc = lib().rpd_compare_moments(_ptr(a), _ptr(b), len(a), C.byref(d))
+    if rc != RPD_OK:
+        raise RpdError(rc, "compare_moments")
+    out = {}
+    for k, _ in d._fields_:
+        v = getattr(d, k)
+        out[k] = list(v) if hasattr(v, "__len__") else v
+    return out
 
 
 class BatchStats(C.Structure):

@@ -306,6 +306,25 @@ size_t rpd_server_bytes_in_use(rpd_server *sv);
  * not used or lighter than keep_volume are left out. */
 int rpd_solver_get_hessian(rpd_solver *s, double *values, int *ids, rpd_mem where);
 
+/* ------------------------------------------------------- result comparison */
+
+/* The figures of the reference's result-diff tool (utils/diffResult/
+ * main.cpp:62-121) for two moment sets a and b of n cells each (m*x, m*y,
+ * m*z, m per cell, e.g. two rpd_solver_get_moments outputs or two .xyzw
+ * result files): the summed moments of each, the largest mass difference
+ * over all cells, and over the cells where both masses are positive the
+ * largest and mean differences of mass, barycentre and first moments.  Host
+ * memory; no device work. */
+typedef struct rpd_moment_diff {
+  long long cells;         /* n */
+  long long cells_both;    /* cells with both masses > 0 */
+  double sum_a[4], sum_b[4];
+  double max_mass;         /* over all cells */
+  double max_bary[3], max_moment[3];
+  double avg_mass, avg_bary[3], avg_moment[3];  /* over cells_both */
+} rpd_moment_diff;
+int rpd_compare_moments(const double *a, const double *b, size_t n, rpd_moment_diff *out);
+
 /* -------------------------------------------------------- batched solves */
 
 /* Many independent diagrams solved together (no counterpart in the
