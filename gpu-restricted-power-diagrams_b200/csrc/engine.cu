@@ -715,6 +715,8 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
   d.sat = s->g_sat.as<const int>();
   d.lists_disjoint = disjoint ? 1 : 0;
   d.tsat = disjoint ? s->g_tsat.as<const int>() : nullptr;
+  s->grid_points = g->num_points();
+  s->grid_triangles = g->num_triangles();
   d.has_border_corners = 0;
   for (char c : g->in_domain)
     if (c == 1) {
@@ -1031,6 +1033,8 @@ void solver_share_grid(rpd_solver *dst, const rpd_solver *src) {
   dst->g_sat.release();
   dst->g_tsat.release();
   dst->grid = src->grid;
+  dst->grid_points = src->grid_points;
+  dst->grid_triangles = src->grid_triangles;
 }
 
 // Releases what only a call in progress needs (binning workspace,

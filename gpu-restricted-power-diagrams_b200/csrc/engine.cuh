@@ -50,6 +50,7 @@ struct DevBuf {
 void set_error(rpd_context *ctx, const std::string &msg);
 int map_cuda(rpd_context *ctx, cudaError_t e, const char *what);
 const HostGrid *host_grid(const rpd_grid *g);
+rpd_grid *grid_handle(HostGrid &&g);
 
 }  // namespace rpd
 
@@ -80,6 +81,7 @@ struct rpd_solver {
   // domain on the device
   rpd::DevBuf g_flags, g_points, g_tris, g_list, g_offsets, g_sat, g_tsat;
   rpd::DevGrid grid;           // grid.size == 0: no domain
+  int grid_points = 0, grid_triangles = 0;  // of the domain's surface
   // results (stored order) and pass bookkeeping
   rpd::DevBuf out;             // double4[n]
   rpd::DevBuf status;          // int[n]

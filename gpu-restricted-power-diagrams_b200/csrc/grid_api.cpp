@@ -11,6 +11,11 @@ struct rpd_grid {
 
 namespace rpd {
 const HostGrid *host_grid(const rpd_grid *g) { return g ? &g->g : nullptr; }
+rpd_grid *grid_handle(HostGrid &&g) {
+  auto *r = new rpd_grid();
+  r->g = std::move(g);
+  return r;
+}
 }  // namespace rpd
 
 extern "C" {

@@ -323,9 +323,12 @@ void make_ellipsoid_blob(int size, int nell, const double *centres, const double
   if (g.volume() < 0) g.swap_orientation();
 }
 
-void make_random_blob(int size, int nell, uint64_t seed, HostGrid &g) {
+void random_blob_params(int nell, uint64_t seed, std::vector<double> &c, std::vector<double> &a,
+                        std::vector<double> &R) {
   SplitMix rng(seed);
-  std::vector<double> c(3 * nell), a(3 * nell), R(9 * nell);
+  c.assign(3 * size_t(nell), 0.0);
+  a.assign(3 * size_t(nell), 0.0);
+  R.assign(9 * size_t(nell), 0.0);
   for (int e = 0; e < nell; ++e) {
     for (int d = 0; d < 3; ++d) c[3 * e + d] = 0.35 + 0.3 * rng.uniform();
     for (int d = 0; d < 3; ++d) a[3 * e + d] = 0.15 + 0.2 * rng.uniform();
@@ -344,6 +347,11 @@ void make_random_blob(int size, int nell, uint64_t seed, HostGrid &g) {
                          2 * (x * z - y * w),     2 * (y * z + x * w),     1 - 2 * (x * x + y * y)};
     for (int r = 0; r < 9; ++r) R[9 * e + r] = m[r];
   }
+}
+
+void make_random_blob(int size, int nell, uint64_t seed, HostGrid &g) {
+  std::vector<double> c, a, R;
+  random_blob_params(nell, seed, c, a, R);
   make_ellipsoid_blob(size, nell, c.data(), a.data(), R.data(), g);
 }
 

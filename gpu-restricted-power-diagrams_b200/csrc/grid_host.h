@@ -44,6 +44,9 @@ void make_ellipsoid_blob(int size, int nell, const double *centres, const double
 // Seeded random blob: centres U[0.35,0.65]^3, semi-axes U[0.15,0.35], random
 // rotations (the domain of the benchmark configurations).
 void make_random_blob(int size, int nell, uint64_t seed, HostGrid &g);
+// The ellipsoids of make_random_blob (centres, semi-axes, rotations).
+void random_blob_params(int nell, uint64_t seed, std::vector<double> &c, std::vector<double> &a,
+                        std::vector<double> &R);
 // The cube [d, 1000-d]^3, d = half a voxel, as a domain: no voxel corner on
 // its surface (flags 0 outside, 2 inside); faces cut by the voxel columns,
 // 2 triangles per rectangle, listed in their voxel.

@@ -102,6 +102,10 @@ def lib():
         L.rpd_solver_trace_cell.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_solver_get_hessian.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_compare_moments.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+        L.rpd_solver_set_grid_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.rpd_solver_set_grid_blob.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64]
+        L.rpd_solver_export_grid.restype = C.c_void_p
+        L.rpd_solver_export_grid.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
         L.rpd_batch_create.restype = C.c_void_p
         L.rpd_batch_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.rpd_batch_launch.argtypes = [C.c_void_p]
@@ -268,6 +272,32 @@ class Solver:
         self.ctx.check(lib().rpd_solver_set_grid(self.h, grid.h if grid is not None else None))
         self._grid = grid
         return self
+
+    def set_grid_blob(self, size, nellipsoids=5, seed=2):
+        """The seeded blob of Grid.blob, built on the device."""
+        self.ctx.check(lib().rpd_solver_set_grid_blob(self.h, int(size), int(nellipsoids), int(seed)))
+        self._grid = None
+        return self
+
+    def set_grid_field(self, field):
+        """The domain {field < 0} of a field on the (S+1)^3 corner lattice
+        (numpy (S+1, S+1, S+1) indexed [z, y, x], or flat x-fastest), built
+        on the device."""
+        f = np.ascontiguousarray(field, np.float32).reshape(-1)
+        s1 = round(len(f) ** (1.0 / 3.0))
+        if s1 ** 3 != len(f) or s1 < 2:
+            raise ValueError("field must hold (S+1)^3 values")
+        self.ctx.check(lib().rpd_solver_set_grid_field(self.h, s1 - 1, _ptr(f), RPD_HOST))
+        self._grid = None
+        return self
+
+    def export_grid(self):
+        """The solver's domain as a host Grid."""
+        err = C.c_int(0)
+        h = lib().rpd_solver_export_grid(self.h, C.byref(err))
+        if not h:
+            raise RpdError(err.value, self.ctx.error())
+        return Grid(h)
 
     def launch(self, params=None, **kw):
         p = params if params is not None else Params.default(**kw)

@@ -142,6 +142,27 @@ rpd_grid *rpd_grid_make_cube(int size, int *err);
  * Returns the number of points (n unless the darts saturate). */
 int rpd_synth_poisson_disk(int n, uint64_t seed, double rfac, float *xyzw);
 
+/* Domains built on the device (no counterpart in the reference, whose
+ * domains come from its host tool utils/createGrid): no host preprocessing
+ * and no host copy, e.g. for served requests with new domains.
+ *
+ * rpd_solver_set_grid_field: the domain {field < 0} of an implicit function
+ * sampled on the (size+1)^3 voxel-corner lattice (x fastest, the lattice
+ * spans [0,1000]^3; host or device memory; the lattice's outer layer is taken
+ * as outside so the surface closes inside the grid).  Corner flags, the
+ * surface by marching the 6 Kuhn tetrahedra of every voxel, per-voxel
+ * triangle lists and the solver's lookup tables are built on the device.
+ * rpd_solver_set_grid_blob: the seeded blob of rpd_grid_make_blob, evaluated
+ * and built on the device: the same corner flags and, voxel by voxel, the
+ * same triangles (vertex coordinates bit for bit) in the same order, so
+ * solves give the same results; only the numbering of the surface vertices
+ * differs.  size <= 1024.  rpd_solver_export_grid copies a solver's domain
+ * (however it was set) into a new host grid, e.g. to save it in the --grid
+ * format. */
+int rpd_solver_set_grid_field(rpd_solver *s, int size, const float *field, rpd_mem where);
+int rpd_solver_set_grid_blob(rpd_solver *s, int size, int nellipsoids, uint64_t seed);
+rpd_grid *rpd_solver_export_grid(rpd_solver *s, int *err);
+
 /* --------------------------------------------------------------- solve */
 
 /* Launch flags. */
