@@ -355,7 +355,7 @@ struct rpd_batch {
   DevBuf d_statics, d_states, d_descs, d_descs_inline, d_knn, d_kstart, d_start_grid, d_start_plain, d_rc_start,
       d_all_start;
   DevBuf f0, f1, s0, s1, scan_tiles;
-  DevBuf retry_knn, defer_slots, defer_part, defer_fail, defer_ctr;
+  DevBuf retry_knn, defer_slots, defer_part, defer_fail, defer_ctr, work;
   DiagState *host_states = nullptr;  // pinned
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -467,6 +467,8 @@ int capture(rpd_batch *b) {
   int Kmin = kMaxK, Kmax = 0, Pmax = 0, Vmax = 0, Tmax = 0, J = 0;
   bool any_grid = false, any_plain = false, defer = true;
   bool class_used[kKnnClasses] = {};
+  long class_rows[kKnnClasses] = {};
+  long rows_grid0 = 0, rows_plain0 = 0;  // the first pass's rows
   std::vector<int> all_start(nd + 1, 0);
   for (int d = 0; d < nd; ++d) {
     const DiagStatic &g = G[d];
@@ -482,7 +484,11 @@ int capture(rpd_batch *b) {
     (g.grid.size > 0 ? any_grid : any_plain) = true;
     if (b->params[d].flags & RPD_FLAG_NO_DEFER) defer = false;
     for (int c = 0; c < kKnnClasses; ++c)
-      if (knn_slots(g.K0) == kKnnClassSlots[c]) class_used[c] = true;
+      if (knn_slots(g.K0) == kKnnClassSlots[c]) {
+        class_used[c] = true;
+        class_rows[c] += g.n;
+      }
+    (g.grid.size > 0 ? rows_grid0 : rows_plain0) += g.n;
   }
   if (cells >= (1ll << 31) - 2) {
     set_error(ctx, "batch: more than 2^31 cells");
@@ -541,6 +547,7 @@ int capture(rpd_batch *b) {
         (e = b->defer_ctr.ensure(sizeof(int) * 2)) != cudaSuccess)
       return map_cuda(ctx, e, "alloc batch defer");
   }
+  if ((e = b->work.ensure(sizeof(int))) != cudaSuccess) return map_cuda(ctx, e, "alloc batch");
   if (!b->host_states && (e = cudaMallocHost(&b->host_states, sizeof(DiagState) * nd)) != cudaSuccess)
     return map_cuda(ctx, e, "alloc batch host");
   for (auto &x : b->ev)
@@ -616,7 +623,8 @@ int capture(rpd_batch *b) {
       const int S = kKnnClassSlots[c];
       const bool want = j == 0 ? class_used[c] : (S >= knn_slots(Kmin) && S <= knn_slots(Kb[j]));
       if (!want) continue;
-      if ((e = knn_batch_launch(S, pl.knn, pl.kstart + c * stride, nd, knn_blocks, st)) != cudaSuccess)
+      if ((e = knn_batch_launch(S, pl.knn, pl.kstart + c * stride, nd, knn_blocks, st, j == 0 ? class_rows[c] : -1)) !=
+          cudaSuccess)
         return fail(e, "batch knn");
       ++launches;
     }
@@ -634,6 +642,11 @@ int capture(rpd_batch *b) {
     cb.V = Vb[j];
     cb.T = Tb[j];
     cb.after_cell = j == 0 ? b->ev[2] : nullptr;
+    // the first pass's rows are every cell: one warp per row; the retries'
+    // rows are known on the device only: persistent, rows from a counter
+    cb.rows_grid = j == 0 ? rows_grid0 : -1;
+    cb.rows_plain = j == 0 ? rows_plain0 : -1;
+    cb.work = b->work.as<int>();
     if ((e = cell_batch_launch(cb, st, ctx->sm_count, &launches)) != cudaSuccess) return fail(e, "batch cells");
     // failing cells of the pass's diagrams
     k_fail_flags_batch<<<flat_blocks, 256, 0, st>>>(ds, sts, pl.rc_start, nd, b->f0.as<int>(), b->f1.as<int>());

@@ -2069,22 +2069,37 @@ __global__ void __launch_bounds__(128, 5) k_cell(const __grid_constant__ CellLau
 // warps stride over the rows.  park_counter (optional): the re-run of the
 // cells that found the defer queue full, which exits unless the queue
 // overflowed.
+// work (optional, zeroed before the launch): warps take their rows one at a
+// time from this counter (persistent launches of unknown row counts, so a
+// warp that drew heavy rows does not hold the launch back); null: warp w
+// takes rows w, w + warps, ... (a grid of one warp per row takes one each).
 template <int VS, bool GRID, bool INL>
 __global__ void __launch_bounds__(128, 5)
     k_cell_batch(const CellLaunch *__restrict__ descs, const int *__restrict__ start, int ndiag,
                  const __grid_constant__ Layout L, int only_status, const int *__restrict__ park_counter,
-                 int park_capacity) {
+                 int park_capacity, int *__restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (park_counter && *park_counter <= park_capacity) return;
   const int lane = threadIdx.x & 31;
   unsigned char *wsmem = smem + size_t(threadIdx.x >> 5) * L.total;
   const int total = start[ndiag];
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < total; r += nwarps) {
+  int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (work) {
+    r = lane == 0 ? atomicAdd(work, 1) : 0;
+    r = __shfl_sync(kFull, r, 0);
+  }
+  while (r < total) {
     const int d = owner_of_row(start, ndiag, r);
     const CellLaunch &a = descs[d];
     cell_row<VS, GRID, INL>(a, L, wsmem, r - start[d], only_status, vertex_capacity(a, L), lane);
     __syncwarp();  // the warp's shared memory is reused by its next row
+    if (work) {
+      r = lane == 0 ? atomicAdd(work, 1) : 0;
+      r = __shfl_sync(kFull, r, 0);
+    } else {
+      r += nwarps;
+    }
   }
 }
 
@@ -2316,17 +2331,28 @@ int resident_blocks(Kernel k, int threads, size_t smem, int sm_count) {
   return per_sm * sm_count;
 }
 
+// rows >= 0: the launch's row count is known: one warp per row.  Else a
+// persistent launch; with `work`, rows are taken from that counter (zeroed
+// here, on the stream).
 template <int VS, bool GRID, bool INL>
 cudaError_t batch_cells(const CellLaunch *descs, const int *start, int ndiag, const Layout &L, int only_status,
-                        const int *park_counter, int park_capacity, cudaStream_t st, int sm_count) {
+                        const int *park_counter, int park_capacity, long rows, int *work, cudaStream_t st,
+                        int sm_count) {
   const int wpb = warps_per_block_for(L);
   if (wpb == 0) return cudaErrorInvalidValue;
   const size_t smem = size_t(L.total) * wpb;
   auto k = k_cell_batch<VS, GRID, INL>;
   cudaError_t e = allow_smem(reinterpret_cast<const void *>(k), smem);
   if (e != cudaSuccess) return e;
-  k<<<resident_blocks(k, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(descs, start, ndiag, L, only_status,
-                                                                         park_counter, park_capacity);
+  int blocks;
+  if (rows >= 0) {
+    blocks = int(std::max<long>(1, (rows + wpb - 1) / wpb));
+    work = nullptr;
+  } else {
+    blocks = resident_blocks(k, wpb * 32, smem, sm_count);
+    if (work && (e = cudaMemsetAsync(work, 0, sizeof(int), st)) != cudaSuccess) return e;
+  }
+  k<<<blocks, wpb * 32, smem, st>>>(descs, start, ndiag, L, only_status, park_counter, park_capacity, work);
   return cudaGetLastError();
 }
 
@@ -2340,23 +2366,23 @@ cudaError_t launch_batch_vs(const CellBatch &b, const Layout &Lg, const Layout &
                             int *launches) {
   cudaError_t e;
   if (b.start_plain) {
-    if ((e = batch_cells<VS, false, true>(b.descs_inline, b.start_plain, b.ndiag, Lp, -1, nullptr, 0, st,
-                                          sm_count)) != cudaSuccess)
+    if ((e = batch_cells<VS, false, true>(b.descs_inline, b.start_plain, b.ndiag, Lp, -1, nullptr, 0, b.rows_plain,
+                                          b.work, st, sm_count)) != cudaSuccess)
       return e;
     if (launches) ++*launches;
   }
   if (!b.start_grid) return record_after_cell(b, st);
   if (!b.defer.slots) {
-    if ((e = batch_cells<VS, true, true>(b.descs_inline, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, st,
-                                         sm_count)) != cudaSuccess)
+    if ((e = batch_cells<VS, true, true>(b.descs_inline, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, b.rows_grid,
+                                         b.work, st, sm_count)) != cudaSuccess)
       return e;
     if (launches) ++*launches;
     return record_after_cell(b, st);
   }
   // every boundary cell parks; the chunked kernel does the triangles, then
   // the cells that found the queue full run again inline
-  if ((e = batch_cells<VS, true, false>(b.descs, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, st, sm_count)) !=
-      cudaSuccess)
+  if ((e = batch_cells<VS, true, false>(b.descs, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, b.rows_grid, b.work, st,
+                                        sm_count)) != cudaSuccess)
     return e;
   if ((e = record_after_cell(b, st)) != cudaSuccess) return e;
   const int wpb = warps_per_block_for(Lg);
@@ -2366,7 +2392,7 @@ cudaError_t launch_batch_vs(const CellBatch &b, const Layout &Lg, const Layout &
   kc<<<resident_blocks(kc, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(b.descs, b.defer, Lg);
   k_cone_finish_batch<<<sm_count * 4, 128, 0, st>>>(b.descs, b.defer, Lg);
   if ((e = batch_cells<VS, true, true>(b.descs_inline, b.start_grid, b.ndiag, Lg, kParkOverflow, b.defer.counters,
-                                       b.defer.capacity, st, sm_count)) != cudaSuccess)
+                                       b.defer.capacity, -1, b.work, st, sm_count)) != cudaSuccess)
     return e;
   if (launches) *launches += 4;
   return cudaGetLastError();

@@ -127,6 +127,10 @@ struct CellBatch {
   DeferQueue defer;                  // slots == null: every boundary cell inline
   int P = 0, V = 0, T = 0;           // layout caps: at least every diagram's caps of this pass
   cudaEvent_t after_cell = nullptr;  // recorded (as a graph node when capturing) after the cell kernel
+  // rows of the diagrams with / without a domain when known when the launch
+  // is made (one warp per row), else -1 (persistent launches)
+  long rows_grid = -1, rows_plain = -1;
+  int *work = nullptr;  // one device int: the row counter of persistent launches (optional)
 };
 cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches = nullptr);
 

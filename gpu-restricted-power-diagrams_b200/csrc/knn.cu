@@ -281,7 +281,9 @@ void ring_bounds(int dim, float *bound) {
   }
 }
 
-cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st) {
+cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st,
+                             long rows) {
+  if (rows >= 0) blocks = int(rows * 32 / kKnnThreads + 1);
   switch (S) {
     case 1: k_knn_batch<1><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;
     case 2: k_knn_batch<2><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;

@@ -38,6 +38,9 @@ constexpr int kKnnClassSlots[kKnnClasses] = {1, 2, 3, 4, 6, 8};
 // Persistent launch over the rows of every diagram of slot class S:
 // start[0..ndiag] (device) are the row prefixes of the diagrams in this
 // class (empty for the others); `blocks` fixed, the rows read on the device.
-cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st);
+// rows >= 0: the class's row count, known when the launch is made: one warp
+// per row; else `blocks` persistent blocks.
+cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st,
+                             long rows = -1);
 
 }  // namespace rpd
