@@ -1985,7 +1985,8 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
       }
     }
   }
-  if (status == kSuccess && !reached && !exhausted && !outside) status = kSecurityRadiusNotReached;
+  if (status == kSuccess && !reached && !exhausted && !outside)
+    status = a.K < a.K_full ? kNeedMoreNeighbours : kSecurityRadiusNotReached;
   const int np_cell = w.np;  // the clipped cell's planes (cone planes come after)
   if (a.border_d > 0) {
     // bordering pass (ConvexCell.cl:756-809): the clipped cell marks its
