@@ -314,8 +314,7 @@ def run_ours(args, cfg, rank, world, local):
     a = grid.arrays() if grid is not None else None
     grid_bytes = 0 if a is None else int(a["in_domain"].nbytes + a["offsets"].nbytes + a["tri_list"].nbytes +
                                          a["triangles"].nbytes + len(a["points"]) * 16)
-    # the first pass's neighbour rows hold min(K, 32) entries (rpd_solver_launch)
-    alg_bytes = n * (4 * min(cfg["K"], 32) + 16 + 32 + 4) + grid_bytes
+    alg_bytes = n * (4 * cfg["K"] + 16 + 32 + 4) + grid_bytes
     cell_avg_ms = sum(cell_ms) / len(cell_ms)
     achieved = alg_bytes / (cell_avg_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()

@@ -1985,8 +1985,7 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
       }
     }
   }
-  if (status == kSuccess && !reached && !exhausted && !outside)
-    status = a.K < a.K_full ? kNeedMoreNeighbours : kSecurityRadiusNotReached;
+  if (status == kSuccess && !reached && !exhausted && !outside) status = kSecurityRadiusNotReached;
   const int np_cell = w.np;  // the clipped cell's planes (cone planes come after)
   if (a.border_d > 0) {
     // bordering pass (ConvexCell.cl:756-809): the clipped cell marks its
@@ -2270,10 +2269,14 @@ cudaError_t allow_smem(const void *fn, size_t smem) {
   if (e != cudaSuccess) return e;
   int optin = 0;
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
-  if (smem > size_t(optin)) return cudaErrorInvalidValue;
+  cudaFuncAttributes fa;
+  if ((e = cudaFuncGetAttributes(&fa, fn)) != cudaSuccess) return e;
+  // the dynamic limit leaves room for the kernel's static shared memory
+  const int room = optin - int(fa.sharedSizeBytes);
+  if (smem > size_t(room)) return cudaErrorInvalidValue;
   std::lock_guard<std::mutex> lock(mu);
   if (done.count({fn, dev})) return cudaSuccess;
-  if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, room)) != cudaSuccess) return e;
   done.insert({fn, dev});
   return cudaSuccess;
 }
@@ -2284,8 +2287,10 @@ int warps_per_block_for(const Layout &L) {
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  // a little room for the kernels' static shared memory
+  const size_t room = size_t(optin) - 256;
   int w = 4;
-  while (w > 0 && size_t(L.total) * w > size_t(optin)) w >>= 1;
+  while (w > 0 && size_t(L.total) * w > room) w >>= 1;
   return w;
 }
 

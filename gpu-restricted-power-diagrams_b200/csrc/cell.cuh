@@ -88,9 +88,6 @@ struct CellLaunch {
   int mark_dist = 0;
   int border_d = 0;
   int diag = 0;  // index of this diagram in a batched launch (parked cells record it)
-  // > K: the neighbour rows are the first K of the pass's K_full nearest;
-  // a cell that needs more gets kNeedMoreNeighbours instead of failing
-  int K_full = 0;
   // --hessian (no defer queue): per cell a row of H facets, HC values each,
   // and their neighbours (stored ids, -1 after the last), stored order
   double *hess = nullptr;
@@ -98,9 +95,6 @@ struct CellLaunch {
   int H = 0, HC = 1;
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
-// internal status: the cell used all K neighbours of a shortened list
-// (K < K_full) without reaching its security radius; re-run with K_full
-constexpr int kNeedMoreNeighbours = 102;
 constexpr int kTraceRecord = 12;
 
 // Largest caps of one build: P <= 255 (uchar plane ids in the reference,

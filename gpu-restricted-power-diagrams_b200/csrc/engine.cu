@@ -189,11 +189,6 @@ __global__ void k_border_flags(const unsigned char *__restrict__ used, const dou
   if (i > n) return;
   f[i] = i < n && int(used[i]) + 1 == d && out[i].w < eps;
 }
-__global__ void k_status_flags(const int *__restrict__ status, int n, int value, int *__restrict__ f) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > n) return;
-  f[i] = i < n && status[i] == value;
-}
 __global__ void k_scatter_flagged(const int *__restrict__ f, const int *__restrict__ pos, int n, int *__restrict__ out,
                                   int *__restrict__ count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -258,27 +253,6 @@ int recompute_ids(rpd_solver *s, const int *ids_in, int num, int cond, int *out0
   return RPD_OK;
 }
 
-// Stored ids of the cells with status `value` into ids_c, ascending.
-int select_status(rpd_solver *s, int value, int &count) {
-  rpd_context *ctx = s->ctx;
-  cudaStream_t st = ctx->stream;
-  cudaError_t e;
-  const int n = s->n;
-  const size_t nsc = scan_workspace_ints(n + 1);
-  if ((e = s->fail_ws.ensure(sizeof(int) * (2 * size_t(n + 1) + nsc + 1))) != cudaSuccess)
-    return map_cuda(ctx, e, "alloc status ws");
-  int *f = s->fail_ws.as<int>(), *pos = f + (n + 1), *tiles = pos + (n + 1), *cnt = tiles + nsc;
-  const int tb = 256;
-  k_status_flags<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(s->status.as<int>(), n, value, f);
-  if ((e = exclusive_scan(f, pos, n + 1, tiles, st)) != cudaSuccess) return map_cuda(ctx, e, "scan");
-  k_scatter_flagged<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(f, pos, n, s->ids_c.as<int>(), cnt);
-  s->stats.kernel_launches += 5;
-  if ((e = cudaMemcpyAsync(&count, cnt, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-    return map_cuda(ctx, e, "copy count");
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "status ids");
-  return RPD_OK;
-}
-
 int select_bordering(rpd_solver *s, int d, int &count) {
   rpd_context *ctx = s->ctx;
   cudaStream_t st = ctx->stream;
@@ -333,11 +307,8 @@ int count_used(rpd_solver *s) {
 // nearest of the listed seeds, then their cells with this pass's caps.
 static_assert(int(RPD_CTR_NUM) == int(kCtrNum), "counter enums out of sync");
 
-// K_full > K: the rows hold the K nearest of the pass's K_full (cells that
-// need more report kNeedMoreNeighbours); sub_pass: the re-run of those cells
-// with K_full, timed into the current pass.
 int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T, float eps, int out_domain,
-             bool counters, bool early_out, int border_d = 0, int K_full = 0, bool sub_pass = false) {
+             bool counters, bool early_out, int border_d = 0) {
   rpd_context *ctx = s->ctx;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
@@ -376,7 +347,6 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.out_domain = out_domain;
   a.early_out = early_out ? 1 : 0;
   a.inner_apex = s->inner_apex ? 1 : 0;
-  a.K_full = K_full;
   if (s->used_on) {
     a.used = s->used.as<unsigned char>();
     a.keep_volume = s->keep_volume;
@@ -433,15 +403,9 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   S.kernel_launches += launches - 1;
   cudaEventRecord(ev[2], st);
   if ((e = cudaEventSynchronize(ev[2])) != cudaSuccess) return map_cuda(ctx, e, "pass");
-  if (sub_pass && pi > 0 && pi <= 8) {
-    float t = 0.f;
-    cudaEventElapsedTime(&t, ev[0], ev[1]);
-    S.pass_knn_ms[pi - 1] += t;
-    cudaEventElapsedTime(&t, ev[1], ev[2]);
-    S.pass_cell_ms[pi - 1] += t;
-  } else if (!sub_pass && pi < 8) {
+  if (pi < 8) {
     S.pass_cells[pi] = num;
-    S.pass_K[pi] = K_full > K ? K_full : K;
+    S.pass_K[pi] = K;
     S.pass_P[pi] = P;
     S.pass_V[pi] = V;
     S.pass_T[pi] = T;
@@ -450,7 +414,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
     if (num > 0) cudaEventElapsedTime(&S.pass_cell_kernel_ms[pi], ev[1], ev[3]);
   }
   for (auto &x : ev) cudaEventDestroy(x);
-  if (!sub_pass) S.npasses++;
+  S.npasses++;
   S.kernel_launches += num > 0 ? 1 : 0;  // the cell kernel (the neighbour kernel counted above)
   return RPD_OK;
 }
@@ -826,20 +790,8 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
     if ((e = s->used.ensure(size_t(n))) != cudaSuccess) return map_cuda(ctx, e, "alloc used");
     cudaMemsetAsync(s->used.ptr, 0, size_t(n), st);
   }
-  // the first pass's neighbour rows hold at most 32 (one register slot of
-  // the search): most cells are done before using them; those that are not
-  // run again with all K (the 32 nearest are the first 32 of the K nearest,
-  // so results are the same as with all K from the start)
-  const int K1 = (p.K > 32 && !counters) ? 32 : p.K;
-  int rc = run_pass(s, nullptr, n, K1, p.P, p.V, T0, eps, 0, counters, early, 0, p.K);
+  int rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
   if (rc != RPD_OK) return rc;
-  if (K1 < p.K) {
-    int more = 0;
-    if ((rc = select_status(s, kNeedMoreNeighbours, more)) != RPD_OK) return rc;
-    if (more > 0 &&
-        (rc = run_pass(s, s->ids_c.as<int>(), more, p.K, p.P, p.V, T0, eps, 0, counters, early, 0, 0, true)) != RPD_OK)
-      return rc;
-  }
   int K = p.K, P = p.P, V = p.V, T = p.T;
   if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {
     int hist[kStatusNum];
