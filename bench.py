@@ -179,6 +179,59 @@ def cpu_baseline(x, grid, cfg, target_s=10.0):
                       f"{t:.2f} s on {os.cpu_count()} host threads"}
 
 
+def accuracy(solver, x, grid, cfg, m_gpu, st_gpu, target_s=10.0):
+    """The device results against the FP64 oracle (restated reference, exact
+    neighbour order) on a bounded sample of the same diagram (every stride-th
+    binned seed, all passes): per-cell relative mass error and barycentre
+    error (normalised by the domain extent, 1000), status mismatches, the
+    symmetric difference of the non-empty cells; and the neighbour lists of
+    every seed against the oracle's (mismatching rows)."""
+    import oracle
+
+    a = grid.arrays() if grid is not None else None
+    ga = (oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+          if a is not None else None)
+    xd = x.astype(np.float64)
+    n = len(x)
+    kw = dict(grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], use_double=True, knn_mode=1,
+              return_stats=True)
+
+    def run(stride):
+        b, s, st = oracle.solve(xd, sample_stride=stride, **kw)
+        return b, s, st["knn_seconds"] + st["cell_seconds"], st["pass_cells"][0], st
+
+    stride = max(1, n // 5000)
+    _, _, t, cells, _ = run(stride)
+    stride = max(1, int(round(n / max(1.0, cells / max(t, 1e-9) * target_s))))
+    b, s, t, cells, ost = run(stride)
+    # the sampled cells: every stride-th seed of the oracle's own binning (in
+    # FP64 a few seeds near bin faces fall into the next bin), as user ids
+    _, perm, _ = oracle.bin_seeds(xd, use_double=True)
+    u = np.asarray(perm)[::stride]
+    both = (st_gpu[u] == 4) & (s[u] == 4)
+    m, mr = m_gpu[u, 3], b[u, 3]
+    rel = np.abs(m - mr)[both] / np.maximum(np.abs(mr[both]), 1e-3)
+    nz = both & (np.abs(mr) > 1e-3) & (np.abs(m) > 1e-3)
+    bary = (np.abs(m_gpu[u][nz, :3] / m[nz, None] - b[u][nz, :3] / mr[nz, None]).max(1) / 1000.0
+            if nz.any() else np.zeros(1))
+    ne = (np.abs(m) > 1e-3) & (st_gpu[u] == 4)
+    ner = (np.abs(mr) > 1e-3) & (s[u] == 4)
+    kg = solver.knn(cfg["K"])
+    ko = oracle.knn(xd, cfg["K"], knn_mode=1)
+    return {"oracle": "FP64 restatement, exact neighbour order", "cells": int(len(u)), "stride": stride,
+            "status_mismatch": int((st_gpu[u] != s[u]).sum()),
+            "nonempty_symdiff": int((ne != ner).sum()),
+            "mass_max_rel": float(rel.max()) if rel.size else 0.0,
+            "mass_rms_rel": float(np.sqrt((rel ** 2).mean())) if rel.size else 0.0,
+            "bary_max": float(bary.max()), "bary_rms": float(np.sqrt((bary ** 2).mean())),
+            "knn_rows_mismatch": int((kg != ko).any(1).sum()), "knn_rows": int(n), "oracle_seconds": round(t, 2),
+            # the reference algorithm's FP64 work on the sample, per cell: 45 flops
+            # per half-space test (det4x4 by cofactors), 41 per vertex from its
+            # three planes, 60 per vertex integrated (restated kernels' counts)
+            "fp64_flops_per_cell": (45.0 * ost["hs_tests"] + 41.0 * ost["vertex_evals"] +
+                                    60.0 * ost["export_vertices"]) / max(1, cells)}
+
+
 def run_reference(args, cfg, rank, world):
     """--impl reference: the reference's CPU implementation of the path on the
     host cores (rank 0 only)."""
@@ -248,14 +301,29 @@ def run_ours(args, cfg, rank, world, local):
                                 device_id=torch.device("cuda", local))
     ctx = rpd.Context(local)
     x = make_seeds(cfg, rank)
+    t0 = time.perf_counter()
     grid = make_grid(cfg)
+    setup = {"grid_host_build_s": time.perf_counter() - t0}
     n = len(x)
     # every timed step is a full solve: neighbours included (repeated launches
     # on unchanged seeds would otherwise reuse the neighbour table)
     params = rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_FRESH_NEIGHBOURS)
     solver = rpd.Solver(ctx).set_points(x)
+    t0 = time.perf_counter()
+    solver.set_points(x)  # again, timed: upload from host memory + binning
+    setup["set_points_ms"] = 1e3 * (time.perf_counter() - t0)
     if grid is not None:
+        t0 = time.perf_counter()
         solver.set_grid(grid)
+        setup["set_grid_ms"] = 1e3 * (time.perf_counter() - t0)
+        if cfg.get("grid") == "blob":
+            # the same domain built on the device instead (rpd_solver_set_grid_blob)
+            scratch = rpd.Solver(ctx).set_points(x[:16])
+            scratch.set_grid_blob(cfg["gsize"], cfg["nell"], cfg["gseed"])
+            t0 = time.perf_counter()
+            scratch.set_grid_blob(cfg["gsize"], cfg["nell"], cfg["gseed"])
+            setup["grid_device_build_ms"] = 1e3 * (time.perf_counter() - t0)
+            scratch.close()
     for _ in range(args.warmup):
         solver.launch(params)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
@@ -285,6 +353,8 @@ def run_ours(args, cfg, rank, world, local):
     barrier()
     clk = clocks.stop()
     last_stats = solver.stats()
+    m_gpu, st_gpu = solver.moments(), solver.status()
+    nonempty = int(((st_gpu == 4) & (m_gpu[:, 3] > 0)).sum())
     # one untimed launch with the work counters on
     solver.launch(rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_COUNTERS))
     work = solver.stats()["counters"]
@@ -348,9 +418,22 @@ def run_ours(args, cfg, rank, world, local):
         "detail": {"knn_ms": sum(knn_ms) / len(knn_ms), "cell_ms_first_pass": cell_avg_ms,
                    "passes": last_stats["passes"], "status": last_stats["status"],
                    "npasses": npasses[-1], "step_ms": step_ms, "work_counters": work},
+        "nonempty_cells": nonempty,
+        "nonempty_cells_per_s": nonempty * world / (ms / 1e3),
+        "setup": setup,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x, grid, cfg, target_s=args.cpu_seconds)
+        line["accuracy"] = acc = accuracy(solver, x, grid, cfg, m_gpu, st_gpu, target_s=args.cpu_seconds)
+        # the clipping's own bound is FP64 issue, not HBM: the reference
+        # algorithm's FP64 operations of the whole solve against B200's FP64 rate
+        # (datasheet: not measured on this pool)
+        flops = acc["fp64_flops_per_cell"] * n
+        line["roofline_fp64"] = {"bound": "fp64", "achieved": flops / (ms / 1e3) / 1e12, "unit": "TFLOP/s",
+                                 "peak": 40.0, "peak_source": "nominal B200 FP64 (datasheet; not measured here)",
+                                 "frac": flops / (ms / 1e3) / 1e12 / 40.0, "flops_per_solve": flops,
+                                 "work_unit": "45 per half-space test + 41 per vertex + 60 per integrated vertex, "
+                                              "the reference algorithm's counts (FP64 oracle on the sample)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     solver.close()
