@@ -705,7 +705,7 @@ def run_serve(args, cfg, rank):
     arrivals = np.cumsum(gaps) - gaps[0]
     kw = dict(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"])
     # warm-up: one solve and one re-solve (allocator pool, grid upload)
-    with rpd.Server(slots=cfg["slots"]) as sv:
+    with rpd.Server(slots=args.slots or cfg["slots"]) as sv:
         t, sess = sv.solve(pool[:200_000], grid=grid_for(200_000)[1], **kw)
         sv.wait(t)
         sv.wait(sv.reweight(sess, pool[:200_000, 3], **kw))
@@ -780,7 +780,7 @@ def run_serve(args, cfg, rank):
     line = {
         "metric": "served cells/s and p50/p99 latency (config 5)", "value": cells / span, "unit": "cells/s",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f64 geometry on f32 seeds", "data": "synthetic",
-        "config": {"workload": "serve-200rps", "description": cfg["desc"], "slots": cfg["slots"]},
+        "config": {"workload": "serve-200rps", "description": cfg["desc"], "slots": args.slots or cfg["slots"]},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "p50_reweight_ms": float(np.percentile([d[2]["latency_ms"] for d in rw], 50)) if rw else None,
         "p50_device_ms": float(np.percentile(dev, 50)), "requests": len(done), "reweights": len(rw),
@@ -802,6 +802,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--slots", type=int, default=None, help="serving configs: concurrent slots (default: the config's)")
     ap.add_argument("--diagrams", type=int, default=None,
                     help="batch configs: solve only the first N diagrams (small cases for profiling)")
     args = ap.parse_args()
