@@ -345,7 +345,9 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.T = T;
   a.cube_eps = eps;
   a.out_domain = out_domain;
-  a.early_out = early_out ? 1 : 0;
+  // an empty cell is used when keep_volume <= 0, and a used cell marks the
+  // plane neighbours of its whole clipped cell: no early exit then
+  a.early_out = early_out && !(s->used_on && s->keep_volume <= 0.0) ? 1 : 0;
   a.inner_apex = s->inner_apex ? 1 : 0;
   if (s->used_on) {
     a.used = s->used.as<unsigned char>();

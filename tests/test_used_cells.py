@@ -20,16 +20,16 @@ def case():
 
 
 @pytest.mark.skipif(not oracle.has_reference_kernels(), reason="reference kernels not built here")
-@pytest.mark.parametrize("keep_distance", [0, 1, 2, 3])
-def test_restatement_bitexact_with_reference_kernels(case, keep_distance):
+@pytest.mark.parametrize("keep_distance,keep_volume", [(0, 1.0), (1, 1.0), (2, 1.0), (3, 1.0), (0, 0.0), (1, 0.0)])
+def test_restatement_bitexact_with_reference_kernels(case, keep_distance, keep_volume):
     x, grid = case
-    kw = dict(K=30, P=30, V=40, T=100, knn_mode=0, keep_distance=keep_distance, keep_volume=1.0)
+    kw = dict(K=30, P=30, V=40, T=100, knn_mode=0, keep_distance=keep_distance, keep_volume=keep_volume)
     b1, s1, u1 = oracle.solve_used(x, grid, kernels=1, **kw)
     b0, s0, u0 = oracle.solve_used(x, grid, kernels=0, **kw)
     assert np.array_equal(s0, s1)
     assert np.array_equal(b0, b1)
     assert np.array_equal(u0, u1)
-    assert u0.max() == max(keep_distance, 1 if (b0[:, 3] >= 1.0).any() else 0)
+    assert u0.max() == max(keep_distance, 1 if (b0[:, 3] >= keep_volume).any() else 0)
 
 
 def test_rings_grow_with_distance(case):

@@ -52,3 +52,23 @@ def test_used_cells_off_by_default(rpd):
     s.launch(K=30, P=30, V=40)
     with pytest.raises(rpd.RpdError):
         s.used()
+
+
+@pytest.mark.parametrize("keep_distance", [0, 1])
+def test_used_cells_at_zero_keep_volume(rpd, keep_distance):
+    """keep_volume 0: every succeeding cell is used, the empty ones outside
+    the domain too, and each marks the plane neighbours of its whole clipped
+    cell (the early exit outside the domain is off)."""
+    g = rpd.Grid.blob(40, 5, 2)
+    a = g.arrays()
+    og = oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+    x = jittered(24, seed=7, weights=True)
+    kw = dict(K=50, P=30, V=40, T=100)
+    s = rpd.Solver().set_points(x).set_grid(g)
+    s.launch(keep_distance=keep_distance, keep_volume=0.0, **kw)
+    rows, ids = s.used()
+    b, st, u = oracle.solve_used(x.astype(np.float64), og, keep_distance=keep_distance, keep_volume=0.0,
+                                 use_double=True, knn_mode=1, **kw)
+    ref_rows, ref_ids = oracle.compact(b, u, keep_distance, 0.0)
+    assert np.array_equal(ids, ref_ids)
+    assert np.array_equal(rows[:, 3] <= -100000.0, ref_rows[:, 3] <= -100000.0)
