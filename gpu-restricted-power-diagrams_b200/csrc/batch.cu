@@ -41,6 +41,7 @@ struct DiagStatic {
   int max_extra;   // retry passes allowed (0: first pass only)
   int out_domain;  // start-corner fallback of the retry passes
   int early_out, inner_apex;
+  const int *wmin;  // the smallest weight of the seeds that are not walls (float_to_ordered)
   float cube_eps;
   DevGrid grid;
   int *status;
@@ -258,6 +259,7 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     a.cube_eps = g.cube_eps;
     a.out_domain = pa.pass == 0 ? 0 : g.out_domain;
     a.early_out = g.early_out;
+    a.wmin = g.wmin;
     a.inner_apex = g.inner_apex;
     a.grid = g.grid;
     a.status = g.status;
@@ -439,6 +441,7 @@ int describe(rpd_batch *b, std::vector<DiagStatic> &out) {
     g.max_extra = (p.flags & RPD_FLAG_FIRST_PASS_ONLY) ? 0 : std::max(0, p.max_extra_passes);
     g.out_domain = p.out_domain >= 0 ? p.out_domain : (grid && s->grid.has_border_corners ? 1 : 0);
     g.early_out = (p.flags & RPD_FLAG_NO_EARLY_OUT) ? 0 : 1;
+    g.wmin = s->wmin.as<int>();
     g.inner_apex = (p.flags & RPD_FLAG_REFERENCE_APEX) ? 0 : 1;
     g.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
     g.grid = s->grid;

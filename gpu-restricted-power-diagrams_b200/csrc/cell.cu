@@ -37,6 +37,8 @@
 #include <utility>
 
 #include "cell.cuh"
+#include "bins.cuh"
+#include "select.cuh"
 
 namespace rpd {
 
@@ -1875,6 +1877,18 @@ __device__ __forceinline__ void mark_neighbours(unsigned char *used, const unsig
   }
 }
 
+// Whether the seed lies strictly inside its own power cell, which is then
+// not empty.  The bisector with b keeps the seed when |s - b|^2 + w_b - w_s
+// > 0 (a wall's plane always does), which holds for every b when
+// w_s - min w < d^2, d^2 a lower bound of the nearest other seed's squared
+// distance (vmask bit 0: there is one) and min w over the seeds that are not
+// walls.  The early exits outside the domain need it: an empty cell's status
+// is empty_cell, not success.  The factor covers the float rounding of
+// neighbour orders and bins.
+__device__ __forceinline__ bool nonempty_cell(float4 s, unsigned vmask, double d2_nearest, const int *wmin) {
+  return (vmask & 1u) && double(s.w) - double(ordered_to_float(__ldg(wmin))) < 0.999 * d2_nearest;
+}
+
 // The vertex capacity a cell of this launch works with.  A batched launch's
 // layout may hold more vertices than a diagram's cap (it is sized for every
 // diagram); capacity-dependent choices follow the diagram's own cap, so a
@@ -1927,8 +1941,8 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
   // ---- power clipping by the K nearest, in order ----
   const unsigned *nrow = a.knn + size_t(row) * a.K;
   bool reached = false, exhausted = false, outside = false;
-  const bool early = GRID && a.early_out && a.grid.sat != nullptr && a.border_d == 0;
-  const double plain2 = early ? plain_radius2(a.grid, s, lane) : -1.0;
+  const bool early = GRID && a.early_out && a.grid.sat != nullptr && a.wmin != nullptr && a.border_d == 0;
+  double plain2 = early ? plain_radius2(a.grid, s, lane) : -1.0;
   for (int i0 = 0; i0 < a.K && status == kSuccess && !reached && !exhausted && !outside; i0 += 32) {
     // every lane builds the bisector of one neighbour, in double
     const int i = i0 + lane;
@@ -1953,6 +1967,7 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
       }
     }
     const unsigned vmask = __ballot_sync(kFull, valid);
+    if (i0 == 0 && plain2 >= 0.0 && !nonempty_cell(s, vmask, __shfl_sync(kFull, nd2, 0), a.wmin)) plain2 = -1.0;
     const int cnt = min(32, a.K - i0);
     for (int j = 0; j < cnt; ++j) {
       if (!((vmask >> j) & 1u)) {
@@ -2062,6 +2077,98 @@ __global__ void __launch_bounds__(128, 5) k_cell(const __grid_constant__ CellLau
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= a.num) return;
   cell_row<VS, GRID, INL>(a, L, smem + size_t(threadIdx.x >> 5) * L.total, row, a.only_status, L.Vc, lane);
+}
+
+// Outside probe (ProbeLaunch), one warp per stored seed.  Candidates: the
+// seeds of the 3x3x3 bins around the seed's bin (up to 8 rounds of 32), the
+// 32 nearest kept by warp bitonic merges; their bisectors clip the box in
+// distance order until the cell fits the plainly-outside ball.
+template <int VS>
+__global__ void __launch_bounds__(128, 6) k_probe(const __grid_constant__ ProbeLaunch p,
+                                                  const __grid_constant__ Layout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= p.n) return;
+  WarpCell w = bind(smem + size_t(threadIdx.x >> 5) * L.total, L);
+  const float4 s = p.stored[row];
+  const double plain2 = s.w <= kNoCellLimits ? -1.0 : plain_radius2(p.grid, s, lane);
+  bool proven = false;
+  if (plain2 >= p.min_plain * p.min_plain) {
+    // candidate rows of the 3x3x3 block: lane q < 9 holds row (y, z) offsets
+    const int dim = p.dim, cin = bin_of(s, dim);
+    const int cx = cin % dim, cy = (cin / dim) % dim, cz = cin / (dim * dim);
+    int a0 = 0, cnt = 0;
+    if (lane < 9) {
+      const int y = cy + lane % 3 - 1, z = cz + lane / 3 - 1;
+      if (y >= 0 && y < dim && z >= 0 && z < dim) {
+        const int rb = (y + z * dim) * dim;
+        a0 = __ldg(&p.bins[rb + max(cx - 1, 0)]);
+        cnt = __ldg(&p.bins[rb + min(cx + 1, dim - 1) + 1]) - a0;
+      }
+    }
+    const int incl = warp_incl_scan(cnt, lane);
+    const int all = __shfl_sync(kFull, incl, 31);
+    const int total = min(all, 8 * 32);
+    unsigned long long best = kEmptyKey;
+    for (int base = 0; base < total; base += 32) {
+      const int c = base + lane;
+      int owner = 0;  // the first lane whose inclusive count exceeds c
+#pragma unroll
+      for (int step = 8; step > 0; step >>= 1) {
+        const int v = __shfl_sync(kFull, incl, owner + step - 1);
+        if (v <= c) owner += step;
+      }
+      const int o_start = __shfl_sync(kFull, a0, owner) - (__shfl_sync(kFull, incl, owner) - __shfl_sync(kFull, cnt, owner));
+      unsigned long long key = kEmptyKey;
+      if (c < total) {
+        const int ptr = o_start + c;
+        if (ptr != row) {
+          const float4 q = __ldg(&p.stored[ptr]);
+          const float dx = q.x - s.x, dy = q.y - s.y, dz = q.z - s.z;
+          const float d = dx * dx + dy * dy + dz * dz;
+          key = (static_cast<unsigned long long>(__float_as_uint(d)) << 32) | unsigned(ptr);
+        }
+      }
+      const unsigned long long sorted = bitonic_sort32(key, lane);
+      best = bitonic_merge32(umin64(best, __shfl_sync(kFull, sorted, 31 - lane)), lane);
+    }
+    // lane j: the bisector with the j-th nearest candidate (as cell_row
+    // builds it)
+    Plane pl{0.0, 0.0, 0.0, 0.0};
+    const bool valid = best != kEmptyKey;
+    double nd2 = 0.0;
+    if (valid) {
+      const float4 b = __ldg(&p.stored[unsigned(best & 0xffffffffull)]);
+      const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
+      nd2 = bx * bx + by * by + bz * bz;
+      const double len = sqrt(nd2), inv = 1.0 / len;
+      const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) * (0.5 * inv);
+      pl = Plane{-bx * inv, -by * inv, -bz * inv, off};
+    }
+    const unsigned vmask = __ballot_sync(kFull, valid);
+    const int nb = __popc(vmask);
+    // every seed within a bin width of this one lies in the block, so the
+    // nearest candidate (when all were read) or that width bounds the
+    // nearest seed's distance
+    const double bw = 0.999 * 1000.0 / dim;
+    const double d2n = fmin(__shfl_sync(kFull, nd2, 0), bw * bw);
+    const bool go = all == total && nonempty_cell(s, vmask, d2n, p.wmin);
+    if (go) init_box(w, s, p.cube_eps, lane);
+    int status = kSuccess;
+    for (int j = 0; go && j < nb && w.np < p.P; ++j) {
+      const int r = clip<VS>(w, shfl_plane(pl, j), p.V, status, lane, nullptr, nullptr, 0);
+      if (r < 0) break;
+      if (r > 0 && cell_radius2<VS>(w, lane) <= plain2) {
+        proven = true;
+        break;
+      }
+    }
+  }
+  if (lane == 0) {
+    p.status[row] = proven ? kSuccess : kProbeMiss;
+    if (proven) p.out[row] = make_double4(0.0, 0.0, 0.0, 0.0);
+  }
 }
 
 // Rows of many diagrams in one persistent launch (batched solves): diagram
@@ -2437,6 +2544,35 @@ cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count, int 
   if (vs <= 4) return launch_vs<4>(a, L, st, sm_count, launches);
   if (vs <= 6) return launch_vs<6>(a, L, st, sm_count, launches);
   return launch_vs<8>(a, L, st, sm_count, launches);
+}
+
+cudaError_t probe_launch(const ProbeLaunch &p, cudaStream_t st) {
+  if (p.n <= 0) return cudaSuccess;
+  if (p.P > kMaxP || p.V > kMaxV || p.P < 7 || p.V < 8 || !p.grid.sat || !p.wmin) return cudaErrorInvalidValue;
+  const Layout L = make_layout(p.P, p.V, 0, false);
+  const int wpb = warps_per_block_for(L);
+  if (wpb == 0) return cudaErrorInvalidValue;
+  const size_t smem = size_t(L.total) * wpb;
+  const int blocks = (p.n + wpb - 1) / wpb;
+  const int vs = L.Vc / 32;
+  cudaError_t e;
+#define RPD_PROBE(VSN)                                                              \
+  e = allow_smem(reinterpret_cast<const void *>(k_probe<VSN>), smem);               \
+  if (e != cudaSuccess) return e;                                                   \
+  k_probe<VSN><<<blocks, wpb * 32, smem, st>>>(p, L);
+  if (vs <= 2) {
+    RPD_PROBE(2)
+  } else if (vs <= 3) {
+    RPD_PROBE(3)
+  } else if (vs <= 4) {
+    RPD_PROBE(4)
+  } else if (vs <= 6) {
+    RPD_PROBE(6)
+  } else {
+    RPD_PROBE(8)
+  }
+#undef RPD_PROBE
+  return cudaGetLastError();
 }
 
 }  // namespace rpd

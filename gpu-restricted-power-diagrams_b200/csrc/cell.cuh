@@ -66,6 +66,8 @@ struct CellLaunch {
   float cube_eps = 0.f;            // box [-eps, 1000+eps]^3
   int out_domain = 0;              // GRID_OUT_DOMAIN fallback for the start corner
   int early_out = 1;               // stop clipping cells proven outside the domain (needs grid.sat)
+  const int *wmin = nullptr;       // the smallest weight of the seeds that are not walls
+                                   // (float_to_ordered); null: no early exit
   int inner_apex = 1;              // cone apex at a grid corner inside the cell when there is one
   DevGrid grid;                    // grid.size == 0: no domain
   int *status = nullptr;           // n, stored order
@@ -95,6 +97,7 @@ struct CellLaunch {
   int H = 0, HC = 1;
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
+constexpr int kProbeMiss = 102;     // internal status: the outside probe proved nothing
 constexpr int kTraceRecord = 12;
 
 // Largest caps of one build: P <= 255 (uchar plane ids in the reference,
@@ -110,6 +113,28 @@ size_t defer_slot_bytes(int P, int V, int T);
 // k_cell over the rows; with a domain and a defer queue, also the chunked
 // boundary-triangle kernel and the per-cell reduction (3 launches).
 cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count = 148, int *launches = nullptr);
+
+// Outside probe of a first pass with a domain: every seed whose ball of
+// plainly-outside voxels (flag 0, no triangle) has a radius of at least
+// min_plain is clipped by its 32 nearest among the 3x3x3 bins around its
+// own (a subset of all seeds, so the clipped cell contains the seed's power
+// cell).  A cell that then fits the ball is the domain's empty cell: status
+// success and mass 0, as the full solve gives it.  Every other row gets
+// kProbeMiss and is solved by the full pass.
+struct ProbeLaunch {
+  const float4 *stored = nullptr;  // n seeds in stored (bin) order
+  int n = 0;
+  const int *bins = nullptr;       // dim^3 + 1 bin starts of the stored order
+  int dim = 0;
+  DevGrid grid;                    // with its summed-volume table (grid.sat)
+  int P = 0, V = 0;                // caps of the first pass
+  float cube_eps = 0.f;
+  double min_plain = 0.0;          // reference-frame units
+  const int *wmin = nullptr;       // the smallest weight of the seeds that are not walls (float_to_ordered)
+  int *status = nullptr;           // n, stored order
+  double4 *out = nullptr;          // n, stored order
+};
+cudaError_t probe_launch(const ProbeLaunch &p, cudaStream_t st);
 
 // Whether one warp's layout for these caps fits a block's shared memory.
 bool cell_caps_fit(int P, int V, int T, bool grid);

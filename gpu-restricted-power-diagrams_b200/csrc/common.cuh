@@ -28,6 +28,17 @@ constexpr unsigned kFull = 0xffffffffu;
 // Bins per axis of the seed grid: round((n / 3.1)^(1/3)) (knearests.cpp:63).
 int bins_per_axis(int n);
 
+// Floats as ints in the same order (atomicMax on float values): the sign
+// bit flips the rest for negative values.
+__host__ __device__ __forceinline__ int float_to_ordered(float f) {
+  union { float f; int i; } u{f};
+  return u.i >= 0 ? u.i : u.i ^ 0x7fffffff;
+}
+__host__ __device__ __forceinline__ float ordered_to_float(int i) {
+  union { int i; float f; } u{i >= 0 ? i : i ^ 0x7fffffff};
+  return u.f;
+}
+
 // Batched launches: diagram d owns rows start[d] .. start[d+1]; the owner of
 // row r (0 <= r < start[ndiag]) is the last d with start[d] <= r, which
 // skips diagrams without rows.

@@ -1,6 +1,8 @@
 // Host side of the engine: context, seed binning and neighbour queries
 // behind the C ABI declared in include/rpd.h.
 #include <algorithm>
+#include <climits>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -112,6 +114,18 @@ __global__ void k_fail_scatter(const int *__restrict__ ids, int num, const int *
   const int sid = ids ? ids[i] : i;
   if (f0[i]) out0[s0[i]] = sid;
   if (f1[i]) out1[s1[i]] = sid;
+}
+
+// Rows the outside probe left: f[i] = 1 where status is kProbeMiss; f[n] = 0.
+__global__ void k_probe_flags(const int *__restrict__ status, int n, int *__restrict__ f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) f[i] = status[i] == kProbeMiss;
+  else if (i == n) f[i] = 0;
+}
+
+__global__ void k_probe_scatter(int n, const int *__restrict__ f, const int *__restrict__ pos, int *__restrict__ ids) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && f[i]) ids[pos[i]] = i;
 }
 
 template <class T>
@@ -303,6 +317,52 @@ int count_used(rpd_solver *s) {
   return rc;
 }
 
+// Outside probe (probe_launch) over every seed of a first pass, then the
+// stored ids of the seeds it left into `ids`, ascending; synchronous.  The
+// probe proves cells empty when their plainly-outside ball is at least 1.5
+// mean seed spacings wide.
+int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
+  rpd_context *ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const int n = s->n;
+  const size_t nsc = scan_workspace_ints(n + 1);
+  if ((e = s->fail_ws.ensure(sizeof(int) * (2 * size_t(n + 1) + nsc))) != cudaSuccess)
+    return map_cuda(ctx, e, "alloc probe ws");
+  int *f = s->fail_ws.as<int>(), *pos = f + (n + 1), *tiles = pos + (n + 1);
+  cudaEvent_t ev[2];
+  for (auto &x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], st);
+  ProbeLaunch pr;
+  pr.stored = s->stored.as<float4>();
+  pr.n = n;
+  pr.bins = s->counters.as<int>();
+  pr.dim = s->dim;
+  pr.grid = s->grid;
+  pr.P = P;
+  pr.V = V;
+  pr.cube_eps = eps;
+  pr.min_plain = 1.5 * 1000.0 / std::cbrt(double(n));
+  pr.wmin = s->wmin.as<int>();
+  pr.status = s->status.as<int>();
+  pr.out = s->out.as<double4>();
+  if ((e = probe_launch(pr, st)) != cudaSuccess) return map_cuda(ctx, e, "probe");
+  const int tb = 256;
+  k_probe_flags<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(s->status.as<int>(), n, f);
+  if ((e = exclusive_scan(f, pos, n + 1, tiles, st)) != cudaSuccess) return map_cuda(ctx, e, "scan");
+  k_probe_scatter<<<(n + tb - 1) / tb, tb, 0, st>>>(n, f, pos, ids);
+  cudaEventRecord(ev[1], st);
+  int cnt = 0;
+  cudaMemcpyAsync(&cnt, pos + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "probe");
+  cudaEventElapsedTime(&s->stats.probe_ms, ev[0], ev[1]);
+  for (auto &x : ev) cudaEventDestroy(x);
+  s->stats.probe_outside = n - cnt;
+  s->stats.kernel_launches += 6;  // probe, flags, scan (3), scatter
+  nmiss = cnt;
+  return RPD_OK;
+}
+
 // One pass (VoroAlgoComputeData::launch, voronoi.cpp:861-1036): the K
 // nearest of the listed seeds, then their cells with this pass's caps.
 static_assert(int(RPD_CTR_NUM) == int(kCtrNum), "counter enums out of sync");
@@ -348,6 +408,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   // an empty cell is used when keep_volume <= 0, and a used cell marks the
   // plane neighbours of its whole clipped cell: no early exit then
   a.early_out = early_out && !(s->used_on && s->keep_volume <= 0.0) ? 1 : 0;
+  a.wmin = s->wmin.as<int>();
   a.inner_apex = s->inner_apex ? 1 : 0;
   if (s->used_on) {
     a.used = s->used.as<unsigned char>();
@@ -371,7 +432,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
     // boundary cells with many triangles are parked and their triangles
     // spread over all warps; cells past the capacity stay inline
     DeferQueue &dq = a.defer;
-    dq.capacity = std::min(num, std::max(32768, num / 8));
+    dq.capacity = std::min(num, std::max(32768, s->n / 8));
     dq.slot_bytes = defer_slot_bytes(P, V, T);
     dq.chunk = 32;  // a warp's lanes take one triangle each
     dq.inline_max = 16;
@@ -487,6 +548,30 @@ void rpd_solver_destroy(rpd_solver *s) {
   delete s;
 }
 
+// The smallest weight of the stored seeds that are not walls
+// (w > RPD_NO_CELL_LIMITS) into *wmin (float_to_ordered; set to INT_MAX
+// first; stays INT_MAX when every seed is a wall).
+__global__ void k_weight_min(const float4 *__restrict__ stored, int n, int *__restrict__ wmin) {
+  int m = INT_MAX;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float w = stored[i].w;
+    if (w > kNoCellLimits) m = min(m, float_to_ordered(w));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(kFull, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMin(wmin, m);
+}
+
+cudaError_t update_wmin(rpd_solver *s, cudaStream_t st) {
+  cudaError_t e;
+  if ((e = s->wmin.ensure(sizeof(int))) != cudaSuccess) return e;
+  static const int highest = INT_MAX;
+  if ((e = cudaMemcpyAsync(s->wmin.ptr, &highest, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  const int blocks = std::min((s->n + 255) / 256, 4 * s->ctx->sm_count);
+  k_weight_min<<<std::max(blocks, 1), 256, 0, st>>>(s->stored.as<float4>(), s->n, s->wmin.as<int>());
+  return cudaGetLastError();
+}
+
 int rpd_solver_set_points(rpd_solver *s, const float *xyzw, int n, rpd_mem where) {
   if (!s || !xyzw || n <= 0) return RPD_ERR_INVALID;
   rpd_context *ctx = s->ctx;
@@ -527,10 +612,12 @@ int rpd_solver_set_points(rpd_solver *s, const float *xyzw, int n, rpd_mem where
     s->n = 0;
     return RPD_ERR_DEGENERATE;
   }
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "bin seeds");
   s->n = n;
+  if ((e = update_wmin(s, st)) != cudaSuccess) return map_cuda(ctx, e, "smallest weight");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "bin seeds");
   s->dim = dim;
   s->knn_full_K = 0;
+  s->launches_since_points = 0;
   return RPD_OK;
 }
 
@@ -561,6 +648,7 @@ int rpd_solver_set_weights(rpd_solver *s, const float *w, rpd_mem where) {
   k_set_weights<<<(n + 255) / 256, 256, 0, st>>>(src, s->user_to_stored.as<int>(), n, s->user.as<float4>(),
                                                  s->stored.as<float4>());
   if ((e = cudaGetLastError()) != cudaSuccess) return map_cuda(ctx, e, "set weights");
+  if ((e = update_wmin(s, st)) != cudaSuccess) return map_cuda(ctx, e, "smallest weight");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "set weights");
   s->have_results = false;
   return RPD_OK;
@@ -792,7 +880,25 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
     if ((e = s->used.ensure(size_t(n))) != cudaSuccess) return map_cuda(ctx, e, "alloc used");
     cudaMemsetAsync(s->used.ptr, 0, size_t(n), st);
   }
-  int rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
+  // outside probe: with a domain, most seeds outside it are proven empty
+  // from a few neighbours and the first pass searches the full K nearest of
+  // the others only.  On the first launch after the seeds were set (or with
+  // fresh neighbours); later launches build the whole neighbour table once,
+  // which weight-only re-solves then keep.
+  const bool table_kept = s->knn_full_K == p.K && !s->fresh_knn;
+  const bool probe = grid && early && s->grid.sat && !counters && s->hess_h == 0 &&
+                     !(s->used_on && s->keep_volume <= 0.0) && !table_kept &&
+                     (s->launches_since_points == 0 || s->fresh_knn) && !(p.flags & RPD_FLAG_NO_PROBE);
+  int rc;
+  if (probe) {
+    int nmiss = 0;
+    int *miss = s->ids_b.as<int>();
+    if ((rc = run_probe(s, p.P, p.V, eps, miss, nmiss)) != RPD_OK) return rc;
+    rc = run_pass(s, miss, nmiss, p.K, p.P, p.V, T0, eps, 0, counters, early);
+    s->stats.pass_cells[0] = n;  // the reference's first pass: every seed
+  } else {
+    rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
+  }
   if (rc != RPD_OK) return rc;
   int K = p.K, P = p.P, V = p.V, T = p.T;
   if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {
@@ -845,6 +951,7 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   for (int i = 0; i < RPD_CTR_NUM; ++i) s->stats.counters[i] = c64[i];
   s->stats.knn_candidates = c64[RPD_CTR_NUM];
   s->have_results = true;
+  s->launches_since_points++;
   return RPD_OK;
 }
 
@@ -922,6 +1029,7 @@ int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *pp, doub
   a.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
   a.out_domain = p.out_domain > 0 ? 1 : 0;
   a.early_out = (p.flags & RPD_FLAG_NO_EARLY_OUT) ? 0 : 1;
+  a.wmin = s->wmin.as<int>();
   a.inner_apex = (p.flags & RPD_FLAG_REFERENCE_APEX) ? 0 : 1;
   a.grid = s->grid;
   a.status = s->status.as<int>();

@@ -70,11 +70,13 @@ struct rpd_solver {
   rpd::DevBuf perm;            // int[n] stored -> user
   rpd::DevBuf user_to_stored;  // int[n]
   rpd::DevBuf weights;         // float[n]: staging for rpd_solver_set_weights
+  rpd::DevBuf wmin;            // int: the smallest weight of the seeds that are not walls (float_to_ordered)
   rpd::DevBuf counters;        // int[dim^3+1]
   rpd::DevBuf bin_ws;
   rpd::DevBuf ring_bound;      // float[dim+2]
   rpd::DevBuf knn;             // unsigned[n*K]: every cell's neighbours (stored ids)
   int knn_full_K = 0;          // K of the table in knn for all n cells (0: none)
+  int launches_since_points = 0;  // launches since the seeds were set (the outside probe runs on the first)
   rpd::DevBuf knn_part;        // unsigned[num*K]: rows of a retry pass or a trace
   rpd::DevBuf knn_user;        // int[n*K]
   rpd::DevBuf counter64;       // unsigned long long[RPD_CTR_NUM + 1]

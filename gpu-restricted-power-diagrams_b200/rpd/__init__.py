@@ -125,6 +125,7 @@ FLAG_NO_EARLY_OUT = 4
 FLAG_NO_DEFER = 8
 FLAG_REFERENCE_APEX = 16
 FLAG_FRESH_NEIGHBOURS = 32
+FLAG_NO_PROBE = 64
 COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
                  "exports", "export_vertices", "outside_early", "cone_empty", "cones_skipped"]
 
@@ -151,7 +152,8 @@ class Stats(C.Structure):
                 ("pass_P", C.c_int * 8), ("pass_V", C.c_int * 8), ("pass_T", C.c_int * 8),
                 ("pass_knn_ms", C.c_float * 8), ("pass_cell_ms", C.c_float * 8), ("status_hist", C.c_int * 11),
                 ("counters", C.c_ulonglong * 11), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
-                ("kernel_launches", C.c_int), ("pass_cell_kernel_ms", C.c_float * 8)]
+                ("kernel_launches", C.c_int), ("pass_cell_kernel_ms", C.c_float * 8), ("probe_outside", C.c_int),
+                ("probe_ms", C.c_float)]
 
     def as_dict(self):
         n = self.npasses
@@ -166,6 +168,8 @@ class Stats(C.Structure):
             "knn_candidates": int(self.knn_candidates),
             "total_ms": self.total_ms,
             "kernel_launches": self.kernel_launches,
+            "probe_outside": self.probe_outside,
+            "probe_ms": self.probe_ms,
         }
 
 

@@ -178,6 +178,9 @@ rpd_grid *rpd_solver_export_grid(rpd_solver *s, int *err);
 #define RPD_FLAG_FRESH_NEIGHBOURS 32u /* recompute the neighbour table even when the
                                          seeds' positions and K are unchanged since
                                          the last launch (same results) */
+#define RPD_FLAG_NO_PROBE 64u       /* no outside probe before the first pass: every
+                                       seed gets its full K-nearest search (same
+                                       results) */
 
 /* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
 typedef struct rpd_params {
@@ -232,6 +235,16 @@ typedef struct rpd_stats {
   float total_ms;                  /* device time of the whole launch */
   int kernel_launches;             /* device kernels this launch ran */
   float pass_cell_kernel_ms[8];    /* of pass_cell_ms: the cell kernel alone (no cone kernels) */
+  /* Outside probe of the first pass (with a domain, on the first launch
+   * after rpd_solver_set_points or with RPD_FLAG_FRESH_NEIGHBOURS; not with
+   * counters, Hessian rows or used cells at keep_volume <= 0): the cells it
+   * proved empty outside the domain without a full neighbour search, and its
+   * device time.  The first pass's neighbour search and cell kernel then
+   * cover the other seeds; pass_cells[0] still counts every seed.  A later
+   * launch builds the whole neighbour table, which weight-only re-solves
+   * keep. */
+  int probe_outside;
+  float probe_ms;
 } rpd_stats;
 
 /* VoroAlgo::setGrid (voronoi.cpp:1079-1082): uploads the domain; null

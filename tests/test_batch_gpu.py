@@ -36,10 +36,16 @@ def build(rpd, sp, with_grid):
 
 
 def alone(rpd, x, g, p):
+    """The diagram solved on its own, without the outside probe (which
+    batches do not run): its per-pass cell counts are the batch's too (the
+    probe can settle in the first pass an empty cell outside the domain
+    that a full clip would retry)."""
     s = rpd.Solver().set_points(x)
     if g is not None:
         s.set_grid(g)
-    s.launch(p)
+    q = rpd.Params.from_buffer_copy(p)
+    q.flags |= rpd.FLAG_NO_PROBE
+    s.launch(q)
     return s
 
 

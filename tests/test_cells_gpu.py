@@ -133,6 +133,60 @@ def test_early_out_and_parking_do_not_change_results(rpd):
     assert np.array_equal(res["ref_apex_no_defer"][0], m0), "the early exit must not change any bit"
 
 
+def test_outside_probe_does_not_change_results(rpd):
+    """The outside probe (cells proven empty outside the domain from the 32
+    nearest of their 3x3x3 bins) changes no bit of any result."""
+    g = rpd.Grid.blob(60, 5, 2)
+    x = jittered(40, seed=6, weights=True)
+    s = rpd.Solver().set_points(x).set_grid(g)
+    fresh = rpd.FLAG_FRESH_NEIGHBOURS
+    s.launch(K=50, P=30, V=40, T=60, flags=fresh)
+    st = s.stats()
+    m1, s1 = s.moments(), s.status()
+    print("probe", st["probe_outside"], "of", len(x), st["probe_ms"], "ms", st["passes"][0])
+    assert st["probe_outside"] > len(x) // 4
+    assert st["passes"][0]["cells"] == len(x)
+    s.launch(K=50, P=30, V=40, T=60, flags=fresh | rpd.FLAG_NO_PROBE)
+    assert s.stats()["probe_outside"] == 0
+    assert np.array_equal(s.status(), s1)
+    assert np.array_equal(s.moments(), m1)
+    # a weight-only re-solve after a probed first launch builds the whole
+    # neighbour table (no probe), which the next one keeps
+    t = rpd.Solver().set_points(x).set_grid(g)
+    t.launch(K=50, P=30, V=40, T=60)
+    assert t.stats()["probe_outside"] > 0
+    x2 = x.copy()
+    for it in range(2):
+        x2[:, 3] = x[:, 3] * (0.5 + 0.25 * it)
+        t.set_weights(x2[:, 3])
+        t.launch(K=50, P=30, V=40, T=60)
+        st = t.stats()
+        assert st["probe_outside"] == 0
+        f = rpd.Solver().set_points(x2).set_grid(g)
+        f.launch(K=50, P=30, V=40, T=60)
+        assert np.array_equal(t.status(), f.status())
+        assert np.array_equal(t.moments(), f.moments())
+    met, *_ = run_case(rpd, x2, grid=g, K=50, P=30, V=40, T=60)
+    assert_parity(met)
+
+
+def test_empty_cells_outside_the_domain(rpd):
+    """Seeds far outside the domain whose weight empties their power cell
+    keep the status empty_cell: the early exits outside the domain (the cell
+    kernel's and the outside probe's) only take cells that cannot be empty."""
+    g = rpd.Grid.blob(40, 5, 2)
+    x = jittered(24, seed=11, weights=True)
+    h2 = (1000.0 / 24) ** 2
+    corner = (x[:, :3] < 150).all(axis=1) | (x[:, :3] > 850).all(axis=1)
+    idx = np.where(corner)[0][::3]
+    x[idx, 3] = 4 * h2
+    for flags in (0, rpd.FLAG_NO_PROBE):
+        met, got, gst, ref, rst, stats = run_case(rpd, x, grid=g, K=50, P=30, V=40,
+                                                  flags=flags | rpd.FLAG_FRESH_NEIGHBOURS)
+        assert (rst[idx] == 6).sum() > len(idx) // 2
+        assert_parity(met)
+
+
 def test_blue_noise_cube_domain(rpd):
     # BASELINE config 3 in small: Poisson-disk seeds, unit cube domain
     from rpd import synth

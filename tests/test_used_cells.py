@@ -20,7 +20,7 @@ def case():
 
 
 @pytest.mark.skipif(not oracle.has_reference_kernels(), reason="reference kernels not built here")
-@pytest.mark.parametrize("keep_distance,keep_volume", [(0, 1.0), (1, 1.0), (2, 1.0), (3, 1.0), (0, 0.0), (1, 0.0)])
+@pytest.mark.parametrize("keep_distance,keep_volume", [(0, 1.0), (1, 1.0), (2, 1.0), (3, 1.0), (0, 0.0), (1, -1.0)])
 def test_restatement_bitexact_with_reference_kernels(case, keep_distance, keep_volume):
     x, grid = case
     kw = dict(K=30, P=30, V=40, T=100, knn_mode=0, keep_distance=keep_distance, keep_volume=keep_volume)

@@ -55,20 +55,23 @@ def test_used_cells_off_by_default(rpd):
 
 
 @pytest.mark.parametrize("keep_distance", [0, 1])
-def test_used_cells_at_zero_keep_volume(rpd, keep_distance):
-    """keep_volume 0: every succeeding cell is used, the empty ones outside
-    the domain too, and each marks the plane neighbours of its whole clipped
-    cell (the early exit outside the domain is off)."""
+def test_used_cells_at_negative_keep_volume(rpd, keep_distance):
+    """keep_volume <= 0: every succeeding cell is used, the empty ones
+    outside the domain too, and each marks the plane neighbours of its whole
+    clipped cell (the early exit outside the domain is off).  At exactly 0
+    the set would hang on the sign of zero masses, which the two cone
+    decompositions round differently; -1 takes every cell."""
     g = rpd.Grid.blob(40, 5, 2)
     a = g.arrays()
     og = oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
     x = jittered(24, seed=7, weights=True)
     kw = dict(K=50, P=30, V=40, T=100)
     s = rpd.Solver().set_points(x).set_grid(g)
-    s.launch(keep_distance=keep_distance, keep_volume=0.0, **kw)
+    s.launch(keep_distance=keep_distance, keep_volume=-1.0, **kw)
     rows, ids = s.used()
-    b, st, u = oracle.solve_used(x.astype(np.float64), og, keep_distance=keep_distance, keep_volume=0.0,
+    b, st, u = oracle.solve_used(x.astype(np.float64), og, keep_distance=keep_distance, keep_volume=-1.0,
                                  use_double=True, knn_mode=1, **kw)
-    ref_rows, ref_ids = oracle.compact(b, u, keep_distance, 0.0)
+    ref_rows, ref_ids = oracle.compact(b, u, keep_distance, -1.0)
     assert np.array_equal(ids, ref_ids)
+    assert len(ids) == int((st == 4).sum())
     assert np.array_equal(rows[:, 3] <= -100000.0, ref_rows[:, 3] <= -100000.0)
