@@ -2079,10 +2079,49 @@ __global__ void __launch_bounds__(128, 5) k_cell(const __grid_constant__ CellLau
   cell_row<VS, GRID, INL>(a, L, smem + size_t(threadIdx.x >> 5) * L.total, row, a.only_status, L.Vc, lane);
 }
 
-// Outside probe (ProbeLaunch), one warp per stored seed.  Candidates: the
-// seeds of the 3x3x3 bins around the seed's bin (up to 8 rounds of 32), the
-// 32 nearest kept by warp bitonic merges; their bisectors clip the box in
-// distance order until the cell fits the plainly-outside ball.
+// Cage test of the outside probe: bit i of the result is set when the
+// candidate's bisector bounds every direction u within kCageCover of the
+// stencil direction d_i (the 26 unit vectors (x, y, z)/|(x, y, z)|, x, y, z
+// in {-1, 0, 1}) to at most r from the seed.  Those directions cover the
+// sphere: every unit vector lies within 27.57 degrees of one of them
+// (kCageCover = 28 keeps a margin).  The bisector keeps x . n <= off (n the
+// unit vector towards the candidate, off its offset, positive for a cell
+// that cannot be empty); along u at angle at most c + t from n (t = the
+// angle of n to d_i) that bounds the cell by off / cos(c + t), which is at
+// most r when cos(c) cos(t) - off/r >= sin(c) sin(t) -- squared, no root.
+// Float, with margins far above its rounding: off/r raised by 0.1%, cos(t)
+// lowered by 1e-3.
+constexpr float kCageCos = 0.882947592858927f;   // cos(28 deg)
+constexpr float kCageSin2 = 0.2204035482646266f;  // sin(28 deg)^2
+constexpr unsigned kCageAll = (1u << 26) - 1u;
+
+__device__ __forceinline__ unsigned cage_bits(float nx, float ny, float nz, float q) {
+  unsigned bits = 0;
+  int i = 0;
+#pragma unroll
+  for (int z = -1; z <= 1; ++z)
+#pragma unroll
+    for (int y = -1; y <= 1; ++y)
+#pragma unroll
+      for (int x = -1; x <= 1; ++x) {
+        if (x == 0 && y == 0 && z == 0) continue;
+        const int nnz = (x != 0) + (y != 0) + (z != 0);
+        const float inv_norm = nnz == 1 ? 1.0f : (nnz == 2 ? 0.70710678f : 0.57735027f);
+        const float ct = (float(x) * nx + float(y) * ny + float(z) * nz) * inv_norm - 1e-3f;
+        const float lhs = kCageCos * ct - q;
+        if (lhs >= 0.0f && lhs * lhs >= kCageSin2 * (1.0f - ct * ct)) bits |= 1u << i;
+        ++i;
+      }
+  return bits;
+}
+
+// Outside probe (ProbeLaunch), one warp per stored seed, over the seeds of
+// the 3x3x3 bins around the seed's bin (up to 8 rounds of 32).  First the
+// cage test (cage_bits) with every candidate: all 26 directions bounded to
+// the plainly-outside ball proves the cell outside without clipping.  Else,
+// with a ball of at least min_plain, the 32 nearest candidates (warp
+// bitonic merges) clip the box in distance order until the cell fits the
+// ball.
 template <int VS>
 __global__ void __launch_bounds__(128, 6) k_probe(const __grid_constant__ ProbeLaunch p,
                                                   const __grid_constant__ Layout L) {
@@ -2094,7 +2133,7 @@ __global__ void __launch_bounds__(128, 6) k_probe(const __grid_constant__ ProbeL
   const float4 s = p.stored[row];
   const double plain2 = s.w <= kNoCellLimits ? -1.0 : plain_radius2(p.grid, s, lane);
   bool proven = false;
-  if (plain2 >= p.min_plain * p.min_plain) {
+  if (plain2 >= p.min_plain_cage * p.min_plain_cage) {
     // candidate rows of the 3x3x3 block: lane q < 9 holds row (y, z) offsets
     const int dim = p.dim, cin = bin_of(s, dim);
     const int cx = cin % dim, cy = (cin / dim) % dim, cz = cin / (dim * dim);
@@ -2110,58 +2149,85 @@ __global__ void __launch_bounds__(128, 6) k_probe(const __grid_constant__ ProbeL
     const int incl = warp_incl_scan(cnt, lane);
     const int all = __shfl_sync(kFull, incl, 31);
     const int total = min(all, 8 * 32);
-    unsigned long long best = kEmptyKey;
-    for (int base = 0; base < total; base += 32) {
-      const int c = base + lane;
-      int owner = 0;  // the first lane whose inclusive count exceeds c
+    // stored index of candidate c (c < total): its row's first seed plus
+    // its rank in the row (owner: the first lane whose inclusive count
+    // exceeds c)
+    auto candidate = [&](int c) {
+      int owner = 0;
 #pragma unroll
       for (int step = 8; step > 0; step >>= 1) {
         const int v = __shfl_sync(kFull, incl, owner + step - 1);
         if (v <= c) owner += step;
       }
-      const int o_start = __shfl_sync(kFull, a0, owner) - (__shfl_sync(kFull, incl, owner) - __shfl_sync(kFull, cnt, owner));
-      unsigned long long key = kEmptyKey;
-      if (c < total) {
-        const int ptr = o_start + c;
-        if (ptr != row) {
+      return __shfl_sync(kFull, a0, owner) - (__shfl_sync(kFull, incl, owner) - __shfl_sync(kFull, cnt, owner)) + c;
+    };
+    // cage test over every candidate
+    const float inv_r = float(1.0 / sqrt(plain2)) * 1.001f;
+    unsigned mask = 0;
+    float mind2 = INFINITY;
+    for (int base = 0; base < total; base += 32) {
+      const int c = base + lane;
+      const int ptr = candidate(c);
+      if (c < total && ptr != row) {
+        const float4 q = __ldg(&p.stored[ptr]);
+        const float dx = q.x - s.x, dy = q.y - s.y, dz = q.z - s.z;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        const float len = sqrtf(d2), inv = 1.0f / len;
+        const float off = q.w <= kNoCellLimits ? len : (d2 + (q.w - s.w)) * (0.5f * inv);
+        mind2 = fminf(mind2, d2);
+        mask |= cage_bits(dx * inv, dy * inv, dz * inv, off * inv_r);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mask |= __shfl_xor_sync(kFull, mask, o);
+      mind2 = fminf(mind2, __shfl_xor_sync(kFull, mind2, o));
+    }
+    // every seed within a bin width of this one lies in the block, so the
+    // nearest candidate (when all were read) or that width bounds the
+    // nearest seed's distance
+    const double bw = 0.999 * 1000.0 / dim;
+    const double d2n = fmin(double(mind2) * (1.0 - 1e-5), bw * bw);
+    const bool nonempty = all == total && nonempty_cell(s, mind2 < INFINITY ? 1u : 0u, d2n, p.wmin);
+    proven = nonempty && mask == kCageAll;
+    if (nonempty && !proven && plain2 >= p.min_plain * p.min_plain) {
+      // the 32 nearest candidates, sorted
+      unsigned long long best = kEmptyKey;
+      for (int base = 0; base < total; base += 32) {
+        const int c = base + lane;
+        const int ptr = candidate(c);
+        unsigned long long key = kEmptyKey;
+        if (c < total && ptr != row) {
           const float4 q = __ldg(&p.stored[ptr]);
           const float dx = q.x - s.x, dy = q.y - s.y, dz = q.z - s.z;
           const float d = dx * dx + dy * dy + dz * dz;
           key = (static_cast<unsigned long long>(__float_as_uint(d)) << 32) | unsigned(ptr);
         }
+        const unsigned long long sorted = bitonic_sort32(key, lane);
+        best = bitonic_merge32(umin64(best, __shfl_sync(kFull, sorted, 31 - lane)), lane);
       }
-      const unsigned long long sorted = bitonic_sort32(key, lane);
-      best = bitonic_merge32(umin64(best, __shfl_sync(kFull, sorted, 31 - lane)), lane);
-    }
-    // lane j: the bisector with the j-th nearest candidate (as cell_row
-    // builds it)
-    Plane pl{0.0, 0.0, 0.0, 0.0};
-    const bool valid = best != kEmptyKey;
-    double nd2 = 0.0;
-    if (valid) {
-      const float4 b = __ldg(&p.stored[unsigned(best & 0xffffffffull)]);
-      const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
-      nd2 = bx * bx + by * by + bz * bz;
-      const double len = sqrt(nd2), inv = 1.0 / len;
-      const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) * (0.5 * inv);
-      pl = Plane{-bx * inv, -by * inv, -bz * inv, off};
-    }
-    const unsigned vmask = __ballot_sync(kFull, valid);
-    const int nb = __popc(vmask);
-    // every seed within a bin width of this one lies in the block, so the
-    // nearest candidate (when all were read) or that width bounds the
-    // nearest seed's distance
-    const double bw = 0.999 * 1000.0 / dim;
-    const double d2n = fmin(__shfl_sync(kFull, nd2, 0), bw * bw);
-    const bool go = all == total && nonempty_cell(s, vmask, d2n, p.wmin);
-    if (go) init_box(w, s, p.cube_eps, lane);
-    int status = kSuccess;
-    for (int j = 0; go && j < nb && w.np < p.P; ++j) {
-      const int r = clip<VS>(w, shfl_plane(pl, j), p.V, status, lane, nullptr, nullptr, 0);
-      if (r < 0) break;
-      if (r > 0 && cell_radius2<VS>(w, lane) <= plain2) {
-        proven = true;
-        break;
+      // lane j: the bisector with the j-th nearest candidate (as cell_row
+      // builds it)
+      Plane pl{0.0, 0.0, 0.0, 0.0};
+      const bool valid = best != kEmptyKey;
+      if (valid) {
+        const float4 b = __ldg(&p.stored[unsigned(best & 0xffffffffull)]);
+        const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
+        const double nd2 = bx * bx + by * by + bz * bz;
+        const double len = sqrt(nd2), inv = 1.0 / len;
+        const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) * (0.5 * inv);
+        pl = Plane{-bx * inv, -by * inv, -bz * inv, off};
+      }
+      const int nb = __popc(__ballot_sync(kFull, valid));
+      init_box(w, s, p.cube_eps, lane);
+      int status = kSuccess;
+      for (int j = 0; j < nb && w.np < p.P; ++j) {
+        const int r = clip<VS>(w, shfl_plane(pl, j), p.V, status, lane, nullptr, nullptr, 0);
+        if (r < 0) break;
+        if (r > 0 && cell_radius2<VS>(w, lane) <= plain2) {
+          proven = true;
+          break;
+        }
       }
     }
   }

@@ -114,13 +114,15 @@ size_t defer_slot_bytes(int P, int V, int T);
 // boundary-triangle kernel and the per-cell reduction (3 launches).
 cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count = 148, int *launches = nullptr);
 
-// Outside probe of a first pass with a domain: every seed whose ball of
-// plainly-outside voxels (flag 0, no triangle) has a radius of at least
-// min_plain is clipped by its 32 nearest among the 3x3x3 bins around its
-// own (a subset of all seeds, so the clipped cell contains the seed's power
-// cell).  A cell that then fits the ball is the domain's empty cell: status
-// success and mass 0, as the full solve gives it.  Every other row gets
-// kProbeMiss and is solved by the full pass.
+// Outside probe of a first pass with a domain.  The seeds of the 3x3x3 bins
+// around a seed's own are a subset of all seeds, so their bisectors bound a
+// region that contains the seed's power cell.  When that region fits the
+// ball of plainly-outside voxels (flag 0, no triangle) around the seed, the
+// cell is the domain's empty cell: status success and mass 0, as the full
+// solve gives it.  Shown by a closed-form bound over 26 directions (balls of
+// at least min_plain_cage) or by clipping with the 32 nearest of them
+// (balls of at least min_plain).  Every other row gets kProbeMiss and is
+// solved by the full pass.
 struct ProbeLaunch {
   const float4 *stored = nullptr;  // n seeds in stored (bin) order
   int n = 0;
@@ -129,7 +131,8 @@ struct ProbeLaunch {
   DevGrid grid;                    // with its summed-volume table (grid.sat)
   int P = 0, V = 0;                // caps of the first pass
   float cube_eps = 0.f;
-  double min_plain = 0.0;          // reference-frame units
+  double min_plain_cage = 0.0;     // the cage test for balls at least this wide (reference frame)
+  double min_plain = 0.0;          // clipping for balls at least this wide
   const int *wmin = nullptr;       // the smallest weight of the seeds that are not walls (float_to_ordered)
   int *status = nullptr;           // n, stored order
   double4 *out = nullptr;          // n, stored order

@@ -319,8 +319,8 @@ int count_used(rpd_solver *s) {
 
 // Outside probe (probe_launch) over every seed of a first pass, then the
 // stored ids of the seeds it left into `ids`, ascending; synchronous.  The
-// probe proves cells empty when their plainly-outside ball is at least 1.5
-// mean seed spacings wide.
+// cage test runs where the plainly-outside ball is at least one mean seed
+// spacing wide, clipping where it is at least 1.5.
 int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
   rpd_context *ctx = s->ctx;
   cudaStream_t st = ctx->stream;
@@ -342,7 +342,9 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
   pr.P = P;
   pr.V = V;
   pr.cube_eps = eps;
-  pr.min_plain = 1.5 * 1000.0 / std::cbrt(double(n));
+  const double spacing = 1000.0 / std::cbrt(double(n));
+  pr.min_plain_cage = 1.0 * spacing;
+  pr.min_plain = 1.5 * spacing;
   pr.wmin = s->wmin.as<int>();
   pr.status = s->status.as<int>();
   pr.out = s->out.as<double4>();
