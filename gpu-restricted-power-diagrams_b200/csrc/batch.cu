@@ -357,7 +357,7 @@ struct rpd_batch {
   DevBuf d_statics, d_states, d_descs, d_descs_inline, d_knn, d_kstart, d_start_grid, d_start_plain, d_rc_start,
       d_all_start;
   DevBuf f0, f1, s0, s1, scan_tiles;
-  DevBuf retry_knn, defer_slots, defer_part, defer_fail, defer_ctr, work;
+  DevBuf retry_knn, defer_slots, defer_part, defer_fail, defer_ctr, defer_chunk_slot, work;
   DiagState *host_states = nullptr;  // pinned
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -547,7 +547,8 @@ int capture(rpd_batch *b) {
     if ((e = b->defer_slots.ensure(slot0 * cap0)) != cudaSuccess ||
         (e = b->defer_part.ensure(sizeof(double) * 4 * items0)) != cudaSuccess ||
         (e = b->defer_fail.ensure(sizeof(int) * items0)) != cudaSuccess ||
-        (e = b->defer_ctr.ensure(sizeof(int) * 2)) != cudaSuccess)
+        (e = b->defer_chunk_slot.ensure(sizeof(int) * items0)) != cudaSuccess ||
+        (e = b->defer_ctr.ensure(sizeof(int) * kDeferCounters)) != cudaSuccess)
       return map_cuda(ctx, e, "alloc batch defer");
   }
   if ((e = b->work.ensure(sizeof(int))) != cudaSuccess) return map_cuda(ctx, e, "alloc batch");
@@ -614,6 +615,7 @@ int capture(rpd_batch *b) {
       dq.part = b->defer_part.as<double>();
       dq.fail = b->defer_fail.as<int>();
       dq.counters = b->defer_ctr.as<int>();
+      dq.chunk_slot = b->defer_chunk_slot.as<int>();
       if (dq.capacity < 1) dq = DeferQueue();
     }
     pa.defer = dq;
@@ -631,7 +633,7 @@ int capture(rpd_batch *b) {
         return fail(e, "batch knn");
       ++launches;
     }
-    if (dq.slots && (e = cudaMemsetAsync(dq.counters, 0, sizeof(int) * 2, st)) != cudaSuccess)
+    if (dq.slots && (e = cudaMemsetAsync(dq.counters, 0, sizeof(int) * kDeferCounters, st)) != cudaSuccess)
       return fail(e, "batch memset");
     if (j == 0 && (e = mark(b->ev[1])) != cudaSuccess) return fail(e, "batch event");
     CellBatch cb;

@@ -67,14 +67,17 @@ __host__ __device__ inline int pow2_at_least(int x) {
   return g;
 }
 
-__host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid, int hc = 0) {
+// T: the pass's triangle cap (the warp's id buffer); t_slot: the ids a
+// parked cell's slot holds, when more than T (triangle overflows parked
+// ahead, CellLaunch::T_ahead).
+__host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid, int hc = 0, int t_slot = 0) {
   Layout L;
   L.HC = hc;
   L.Pc = (P + 3) & ~3;
   L.Vc = (V + 31) & ~31;
   L.G = grid ? pow2_at_least(2 * T) : 0;
   L.Mw = (L.Pc + 31) / 32;
-  L.T = T;
+  L.T = T > t_slot ? T : t_slot;
   unsigned o = 0;
   L.o_plane = o; o = align16(o + 32u * L.Pc);
   L.o_cx = o; o = align16(o + 8u * L.Vc);
@@ -1626,7 +1629,9 @@ struct DeferHeader {
   double pt0[3];
   double acc[4];
   int inner, diag;  // diag: index of the cell's diagram in a batched launch
-  double pad[8];
+  int chunk_base;   // its first work item
+  int fixed;        // >= 0: the cell's status, without any work (a cell parked ahead that failed)
+  double pad[7];
 };
 static_assert(sizeof(DeferHeader) == 144, "defer header size");
 
@@ -1634,8 +1639,15 @@ __host__ __device__ inline size_t slot_bytes_for(const Layout &L, int T) {
   return size_t(align16(unsigned(sizeof(DeferHeader) + 32u * L.Pc + 44u * L.Vc + 4u * ((T + 3) & ~3) + 4u * L.Pc)));
 }
 
+// The slot's triangle-id list (nuniq ids, room for L.T).
+__device__ __forceinline__ int *slot_list(const DeferQueue &dq, int slot, const Layout &L) {
+  unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
+  return reinterpret_cast<int *>(base + sizeof(DeferHeader) + 32u * L.Pc + 44u * L.Vc);
+}
+
+// list_in_place: the ids were gathered into the slot already.
 __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, const Layout &L, int diag, int sid,
-                          int nuniq, bool inner, const double acc[4], int lane) {
+                          int nuniq, bool inner, const double acc[4], int lane, bool list_in_place = false) {
   const int T = L.T;
   unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
   DeferHeader *h = reinterpret_cast<DeferHeader *>(base);
@@ -1644,16 +1656,23 @@ __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, con
   double *vy = vx + L.Vc, *vz = vy + L.Vc, *vw = vz + L.Vc, *vd = vw + L.Vc;
   unsigned *vt = reinterpret_cast<unsigned *>(vd + L.Vc);
   int *tl = reinterpret_cast<int *>(vt + L.Vc);
+  const int nch = (nuniq + dq.chunk - 1) / dq.chunk;
+  int cb = 0;
   if (lane == 0) {
+    cb = atomicAdd(&dq.counters[2], nch);
     h->sid = sid;
     h->nuniq = nuniq;
     h->nv = w.nv;
     h->np = w.np;
     h->inner = inner ? 1 : 0;
     h->diag = diag;
+    h->chunk_base = cb;
+    h->fixed = -1;
     for (int d = 0; d < 3; ++d) h->pt0[d] = w.pts[d];
     for (int d = 0; d < 4; ++d) h->acc[d] = acc[d];
   }
+  cb = __shfl_sync(kFull, cb, 0);
+  for (int c = lane; c < nch; c += 32) dq.chunk_slot[cb + c] = slot;
   for (int i = lane; i < w.np; i += 32) pl[i] = w.plane[i];
   for (int v = lane; v < w.nv; v += 32) {
     vx[v] = w.cx[v];
@@ -1663,10 +1682,27 @@ __device__ void park_cell(const WarpCell &w, const DeferQueue &dq, int slot, con
     vd[v] = w.d2[v];
     vt[v] = w.tri[v];
   }
-  for (int i = lane; i < nuniq; i += 32) tl[i] = w.tlist[i];
+  if (!list_in_place)
+    for (int i = lane; i < nuniq; i += 32) tl[i] = w.tlist[i];
   if (w.pnb) {
     int *nb = tl + ((T + 3) & ~3);
     for (int i = lane; i < w.np; i += 32) nb[i] = w.pnb[i];
+  }
+}
+
+// A slot taken for a cell parked ahead whose restriction ended early: its
+// status, no work items (k_cone_finish writes every taken slot's cell).
+__device__ void park_fixed(const DeferQueue &dq, int slot, int diag, int sid, int status, int lane) {
+  if (lane == 0) {
+    DeferHeader *h = reinterpret_cast<DeferHeader *>(dq.slots + size_t(slot) * dq.slot_bytes);
+    h->sid = sid;
+    h->nuniq = 0;
+    h->nv = h->np = 0;
+    h->inner = 0;
+    h->diag = diag;
+    h->chunk_base = 0;
+    h->fixed = status;
+    for (int d = 0; d < 4; ++d) h->acc[d] = 0.0;
   }
 }
 
@@ -1706,6 +1742,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   const int S = g.size;
   const int ex = vmax[0] - vmin[0] + 1, ey = vmax[1] - vmin[1] + 1, ez = vmax[2] - vmin[2] + 1;
   const int nvox = (ex > 0 && ey > 0 && ez > 0) ? ex * ey * ez : 0;
+  bool ahead = false;
   if (g.tsat && nvox > 0) {
     // disjoint lists: the range's triangle count from the summed counts
     // (lane q < 8 reads corner q); more than T fails as the merge would,
@@ -1720,7 +1757,23 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     }
 #pragma unroll
     for (int o = 4; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
-    if (__shfl_sync(kFull, part, 0) > a.T) return kTriangleOverflow;
+    const int count = __shfl_sync(kFull, part, 0);
+    if (count > a.T) {
+      // more than T: the retry passes would clip this cell again to the
+      // same cell and restrict it with a larger T; within T_ahead it is
+      // parked now, its ids gathered straight into its slot
+      if (INL || count > a.T_ahead || !a.defer.slots) return kTriangleOverflow;
+      ahead = true;
+    }
+  }
+  const DeferQueue &dq = a.defer;
+  int *tl = w.tlist, tcap = L.G, slot = 0;
+  if (ahead) {
+    if (lane == 0) slot = atomicAdd(&dq.counters[0], 1);
+    slot = __shfl_sync(kFull, slot, 0);
+    if (slot >= dq.capacity) return kTriangleOverflow;  // the retry passes take it
+    tl = slot_list(dq, slot, L);
+    tcap = L.T;
   }
   // first corner with flag != 1 in (z, y, x) scan order, and the triangle ids
   // of every voxel in the range
@@ -1748,10 +1801,10 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     }
     const int incl = warp_incl_scan(cntv, lane);
     const int tot = __shfl_sync(kFull, incl, 31);
-    if (ntr + tot > L.G) {
+    if (ntr + tot > tcap) {
       spill = true;
     } else if (!spill) {
-      for (int k = 0; k < cntv; ++k) w.tlist[ntr + incl - cntv + k] = __ldg(&g.list[lo_off + k]);
+      for (int k = 0; k < cntv; ++k) tl[ntr + incl - cntv + k] = __ldg(&g.list[lo_off + k]);
     }
     ntr += tot;
   }
@@ -1759,7 +1812,10 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   int nuniq = 0;
   if (g.lists_disjoint) {
     // no triangle is listed twice: the union is the concatenation
-    if (ntr > a.T) return kTriangleOverflow;
+    if (ntr > (ahead ? a.T_ahead : a.T)) {
+      if (ahead) park_fixed(dq, slot, a.diag, sid_of_cell, kTriangleOverflow, lane);
+      return ahead ? kDeferred : kTriangleOverflow;
+    }
     nuniq = ntr;
   } else if (spill) {
     // more ids (with repeats) than the sort buffer holds: one lane builds the
@@ -1790,9 +1846,13 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   double pt0[3] = {0, 0, 0};
   if (in_domain == 1) {
     int px = 0, py = 0, pz = 0, f = 1;
-    if (a.out_domain && lane == 0) f = out_domain_corner(g, vmin, vmax, px, py, pz);
+    // a cell parked ahead is restricted as a retry pass would restrict it
+    if ((ahead ? a.out_domain_ahead : a.out_domain) && lane == 0) f = out_domain_corner(g, vmin, vmax, px, py, pz);
     f = __shfl_sync(kFull, f, 0);
-    if (f == 1) return kFindAnotherBeginningVertex;
+    if (f == 1) {
+      if (ahead) park_fixed(dq, slot, a.diag, sid_of_cell, kFindAnotherBeginningVertex, lane);
+      return ahead ? kDeferred : kFindAnotherBeginningVertex;
+    }
     in_domain = f;
     pt0[0] = __shfl_sync(kFull, px, 0) * double(g.voxel) - s.x;
     pt0[1] = __shfl_sync(kFull, py, 0) * double(g.voxel) - s.y;
@@ -1810,22 +1870,34 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   bool inner = false;
   if (nuniq > 0 && a.inner_apex) {
     double ap[3];
-    const int f = inner_apex(w, g, s, vmin, vmax, w.tlist, nuniq, ap, lane);
+    const int f = inner_apex(w, g, s, vmin, vmax, tl, nuniq, ap, lane);
     if (f >= 0) {
       inner = true;
       in_domain = f;
       for (int d = 0; d < 3; ++d) pt0[d] = ap[d];
-      const int kept = drop_separated(w, g, s, w.tlist, nuniq, lane);
+      const int kept = drop_separated(w, g, s, tl, nuniq, lane);
       count(ctr, kCtrConesSkipped, nuniq - kept, lane);
       nuniq = kept;
     }
   }
   trace_rec(tr, trcap, lane, 5, pt0[0], pt0[1], pt0[2], in_domain, nuniq);
   if (in_domain == 2) integrate<VS, INL>(w, 1.0, acc, lane, ctr, tr, trcap);
-  if (nuniq == 0) return kSuccess;
+  if (nuniq == 0 && !ahead) return kSuccess;
   if (lane < 3) w.pts[lane] = pt0[lane];
   __syncwarp();
-  const DeferQueue &dq = a.defer;
+  if (ahead) {
+    // its slot is taken: parked even without triangles.  Without an inner
+    // apex the cones clip the cell, which depends on the retry pass's P and
+    // V: the retries take it, as a triangle overflow now
+    if (!inner) {
+      park_fixed(dq, slot, a.diag, sid_of_cell, kTriangleOverflow, lane);
+    } else {
+      park_cell(w, dq, slot, L, a.diag, sid_of_cell, nuniq, inner, acc, lane, true);
+      // the retry passes' T schedule follows the counts settled ahead
+      if (lane == 0) atomicMax(&dq.counters[3], ntr);
+    }
+    return kDeferred;
+  }
   if (dq.slots && (!INL || nuniq > dq.inline_max)) {
     // park the cell: its triangles become work items of k_cone
     int slot = 0;
@@ -2296,17 +2368,16 @@ template <int VS, class Desc>
 __device__ __forceinline__ void cone_items(const DeferQueue &dq, const Layout &L, Desc desc, unsigned char *wsmem,
                                            int lane) {
   WarpCell w = bind(wsmem, L);
-  const int parked = min(*(volatile int *)&dq.counters[0], dq.capacity);
-  const int items = parked * dq.max_chunks;
+  const int items = min(*(volatile int *)&dq.counters[2], dq.capacity * dq.max_chunks);
   for (;;) {
     int item = 0;
     if (lane == 0) item = atomicAdd(&dq.counters[1], 1);
     item = __shfl_sync(kFull, item, 0);
     if (item >= items) break;
-    const int slot = item / dq.max_chunks, chunk = item % dq.max_chunks;
+    const int slot = dq.chunk_slot[item];
     const unsigned char *base = dq.slots + size_t(slot) * dq.slot_bytes;
     const DeferHeader *h = reinterpret_cast<const DeferHeader *>(base);
-    const int nuniq = h->nuniq;
+    const int nuniq = h->nuniq, chunk = item - h->chunk_base;
     const int t0 = chunk * dq.chunk;
     if (t0 >= nuniq) continue;
     const int t1 = min(t0 + dq.chunk, nuniq);
@@ -2385,9 +2456,9 @@ __device__ __forceinline__ void finish_slot(const DeferQueue &dq, const Layout &
   const CellLaunch &a = desc(h->diag);
   const int sid = h->sid, nch = (h->nuniq + dq.chunk - 1) / dq.chunk;
   double acc[4] = {h->acc[0], h->acc[1], h->acc[2], h->acc[3]};
-  int status = kSuccess;
+  int status = h->fixed >= 0 ? h->fixed : kSuccess;
   for (int c = 0; c < nch; ++c) {
-    const int item = slot * dq.max_chunks + c;
+    const int item = h->chunk_base + c;
     const int f = dq.fail[item];
     if (f != 0x7fffffff) {
       status = f & 15;
@@ -2602,8 +2673,10 @@ cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count, int 
   if (a.num <= 0) return cudaSuccess;
   if (a.P > kMaxP || a.V > kMaxV || a.T > kMaxT || a.P < 7 || a.V < 8) return cudaErrorInvalidValue;
   if (a.hess && (a.defer.slots || a.H < 1 || (a.HC != 1 && a.HC != 4))) return cudaErrorInvalidValue;
-  const Layout L = make_layout(a.P, a.V, a.T, a.grid.size > 0, a.hess ? a.HC : 0);
-  if (a.defer.slots && a.defer.slot_bytes < slot_bytes_for(L, a.T)) return cudaErrorInvalidValue;
+  if (a.T_ahead > kMaxT || (a.T_ahead > a.T && (!a.defer.slots || a.hess))) return cudaErrorInvalidValue;
+  const Layout L = make_layout(a.P, a.V, a.T, a.grid.size > 0, a.hess ? a.HC : 0, a.T_ahead);
+  if (a.defer.slots && (a.defer.slot_bytes < slot_bytes_for(L, L.T) || a.defer.max_chunks * a.defer.chunk < L.T))
+    return cudaErrorInvalidValue;
   const int vs = L.Vc / 32;
   if (vs <= 2) return launch_vs<2>(a, L, st, sm_count, launches);
   if (vs <= 3) return launch_vs<3>(a, L, st, sm_count, launches);

@@ -47,8 +47,13 @@ struct DeferQueue {
   unsigned char *slots = nullptr;  // capacity slots of slot_bytes
   int capacity = 0;
   size_t slot_bytes = 0;
-  int *counters = nullptr;         // [0] cells parked, [1] next work item (zeroed before a pass)
-  double *part = nullptr;          // capacity * max_chunks * 4 partial moments
+  // [0] cells parked, [1] next work item, [2] chunks taken, [3] the largest
+  // triangle count parked ahead (CellLaunch::T_ahead); zeroed before a pass
+  int *counters = nullptr;
+  // Work items are chunks, numbered compactly: a parked cell takes its
+  // chunks' range from counters[2] and writes its slot for each of them
+  int *chunk_slot = nullptr;       // capacity * max_chunks
+  double *part = nullptr;          // capacity * max_chunks * 4 partial moments, by work item
   int *fail = nullptr;             // capacity * max_chunks: (triangle << 4) | status, or INT_MAX
   int max_chunks = 0;              // ceil(T / chunk)
   int chunk = 32;                  // triangles per work item
@@ -63,6 +68,12 @@ struct CellLaunch {
   const int *ids = nullptr;        // stored ids of the rows (null: row i = seed i)
   int num = 0;
   int P = 0, V = 0, T = 0;         // caps of this pass
+  // first pass: a cell whose clip succeeded and whose range holds more than T
+  // but at most T_ahead triangles (with disjoint lists, counted by grid.tsat)
+  // is parked now with all of them -- the result the retry passes would give
+  // it -- its start corner found as they would (out_domain_ahead); 0: off
+  int T_ahead = 0;
+  int out_domain_ahead = 0;
   float cube_eps = 0.f;            // box [-eps, 1000+eps]^3
   int out_domain = 0;              // GRID_OUT_DOMAIN fallback for the start corner
   int early_out = 1;               // stop clipping cells proven outside the domain (needs grid.sat)
@@ -98,6 +109,7 @@ struct CellLaunch {
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
 constexpr int kProbeMiss = 102;     // internal status: the outside probe proved nothing
+constexpr int kDeferCounters = 4;   // ints of DeferQueue::counters
 constexpr int kTraceRecord = 12;
 
 // Largest caps of one build: P <= 255 (uchar plane ids in the reference,

@@ -370,7 +370,7 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
 static_assert(int(RPD_CTR_NUM) == int(kCtrNum), "counter enums out of sync");
 
 int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T, float eps, int out_domain,
-             bool counters, bool early_out, int border_d = 0) {
+             bool counters, bool early_out, int border_d = 0, int T_ahead = 0, int out_domain_ahead = 0) {
   rpd_context *ctx = s->ctx;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
@@ -434,17 +434,22 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
     // boundary cells with many triangles are parked and their triangles
     // spread over all warps; cells past the capacity stay inline
     DeferQueue &dq = a.defer;
+    const int t_slot = std::max(T, T_ahead);
     dq.capacity = std::min(num, std::max(32768, s->n / 8));
-    dq.slot_bytes = defer_slot_bytes(P, V, T);
+    dq.slot_bytes = defer_slot_bytes(P, V, t_slot);
     dq.chunk = 32;  // a warp's lanes take one triangle each
     dq.inline_max = 16;
-    dq.max_chunks = std::max(1, (T + dq.chunk - 1) / dq.chunk);
+    dq.max_chunks = std::max(1, (t_slot + dq.chunk - 1) / dq.chunk);
+    a.T_ahead = T_ahead > T ? T_ahead : 0;
+    a.out_domain_ahead = out_domain_ahead;
     const size_t items = size_t(dq.capacity) * dq.max_chunks;
     if ((e = s->defer_slots.ensure(dq.slot_bytes * dq.capacity)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
     if ((e = s->defer_part.ensure(sizeof(double) * 4 * items)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
     if ((e = s->defer_fail.ensure(sizeof(int) * items)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
-    if ((e = s->defer_ctr.ensure(sizeof(int) * 2)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
-    cudaMemsetAsync(s->defer_ctr.ptr, 0, sizeof(int) * 2, st);
+    if ((e = s->defer_chunk_slot.ensure(sizeof(int) * items)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
+    if ((e = s->defer_ctr.ensure(sizeof(int) * kDeferCounters)) != cudaSuccess) return map_cuda(ctx, e, "alloc defer");
+    cudaMemsetAsync(s->defer_ctr.ptr, 0, sizeof(int) * kDeferCounters, st);
+    dq.chunk_slot = s->defer_chunk_slot.as<int>();
     dq.slots = s->defer_slots.as<unsigned char>();
     dq.part = s->defer_part.as<double>();
     dq.fail = s->defer_fail.as<int>();
@@ -454,12 +459,15 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   if ((e = cell_launch(a, st, ctx->sm_count, &launches)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
   if (a.defer.slots) {
     // cells that found the queue full run again with their cones inline
-    int parked = 0;
-    cudaMemcpyAsync(&parked, a.defer.counters, sizeof(int), cudaMemcpyDeviceToHost, st);
+    int ctrs[kDeferCounters] = {};
+    cudaMemcpyAsync(ctrs, a.defer.counters, sizeof(ctrs), cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
+    const int parked = ctrs[0];
+    if (a.T_ahead > 0) s->ahead_max = ctrs[3];
     if (parked > a.defer.capacity) {
       CellLaunch b = a;
       b.defer = DeferQueue();
+      b.T_ahead = 0;
       b.only_status = kParkOverflow;
       b.after_cell = nullptr;
       if ((e = cell_launch(b, st, ctx->sm_count, &launches)) != cudaSuccess) return map_cuda(ctx, e, "cell kernel");
@@ -891,15 +899,37 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   const bool probe = grid && early && s->grid.sat && !counters && s->hess_h == 0 &&
                      !(s->used_on && s->keep_volume <= 0.0) && !table_kept &&
                      (s->launches_since_points == 0 || s->fresh_knn) && !(p.flags & RPD_FLAG_NO_PROBE);
+  // triangle overflows settled ahead: a cell that clips in the first pass
+  // and holds more than T triangles is clipped to the same cell by every
+  // retry pass, which restricts it once T has grown past its count.  The
+  // retries certainly run while this cell fails, up to max_extra_passes,
+  // unless P or K outgrow their limits; assuming both grow in every pass,
+  // the first pass parks such cells up to the T of the last retry that
+  // surely runs, and restricts them as a retry would
+  const int out_domain = p.out_domain >= 0 ? p.out_domain : (grid && s->grid.has_border_corners ? 1 : 0);
+  int T_ahead = 0;
+  s->ahead_max = 0;
+  if (grid && s->grid.tsat && s->use_defer && s->inner_apex && s->hess_h == 0 && !counters &&
+      !(p.flags & (RPD_FLAG_FIRST_PASS_ONLY | RPD_FLAG_NO_T_AHEAD))) {
+    int Pj = p.P, Kj = p.K, Tj = p.T;
+    for (int j = 0; j < p.max_extra_passes; ++j) {
+      const int Pn = int(Pj * 1.5), Kn = int(Kj * 1.5);
+      if (Pn > kMaxP || knn_slots(Kn) < 0) break;
+      Pj = Pn;
+      Kj = Kn;
+      Tj = std::min(int(Tj * 1.5), kMaxT);
+      T_ahead = Tj;
+    }
+  }
   int rc;
   if (probe) {
     int nmiss = 0;
     int *miss = s->ids_b.as<int>();
     if ((rc = run_probe(s, p.P, p.V, eps, miss, nmiss)) != RPD_OK) return rc;
-    rc = run_pass(s, miss, nmiss, p.K, p.P, p.V, T0, eps, 0, counters, early);
+    rc = run_pass(s, miss, nmiss, p.K, p.P, p.V, T0, eps, 0, counters, early, 0, T_ahead, out_domain);
     s->stats.pass_cells[0] = n;  // the reference's first pass: every seed
   } else {
-    rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early);
+    rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early, 0, T_ahead, out_domain);
   }
   if (rc != RPD_OK) return rc;
   int K = p.K, P = p.P, V = p.V, T = p.T;
@@ -909,13 +939,14 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
     int *A = s->ids_a.as<int>(), *B = s->ids_b.as<int>(), *Cc = s->ids_c.as<int>();
     // extra passes (voronoi.cpp:1311-1376): caps grow x1.5 by failing status
     if ((rc = recompute_ids(s, nullptr, n, 0, A, Cc, n0, n1, hist)) != RPD_OK) return rc;
-    const int out_domain = p.out_domain >= 0 ? p.out_domain : (grid && s->grid.has_border_corners ? 1 : 0);
     for (int step = 0; step < p.max_extra_passes && n0 > 0; ++step) {
       bool relaunch = false;
       if (hist[kVertexOverflow]) { relaunch = true; V = int(V * 1.5); }
       if (hist[kPlaneOverflow]) { relaunch = true; P = int(P * 1.5); }
       if (hist[kSecurityRadiusNotReached]) { relaunch = true; K = int(K * 1.5); }
-      if (hist[kTriangleOverflow]) { relaunch = true; T = int(T * 1.5); }
+      // cells parked ahead still fail in the reference's passes while T is
+      // below their count, and keep T growing
+      if (hist[kTriangleOverflow] || T < s->ahead_max) { relaunch = true; T = int(T * 1.5); }
       if (!relaunch) break;
       if (P > kMaxP || knn_slots(K) < 0) break;  // the reference stops at P >= 256 (voronoi.cpp:867)
       V = std::min(V, kMaxV);
@@ -1166,6 +1197,7 @@ void solver_trim(rpd_solver *s) {
   s->defer_part.release();
   s->defer_fail.release();
   s->defer_ctr.release();
+  s->defer_chunk_slot.release();
 }
 
 size_t solver_device_bytes(const rpd_solver *s) {
@@ -1173,7 +1205,7 @@ size_t solver_device_bytes(const rpd_solver *s) {
                        &s->ring_bound, &s->knn, &s->knn_part, &s->knn_user, &s->counter64, &s->g_flags, &s->g_points,
                        &s->g_tris, &s->g_list, &s->g_offsets, &s->g_sat, &s->g_tsat, &s->out, &s->status, &s->ids_a, &s->ids_b,
                        &s->ids_c, &s->fail_ws, &s->hist, &s->gather, &s->defer_slots, &s->defer_part, &s->defer_fail,
-                       &s->defer_ctr};
+                       &s->defer_ctr, &s->defer_chunk_slot, &s->wmin, &s->used, &s->hess, &s->hessid};
   size_t t = 0;
   for (const DevBuf *x : b) t += x->bytes;
   return t;

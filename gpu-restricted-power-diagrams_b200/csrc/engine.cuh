@@ -91,7 +91,8 @@ struct rpd_solver {
   rpd::DevBuf fail_ws;         // flags + scans
   rpd::DevBuf hist;            // int[16]: status histogram + counts
   rpd::DevBuf gather;          // user-order staging for outputs
-  rpd::DevBuf defer_slots, defer_part, defer_fail, defer_ctr;  // parked boundary cells
+  rpd::DevBuf defer_slots, defer_part, defer_fail, defer_ctr, defer_chunk_slot;  // parked boundary cells
+  int ahead_max = 0;           // the largest triangle count the first pass parked ahead
   bool have_results = false;
   bool use_defer = true;       // park heavy boundary cells for the chunked kernel
   bool inner_apex = true;      // cone apex at a grid corner inside the cell

@@ -126,6 +126,7 @@ FLAG_NO_DEFER = 8
 FLAG_REFERENCE_APEX = 16
 FLAG_FRESH_NEIGHBOURS = 32
 FLAG_NO_PROBE = 64
+FLAG_NO_T_AHEAD = 128
 COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
                  "exports", "export_vertices", "outside_early", "cone_empty", "cones_skipped"]
 

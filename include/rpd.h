@@ -181,6 +181,10 @@ rpd_grid *rpd_solver_export_grid(rpd_solver *s, int *err);
 #define RPD_FLAG_NO_PROBE 64u       /* no outside probe before the first pass: every
                                        seed gets its full K-nearest search (same
                                        results) */
+#define RPD_FLAG_NO_T_AHEAD 128u    /* leave every triangle overflow of the first pass
+                                       to the retry passes instead of restricting at
+                                       once the cells the retries would settle (same
+                                       results) */
 
 /* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
 typedef struct rpd_params {

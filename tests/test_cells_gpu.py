@@ -170,6 +170,28 @@ def test_outside_probe_does_not_change_results(rpd):
     assert_parity(met)
 
 
+@pytest.mark.parametrize("T", [20, 40])
+def test_triangle_overflows_settled_ahead(rpd, T):
+    """Small T: the first pass parks the cells that only overflow T and
+    restricts them at once, as the retry passes would; the results are those
+    of the retry passes (bit for bit) and of the oracle, with far fewer cells
+    retried."""
+    g = rpd.Grid.blob(40, 5, 2)
+    x = jittered(30, seed=5, weights=True)
+    s = rpd.Solver().set_points(x).set_grid(g)
+    s.launch(K=50, P=30, V=40, T=T, flags=rpd.FLAG_FRESH_NEIGHBOURS)
+    m1, s1, st1 = s.moments(), s.status(), s.stats()
+    s.launch(K=50, P=30, V=40, T=T, flags=rpd.FLAG_FRESH_NEIGHBOURS | rpd.FLAG_NO_T_AHEAD)
+    m0, s0, st0 = s.moments(), s.status(), s.stats()
+    print("passes ahead", [p["cells"] for p in st1["passes"]], "retries", [p["cells"] for p in st0["passes"]])
+    retried = lambda st: sum(p["cells"] for p in st["passes"][1:])  # noqa: E731
+    assert st0["npasses"] >= 3 and retried(st1) < retried(st0) / 2
+    assert np.array_equal(s1, s0)
+    assert np.array_equal(m1, m0)
+    met, *_ = run_case(rpd, x, grid=g, K=50, P=30, V=40, T=T)
+    assert_parity(met)
+
+
 def test_empty_cells_outside_the_domain(rpd):
     """Seeds far outside the domain whose weight empties their power cell
     keep the status empty_cell: the early exits outside the domain (the cell
