@@ -741,6 +741,7 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
   rpd_context *ctx = s->ctx;
   cudaSetDevice(ctx->device);
   s->grid = DevGrid();
+  s->grid_nonplain = -1;
   if (!gh) return RPD_OK;
   const HostGrid *g = host_grid(gh);
   const size_t nv = size_t(g->size) * g->size * g->size;
@@ -824,6 +825,7 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
       break;
     }
   s->grid = d;
+  s->grid_nonplain = -1;
   return RPD_OK;
 }
 
@@ -896,9 +898,22 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   // fresh neighbours); later launches build the whole neighbour table once,
   // which weight-only re-solves then keep.
   const bool table_kept = s->knn_full_K == p.K && !s->fresh_knn;
-  const bool probe = grid && early && s->grid.sat && !counters && s->hess_h == 0 &&
-                     !(s->used_on && s->keep_volume <= 0.0) && !table_kept &&
-                     (s->launches_since_points == 0 || s->fresh_knn) && !(p.flags & RPD_FLAG_NO_PROBE);
+  bool probe = grid && early && s->grid.sat && !counters && s->hess_h == 0 &&
+               !(s->used_on && s->keep_volume <= 0.0) && !table_kept &&
+               (s->launches_since_points == 0 || s->fresh_knn) && !(p.flags & RPD_FLAG_NO_PROBE);
+  if (probe) {
+    // a domain that fills (nearly) the whole box leaves nothing to prove
+    const long long S = s->grid.size, S1 = S + 1;
+    if (s->grid_nonplain < 0) {
+      int v = 0;
+      if ((e = cudaMemcpyAsync(&v, s->grid.sat + (S1 * S1 * S1 - 1), sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+              cudaSuccess ||
+          (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return map_cuda(ctx, e, "read grid table");
+      s->grid_nonplain = v;
+    }
+    probe = s->grid_nonplain < 0.95 * double(S * S * S);
+  }
   // triangle overflows settled ahead: a cell that clips in the first pass
   // and holds more than T triangles is clipped to the same cell by every
   // retry pass, which restricts it once T has grown past its count.  The
@@ -1176,6 +1191,7 @@ void solver_share_grid(rpd_solver *dst, const rpd_solver *src) {
   dst->g_sat.release();
   dst->g_tsat.release();
   dst->grid = src->grid;
+  dst->grid_nonplain = src->grid_nonplain;
   dst->grid_points = src->grid_points;
   dst->grid_triangles = src->grid_triangles;
 }

@@ -77,6 +77,7 @@ struct rpd_solver {
   rpd::DevBuf knn;             // unsigned[n*K]: every cell's neighbours (stored ids)
   int knn_full_K = 0;          // K of the table in knn for all n cells (0: none)
   int launches_since_points = 0;  // launches since the seeds were set (the outside probe runs on the first)
+  long long grid_nonplain = -1;   // voxels of the grid that are not plainly outside (-1: not read yet)
   rpd::DevBuf knn_part;        // unsigned[num*K]: rows of a retry pass or a trace
   rpd::DevBuf knn_user;        // int[n*K]
   rpd::DevBuf counter64;       // unsigned long long[RPD_CTR_NUM + 1]

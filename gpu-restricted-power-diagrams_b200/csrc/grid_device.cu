@@ -377,6 +377,7 @@ int build_from_field(rpd_solver *s, int S, DevBuf &f) {
   d.lists_disjoint = 1;       // every triangle is listed in its own voxel
   d.has_border_corners = 0;   // corner flags are 0 or 2
   s->grid = d;
+  s->grid_nonplain = -1;
   s->grid_points = npts;
   s->grid_triangles = ntri;
   return RPD_OK;
@@ -399,6 +400,7 @@ int rpd_solver_set_grid_field(rpd_solver *s, int size, const float *field, rpd_m
   cudaStream_t st = ctx->stream;
   cudaError_t e;
   s->grid = DevGrid();
+  s->grid_nonplain = -1;
   const long nl = long(size + 1) * (size + 1) * (size + 1);
   DevBuf f;
   SyncOnExit guard{st};
@@ -417,6 +419,7 @@ int rpd_solver_set_grid_blob(rpd_solver *s, int size, int nellipsoids, uint64_t 
   cudaStream_t st = ctx->stream;
   cudaError_t e;
   s->grid = DevGrid();
+  s->grid_nonplain = -1;
   std::vector<double> c, a, R;
   random_blob_params(nellipsoids, seed, c, a, R);
   std::vector<double> params(c);
