@@ -42,6 +42,7 @@ struct DiagStatic {
   int out_domain;  // start-corner fallback of the retry passes
   int early_out, inner_apex;
   const int *wmin;  // the smallest weight of the seeds that are not walls (float_to_ordered)
+  int T_ahead;      // first pass: triangle overflows up to this count parked at once (0: off)
   float cube_eps;
   DevGrid grid;
   int *status;
@@ -62,6 +63,7 @@ struct DiagState {
   const int *rc_ids;  // rows of the recompute (null: every cell)
   int rc_cond;        // 1: empty cells are not re-solved
   int hist[16];       // status histogram of the failing cells of the last recompute
+  int ahead_max;      // the largest triangle count the first pass parked ahead
   int final_hist[16]; // status histogram of every cell at the end
   int pass_cells[kPassRecord], pass_K[kPassRecord], pass_P[kPassRecord], pass_V[kPassRecord], pass_T[kPassRecord];
 };
@@ -136,6 +138,7 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
       s.rc_ids = nullptr;
       s.rc_cond = 0;
       s.rc_num = g.n;
+      s.ahead_max = 0;
       continue;
     }
     if (!s.active) continue;
@@ -146,7 +149,9 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
       if (s.hist[kVertexOverflow]) { relaunch = true; V = int(V * 1.5); }
       if (s.hist[kPlaneOverflow]) { relaunch = true; P = int(P * 1.5); }
       if (s.hist[kSecurityRadiusNotReached]) { relaunch = true; K = int(K * 1.5); }
-      if (s.hist[kTriangleOverflow]) { relaunch = true; T = int(T * 1.5); }
+      // cells parked ahead still fail in the reference's passes while T is
+      // below their count, and keep T growing
+      if (s.hist[kTriangleOverflow] || T < s.ahead_max) { relaunch = true; T = int(T * 1.5); }
       if (!relaunch || P > kMaxP || K > kMaxK) {
         go = false;  // the reference stops at P >= 256 (voronoi.cpp:867)
       } else {
@@ -258,6 +263,11 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     a.T = s.T;
     a.cube_eps = g.cube_eps;
     a.out_domain = pa.pass == 0 ? 0 : g.out_domain;
+    if (pa.pass == 0 && pa.defer.slots) {
+      a.T_ahead = g.T_ahead;
+      a.out_domain_ahead = g.out_domain;
+      a.ahead_max = &s.ahead_max;
+    }
     a.early_out = g.early_out;
     a.wmin = g.wmin;
     a.inner_apex = g.inner_apex;
@@ -268,6 +278,7 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     a.defer = pa.defer;
     pl.descs[d] = a;
     a.defer = DeferQueue();
+    a.T_ahead = 0;
     pl.descs_inline[d] = a;
   }
 }
@@ -442,6 +453,12 @@ int describe(rpd_batch *b, std::vector<DiagStatic> &out) {
     g.out_domain = p.out_domain >= 0 ? p.out_domain : (grid && s->grid.has_border_corners ? 1 : 0);
     g.early_out = (p.flags & RPD_FLAG_NO_EARLY_OUT) ? 0 : 1;
     g.wmin = s->wmin.as<int>();
+    // triangle overflows parked ahead, as rpd_solver_launch does
+    g.T_ahead = grid && s->grid.tsat && !(p.flags & (RPD_FLAG_NO_DEFER | RPD_FLAG_REFERENCE_APEX |
+                                                     RPD_FLAG_FIRST_PASS_ONLY | RPD_FLAG_NO_T_AHEAD))
+                    ? t_ahead_cap(p.P, p.K, p.T, std::max(0, p.max_extra_passes))
+                    : 0;
+    if (g.T_ahead <= p.T) g.T_ahead = 0;
     g.inner_apex = (p.flags & RPD_FLAG_REFERENCE_APEX) ? 0 : 1;
     g.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
     g.grid = s->grid;
@@ -541,8 +558,11 @@ int capture(rpd_batch *b) {
   // first pass; later passes (larger slots) hold fewer cells
   const int chunk = 32;  // the cone kernels' chunk (a warp's lanes take one triangle each)
   const int cap0 = int(std::min<long long>(cells, std::max<long long>(32768, cells / 8)));
-  const size_t slot0 = defer_slot_bytes(Pb[0], Vb[0], Tb[0]);
-  const size_t items0 = size_t(cap0) * std::max(1, (Tb[0] + chunk - 1) / chunk);
+  // the first pass's slots hold the triangle overflows parked ahead
+  int Tslot0 = Tb[0];
+  for (int d = 0; d < nd; ++d) Tslot0 = std::max(Tslot0, G[d].T_ahead);
+  const size_t slot0 = defer_slot_bytes(Pb[0], Vb[0], Tslot0);
+  const size_t items0 = size_t(cap0) * std::max(1, (Tslot0 + chunk - 1) / chunk);
   if (any_grid && defer) {
     if ((e = b->defer_slots.ensure(slot0 * cap0)) != cudaSuccess ||
         (e = b->defer_part.ensure(sizeof(double) * 4 * items0)) != cudaSuccess ||
@@ -605,10 +625,11 @@ int capture(rpd_batch *b) {
     pa.Kb = Kb[j];
     DeferQueue dq;
     if (any_grid && defer) {
-      dq.slot_bytes = defer_slot_bytes(Pb[j], Vb[j], Tb[j]);
+      const int Ts = j == 0 ? Tslot0 : Tb[j];
+      dq.slot_bytes = defer_slot_bytes(Pb[j], Vb[j], Ts);
       dq.chunk = chunk;
       dq.inline_max = 16;
-      dq.max_chunks = std::max(1, (Tb[j] + chunk - 1) / chunk);
+      dq.max_chunks = std::max(1, (Ts + chunk - 1) / chunk);
       const size_t by_slots = (slot0 * cap0) / dq.slot_bytes, by_items = items0 / dq.max_chunks;
       dq.capacity = int(std::min<size_t>({size_t(cap0), by_slots, by_items}));
       dq.slots = b->defer_slots.as<unsigned char>();
@@ -646,6 +667,7 @@ int capture(rpd_batch *b) {
     cb.P = Pb[j];
     cb.V = Vb[j];
     cb.T = Tb[j];
+    cb.T_slot = j == 0 && dq.slots ? Tslot0 : 0;
     cb.after_cell = j == 0 ? b->ev[2] : nullptr;
     // the first pass's rows are every cell: one warp per row; the retries'
     // rows are known on the device only: persistent, rows from a counter

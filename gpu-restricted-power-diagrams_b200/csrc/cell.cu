@@ -1894,7 +1894,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     } else {
       park_cell(w, dq, slot, L, a.diag, sid_of_cell, nuniq, inner, acc, lane, true);
       // the retry passes' T schedule follows the counts settled ahead
-      if (lane == 0) atomicMax(&dq.counters[3], ntr);
+      if (lane == 0) atomicMax(a.ahead_max ? a.ahead_max : &dq.counters[3], ntr);
     }
     return kDeferred;
   }
@@ -2657,8 +2657,9 @@ bool cell_caps_fit(int P, int V, int T, bool grid) { return warps_per_block_for(
 cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches) {
   if (b.ndiag <= 0) return cudaSuccess;
   if (b.P > kMaxP || b.V > kMaxV || b.T > kMaxT || b.P < 7 || b.V < 8) return cudaErrorInvalidValue;
-  const Layout Lg = make_layout(b.P, b.V, b.T, true), Lp = make_layout(b.P, b.V, b.T, false);
-  if (b.defer.slots && b.defer.slot_bytes < slot_bytes_for(Lg, b.T)) return cudaErrorInvalidValue;
+  const Layout Lg = make_layout(b.P, b.V, b.T, true, 0, b.T_slot), Lp = make_layout(b.P, b.V, b.T, false);
+  if (b.defer.slots && (b.defer.slot_bytes < slot_bytes_for(Lg, Lg.T) || b.defer.max_chunks * b.defer.chunk < Lg.T))
+    return cudaErrorInvalidValue;
   const int vs = Lg.Vc / 32;
   if (vs <= 2) return launch_batch_vs<2>(b, Lg, Lp, st, sm_count, launches);
   if (vs <= 3) return launch_batch_vs<3>(b, Lg, Lp, st, sm_count, launches);

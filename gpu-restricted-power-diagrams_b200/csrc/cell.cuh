@@ -74,6 +74,7 @@ struct CellLaunch {
   // it -- its start corner found as they would (out_domain_ahead); 0: off
   int T_ahead = 0;
   int out_domain_ahead = 0;
+  int *ahead_max = nullptr;  // the largest count parked ahead (atomicMax; null: defer.counters[3])
   float cube_eps = 0.f;            // box [-eps, 1000+eps]^3
   int out_domain = 0;              // GRID_OUT_DOMAIN fallback for the start corner
   int early_out = 1;               // stop clipping cells proven outside the domain (needs grid.sat)
@@ -166,6 +167,7 @@ struct CellBatch {
   int ndiag = 0;
   DeferQueue defer;                  // slots == null: every boundary cell inline
   int P = 0, V = 0, T = 0;           // layout caps: at least every diagram's caps of this pass
+  int T_slot = 0;                    // ids a parked cell's slot holds, when more than T (T_ahead)
   cudaEvent_t after_cell = nullptr;  // recorded (as a graph node when capturing) after the cell kernel
   // rows of the diagrams with / without a domain when known when the launch
   // is made (one warp per row), else -1 (persistent launches)

@@ -925,17 +925,8 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   int T_ahead = 0;
   s->ahead_max = 0;
   if (grid && s->grid.tsat && s->use_defer && s->inner_apex && s->hess_h == 0 && !counters &&
-      !(p.flags & (RPD_FLAG_FIRST_PASS_ONLY | RPD_FLAG_NO_T_AHEAD))) {
-    int Pj = p.P, Kj = p.K, Tj = p.T;
-    for (int j = 0; j < p.max_extra_passes; ++j) {
-      const int Pn = int(Pj * 1.5), Kn = int(Kj * 1.5);
-      if (Pn > kMaxP || knn_slots(Kn) < 0) break;
-      Pj = Pn;
-      Kj = Kn;
-      Tj = std::min(int(Tj * 1.5), kMaxT);
-      T_ahead = Tj;
-    }
-  }
+      !(p.flags & (RPD_FLAG_FIRST_PASS_ONLY | RPD_FLAG_NO_T_AHEAD)))
+    T_ahead = t_ahead_cap(p.P, p.K, p.T, p.max_extra_passes);
   int rc;
   if (probe) {
     int nmiss = 0;
@@ -1225,6 +1216,19 @@ size_t solver_device_bytes(const rpd_solver *s) {
   size_t t = 0;
   for (const DevBuf *x : b) t += x->bytes;
   return t;
+}
+
+int t_ahead_cap(int P, int K, int T, int max_extra) {
+  int T_ahead = 0;
+  for (int j = 0; j < max_extra; ++j) {
+    const int Pn = int(P * 1.5), Kn = int(K * 1.5);
+    if (Pn > kMaxP || knn_slots(Kn) < 0) break;
+    P = Pn;
+    K = Kn;
+    T = std::min(int(T * 1.5), kMaxT);
+    T_ahead = T;
+  }
+  return T_ahead;
 }
 
 }  // namespace rpd

@@ -117,4 +117,10 @@ void solver_rebind(rpd_solver *s, rpd_context *ctx);
 void solver_share_grid(rpd_solver *dst, const rpd_solver *src);
 size_t solver_device_bytes(const rpd_solver *s);
 void solver_trim(rpd_solver *s);
+// The T of the last retry pass that surely runs after a cell's triangle
+// overflow: passes grow T x1.5 while the cell fails, up to max_extra, and
+// stop once P or K (assumed to grow in every pass) outgrow their limits
+// (voronoi.cpp:867); 0 when no retry surely runs.
+int t_ahead_cap(int P, int K, int T, int max_extra);
+
 }  // namespace rpd

@@ -36,15 +36,15 @@ def build(rpd, sp, with_grid):
 
 
 def alone(rpd, x, g, p):
-    """The diagram solved on its own, without the outside probe and the
-    triangle overflows settled ahead (which batches do not do): its per-pass
-    cell counts are the batch's too (both settle in the first pass cells
-    that a retry pass would settle)."""
+    """The diagram solved on its own, without the outside probe (which
+    batches do not run): its per-pass cell counts are the batch's too (the
+    probe can settle in the first pass an empty cell outside the domain
+    that a full clip would retry).  Both settle triangle overflows ahead."""
     s = rpd.Solver().set_points(x)
     if g is not None:
         s.set_grid(g)
     q = rpd.Params.from_buffer_copy(p)
-    q.flags |= rpd.FLAG_NO_PROBE | rpd.FLAG_NO_T_AHEAD
+    q.flags |= rpd.FLAG_NO_PROBE
     s.launch(q)
     return s
 
