@@ -87,13 +87,15 @@ size_t resident_bytes(int n, const rpd_params &p) {
 
 // Device bytes a launch needs on top: binning workspace, failing-id lists,
 // staging, parked boundary cells, neighbour rows of retry passes (caps grown
-// x1.5 up to 5 times: bounded by 8x the first caps).
+// x1.5 up to 5 times: bounded by 8x the first caps, which also bounds the
+// first pass's slots for triangle overflows parked ahead).  Per work item of
+// the parked cells: partial moments, failure, owning slot (40 bytes).
 size_t transient_bytes(int n, const rpd_params &p) {
   const size_t cap = std::min<size_t>(size_t(n), std::max<size_t>(32768, size_t(n) / 8));
   const size_t P = size_t(std::min(255, p.P * 8)), V = size_t(std::min(256, p.V * 8)),
                T = size_t(std::min(4096, p.T * 8));
   const size_t slot = 144 + 32 * P + 44 * V + 4 * T;
-  return size_t(n) * (12 + 16 + 32 + 12) + cap * (slot / 4 + 36 * (T / 32 + 1) / 4) +
+  return size_t(n) * (12 + 16 + 32 + 12) + cap * (slot / 4 + 40 * (T / 32 + 1) / 4) +
          size_t(n) / 4 * size_t(p.K) * 8 * 4 + (size_t(1) << 20);
 }
 
