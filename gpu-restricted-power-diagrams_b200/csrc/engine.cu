@@ -116,6 +116,22 @@ __global__ void k_fail_scatter(const int *__restrict__ ids, int num, const int *
   if (f1[i]) out1[s1[i]] = sid;
 }
 
+// CUDA events of one call, destroyed on every return (a recorded event is
+// released once the device has passed it).
+template <int N>
+struct Events {
+  cudaEvent_t ev[N];
+  Events() {
+    for (auto &x : ev) cudaEventCreate(&x);
+  }
+  ~Events() {
+    for (auto &x : ev) cudaEventDestroy(x);
+  }
+  Events(const Events &) = delete;
+  Events &operator=(const Events &) = delete;
+  cudaEvent_t operator[](int i) const { return ev[i]; }
+};
+
 // Rows the outside probe left: f[i] = 1 where status is kProbeMiss; f[n] = 0.
 __global__ void k_probe_flags(const int *__restrict__ status, int n, int *__restrict__ f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -330,8 +346,7 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
   if ((e = s->fail_ws.ensure(sizeof(int) * (2 * size_t(n + 1) + nsc))) != cudaSuccess)
     return map_cuda(ctx, e, "alloc probe ws");
   int *f = s->fail_ws.as<int>(), *pos = f + (n + 1), *tiles = pos + (n + 1);
-  cudaEvent_t ev[2];
-  for (auto &x : ev) cudaEventCreate(&x);
+  Events<2> ev;
   cudaEventRecord(ev[0], st);
   ProbeLaunch pr;
   pr.stored = s->stored.as<float4>();
@@ -358,7 +373,6 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
   cudaMemcpyAsync(&cnt, pos + n, sizeof(int), cudaMemcpyDeviceToHost, st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "probe");
   cudaEventElapsedTime(&s->stats.probe_ms, ev[0], ev[1]);
-  for (auto &x : ev) cudaEventDestroy(x);
   s->stats.probe_outside = n - cnt;
   s->stats.kernel_launches += 6;  // probe, flags, scan (3), scatter
   nmiss = cnt;
@@ -382,8 +396,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   rpd::DevBuf &kb = all_cells ? s->knn : s->knn_part;
   const bool reuse = all_cells && s->knn_full_K == K && !counters && !s->fresh_knn;
   if ((e = kb.ensure(sizeof(unsigned) * size_t(num) * K)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
-  cudaEvent_t ev[4];
-  for (auto &x : ev) cudaEventCreate(&x);
+  Events<4> ev;
   unsigned long long *ctr = counters ? s->counter64.as<unsigned long long>() : nullptr;
   cudaEventRecord(ev[0], st);
   if (!reuse) {
@@ -486,7 +499,6 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
     cudaEventElapsedTime(&S.pass_cell_ms[pi], ev[1], ev[2]);
     if (num > 0) cudaEventElapsedTime(&S.pass_cell_kernel_ms[pi], ev[1], ev[3]);
   }
-  for (auto &x : ev) cudaEventDestroy(x);
   S.npasses++;
   S.kernel_launches += num > 0 ? 1 : 0;  // the cell kernel (the neighbour kernel counted above)
   return RPD_OK;
@@ -690,9 +702,7 @@ int rpd_solver_knn(rpd_solver *s, int K, int *knn_user, rpd_mem where, float *de
   cudaError_t e;
   if ((e = s->knn.ensure(sizeof(unsigned) * nk)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
   if ((e = s->knn_user.ensure(sizeof(int) * nk)) != cudaSuccess) return map_cuda(ctx, e, "alloc knn");
-  cudaEvent_t ev[2];
-  cudaEventCreate(&ev[0]);
-  cudaEventCreate(&ev[1]);
+  Events<2> ev;
   cudaEventRecord(ev[0], st);
   s->knn_full_K = 0;
   e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, nullptr, s->n, K, s->ring_bound.as<float>(),
@@ -711,8 +721,6 @@ int rpd_solver_knn(rpd_solver *s, int K, int *knn_user, rpd_mem where, float *de
   }
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "knn");
   if (device_ms) cudaEventElapsedTime(device_ms, ev[0], ev[1]);
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
   return RPD_OK;
 }
 
@@ -858,9 +866,8 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   s->have_results = false;
   const bool grid = s->grid.size > 0;
   const float eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
-  cudaEvent_t t0, t1;
-  cudaEventCreate(&t0);
-  cudaEventCreate(&t1);
+  Events<2> tt;
+  const cudaEvent_t t0 = tt[0], t1 = tt[1];
   cudaEventRecord(t0, st);
   // pass "first" + "tr_overflow" in one: T = caps.T from the start gives
   // every cell the result the two reference passes give it
@@ -984,8 +991,6 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   if (counters) cudaMemcpyAsync(c64, s->counter64.ptr, sizeof(c64), cudaMemcpyDeviceToHost, st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "launch");
   cudaEventElapsedTime(&s->stats.total_ms, t0, t1);
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
   for (int i = 0; i < kStatusNum; ++i) s->stats.status_hist[i] = hh[i];
   for (int i = 0; i < RPD_CTR_NUM; ++i) s->stats.counters[i] = c64[i];
   s->stats.knn_candidates = c64[RPD_CTR_NUM];
