@@ -47,3 +47,45 @@ def test_params_defaults_match_reference_options():
     p = rpd.Params.default()
     # Options.cpp:22-28 (K 20, P 25, T 100, V 30); voronoi.cpp:1321 (5 extra passes)
     assert (p.K, p.P, p.V, p.T, p.max_extra_passes) == (20, 25, 30, 100, 5)
+
+
+STRUCTS = {"Params": "rpd_params", "Stats": "rpd_stats", "RequestInfo": "rpd_request_info",
+           "MomentDiff": "rpd_moment_diff", "BatchStats": "rpd_batch_stats"}
+
+
+def test_python_structures_match_the_header(tmp_path):
+    """Every ctypes mirror of an rpd.h structure has the C layout: the same
+    size and the same offset for every field (a C program built against the
+    header prints them)."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    import rpd
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rpd.h"', "int main(void) {"]
+    for py, c in STRUCTS.items():
+        cls = getattr(rpd, py)
+        lines.append(f'  printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in cls._fields_:
+            lines.append(f'  printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    bad = []
+    for ln in out:
+        if not ln:
+            continue
+        py, name, val = ln.split()
+        cls = getattr(rpd, py)
+        got = C.sizeof(cls) if name == "size" else getattr(cls, name).offset
+        if got != int(val):
+            bad.append((py, name, got, int(val)))
+    assert not bad, bad
