@@ -28,3 +28,28 @@ def test_unit_cube_volume_fp64():
     b, s = oracle.solve(x, K=30, P=40, V=60, use_double=True)
     assert (s == oracle.SUCCESS).all()
     assert abs(b[:, 3].sum() - 1e9) < 1e-3
+
+
+@pytest.mark.skipif(not oracle.has_reference_kernels(), reason="reference kernels not built here")
+def test_restatement_bitexact_with_reference_kernels_empty_cells_in_a_domain():
+    """Seeds far outside a blob domain whose weight empties their power cell:
+    the restatement gives them the reference kernels' empty_cell status and
+    every other cell the same bits (the configuration of the device test of
+    the early exits outside the domain)."""
+    import rpd
+
+    g = rpd.Grid.blob(40, 5, 2)
+    a = g.arrays()
+    grid = oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+    x = jittered(24, seed=11, weights=True)
+    h2 = (1000.0 / 24) ** 2
+    corner = (x[:, :3] < 150).all(axis=1) | (x[:, :3] > 850).all(axis=1)
+    idx = np.where(corner)[0][::3]
+    x[idx, 3] = 4 * h2
+    x = x.astype(np.float64)
+    kw = dict(grid=grid, K=50, P=30, V=40, T=100, use_double=True)
+    b1, s1 = oracle.solve(x, kernels=1, **kw)
+    b0, s0 = oracle.solve(x, kernels=0, **kw)
+    assert np.array_equal(s0, s1)
+    assert np.array_equal(b0, b1)
+    assert (s0[idx] == 6).sum() > len(idx) // 2
