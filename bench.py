@@ -37,7 +37,7 @@ CONFIGS = {
     "voronoi-100k": dict(kind="uniform", n=100_000, weights=False, grid="blob", gsize=100, nell=5, gseed=2,
                          sseed=1, K=70, P=30, V=40, T=100,
                          desc="100K i.i.d. uniform seeds (weights 0), 5-ellipsoid blob at 100^3, K=70 P=30 V=40"),
-    # BASELINE config 3: blue noise at 5M seeds, unit cube domain
+    # blue noise at 5M seeds, unit cube domain
     "poisson-5m": dict(kind="poisson", n=5_000_000, rfac=0.7, weights=False, grid="cube", gsize=128, sseed=3,
                        K=20, P=25, V=30, T=100,
                        desc="5M seeds by seeded Poisson-disk dart throwing in [0,1]^3 (min distance 0.7 N^(-1/3)), "
@@ -50,7 +50,7 @@ CONFIGS = {
                            "in [1K, 200K], uniform or jittered-lattice seeds (alternating), weights U[0, 0.1h^2], "
                            "each with its own seeded 5-ellipsoid blob domain at 64^3..160^3 voxels, K drawn from "
                            "{20, 50, 70}, P=30 V=40 T=100; compared with the same 256 solved one after another"),
-    # BASELINE config 5: a serving loop (one GPU)
+    # a serving loop (one GPU)
     "serve-200rps": dict(kind="serve", rate=200.0, requests=600, nmin=10_000, nmax=2_000_000, reweight=0.3,
                          grid="blob", gsizes=(48, 64, 96, 128, 160, 200), nell=5, gseed=2, sseed=5, K=50, P=30, V=40,
                          T=100, slots=4, resident=24,

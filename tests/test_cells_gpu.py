@@ -210,7 +210,7 @@ def test_empty_cells_outside_the_domain(rpd):
 
 
 def test_blue_noise_cube_domain(rpd):
-    # BASELINE config 3 in small: Poisson-disk seeds, unit cube domain
+    # the 5M blue-noise workload in small: Poisson-disk seeds, unit cube domain
     from rpd import synth
 
     x = synth.poisson_disk(30_000, seed=3)
