@@ -783,7 +783,7 @@ def run_serve(args, cfg, rank):
     errs = max(clean) if clean else None
     rw = [d for d in ok if d[0] == "reweight"]
     line = {
-        "metric": "served cells/s and p50/p99 latency (config 5)", "value": cells / span, "unit": "cells/s",
+        "metric": "served cells/s and p50/p99 latency", "value": cells / span, "unit": "cells/s",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f64 geometry on f32 seeds", "data": "synthetic",
         "config": {"workload": "serve-200rps", "description": cfg["desc"], "slots": args.slots or cfg["slots"]},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
