@@ -89,3 +89,57 @@ def test_python_structures_match_the_header(tmp_path):
         if got != int(val):
             bad.append((py, name, got, int(val)))
     assert not bad, bad
+
+
+def test_cpp_facade_compiles_and_its_grid_runs_without_a_gpu(tmp_path):
+    """include/rpd.hpp, the C++ facade with the reference's class names, as a
+    user of the reference would call it: the whole header compiles and links
+    against librpd.so; the host-side Grid part runs without a GPU."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    pkg = os.path.join(ROOT, "gpu-restricted-power-diagrams_b200")
+    src = tmp_path / "facade.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include "rpd.hpp"
+
+// the reference's driver flow (test_voronoi.cpp): compiled, run only with a GPU
+static int solve(std::vector<float> const &xyzw, rpd::Grid const &grid) {
+  auto ctx = rpd::Context::create(0);
+  if (!ctx) return 1;
+  rpd::VoroAlgo algo(ctx);
+  algo.m_K = 50; algo.m_P = 30; algo.m_V = 40; algo.m_T = 100;
+  algo.setInputPoints(xyzw);
+  algo.setGrid(grid);
+  std::vector<double> bary;
+  std::vector<rpd::VoroAlgoStat> stats;
+  algo.launch([&](rpd::VoroAlgo const &a) { bary = a.getBarycenters(); return true; }, stats);
+  rpd::KNearests kn(ctx, xyzw);
+  double t = 0;
+  kn.buildKnearests(20, t);
+  return bary.empty() ? 1 : 0;
+}
+
+int main(int argc, char **argv) {
+  auto grid = rpd::Grid::blob(24, 3, 1);
+  if (!grid || !grid->valid()) return 2;
+  grid->printInvariants(std::cout);
+  std::printf("volume %.6f\n", grid->getVolume());
+  if (argc > 1 && std::strcmp(argv[1], "solve") == 0) return solve(std::vector<float>(4000, 1.f), *grid);
+  return 0;
+}
+''')
+    exe = tmp_path / "facade"
+    subprocess.run([cxx, "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", pkg, "-lrpd", f"-Wl,-rpath,{pkg}"], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    vol = float(out.split("volume")[-1])
+    assert 1e6 < vol < 1e9
