@@ -1,8 +1,9 @@
 // rpd_voronoi: command-line driver with the reference test_voronoi's options
 // (test_voronoi.cpp:65-223, Options.cpp:70-92) over librpd.
 //
-//   rpd_voronoi [--K=k] [--P=p] [--V=v] [--T=t] [--grid=FILE] [--output=xyz|mg|volume]
-//               [--points4D] [--keepVolume=v] [--printInvariants] [--checkGrid] [--debug] seeds.xyz
+//   rpd_voronoi [--K=k] [--P=p] [--V=v] [--T=t] [--grid=FILE] [--output=xyz|mg|volume|geogram]
+//               [--points4D] [--loadBinaryPoints] [--saveBinaryPoints=FILE] [--keepVolume=v]
+//               [--printInvariants] [--checkGrid] [--debug] seeds.xyz
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -17,37 +18,40 @@
 
 namespace {
 
-// Utils::loadSeedsFile (Utils.cpp:36-79) without normalisation: a count
-// line, then x y z [w] per line.
-bool load_seeds(const char *path, bool four_d, std::vector<float> &xyzw) {
-  std::ifstream in(path);
-  if (!in.is_open()) return false;
-  std::string line;
-  bool first = true;
-  int npts = 0;
-  while (std::getline(in, line)) {
-    if (line.empty()) continue;
-    std::istringstream iss(line);
-    if (first) {
-      iss >> npts;
-      xyzw.reserve(4 * size_t(std::max(npts, 0)));
-      first = false;
-      continue;
-    }
-    float x = 0, y = 0, z = 0, w = 0;
-    iss >> x >> y >> z;
-    if (four_d) iss >> w;
-    xyzw.insert(xyzw.end(), {x, y, z, w});
-  }
-  return int(xyzw.size() / 4) == npts;
+// Seeds through the library's loader: the reference's text format
+// (Utils::loadSeedsFile, Utils.cpp:36-79, not normalised) or, with
+// --loadBinaryPoints, its binary format (Utils.cpp:81-97).
+bool load_seeds(const char *path, bool four_d, bool binary, std::vector<float> &xyzw) {
+  float *p = nullptr;
+  int n = 0;
+  if (rpd_seeds_load(path, four_d ? 1 : 0, binary ? 1 : 0, &p, &n) != RPD_OK) return false;
+  xyzw.assign(p, p + 4 * size_t(n));
+  rpd_seeds_free(p);
+  return n > 0;
+}
+
+// --output=geogram (Utils::dropXYZGeogram, Utils.cpp:146-170, as
+// test_voronoi.cpp:162-167 calls it): every seed's barycentre as a vertex
+// and its mass as the attribute "w", in geogram's ASCII layout.
+void write_geogram(const char *path, const std::vector<double> &bary) {
+  const size_t n = bary.size() / 4;
+  std::ofstream f(path, std::ios::binary);
+  f << "[HEAD]\n\"GEOGRAM\"\n\"1.0\"\n[ATTS]\n\"GEO::Mesh::vertices\"\n" << n << "\n";
+  f << "[ATTR]\n\"GEO::Mesh::vertices\"\n\"point\"\n\"double\"\n8\n3\n";
+  for (size_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) f << bary[4 * i + d] / bary[4 * i + 3] << "\n";
+  f << "[ATTR]\n\"GEO::Mesh::vertices\"\n\"w\"\n\"double\"\n8\n1\n";
+  for (size_t i = 0; i < n; ++i) f << bary[4 * i + 3] << "\n";
 }
 
 void usage(const char *argv0) {
   std::cerr << "Usage: " << argv0 << " [options] points.xyz\n"
             << "\t--K=k --P=p --V=v --T=t: first-pass caps (default 20/25/30/100)\n"
             << "\t--grid=FILE: volume domain in the --grid text format\n"
-            << "\t--output=xyz|mg|volume (repeatable)\n"
+            << "\t--output=xyz|mg|volume|geogram (repeatable)\n"
             << "\t--points4D: the seed file has a weight column\n"
+            << "\t--loadBinaryPoints: the seed file is a 4D binary file\n"
+            << "\t--saveBinaryPoints=file: save the seeds in a 4D binary file\n"
             << "\t--keepVolume=v: cells with volume below v are empty (default 1)\n"
             << "\t--keepDist2=d: with --grid, keep the used cells and d rings around them (default 0; -1 all)\n"
             << "\t--hessian: compute the facet-area rows (--H=h facets per row, default 50; --HC=1|4)\n"
@@ -60,7 +64,8 @@ int main(int argc, char **argv) {
   int K = 20, P = 25, V = 30, T = 100;
   std::string grid_file, seeds_file;
   std::vector<std::string> outputs;
-  bool points4d = false, invariants = false, check_grid = false, debug = false;
+  bool points4d = false, invariants = false, check_grid = false, debug = false, load_binary = false;
+  std::string save_binary;
   double keep_volume = 1;
   int keep_dist2 = 0;  // test_voronoi's final keep distance (Options.cpp:42, test_voronoi.cpp:38)
   bool hessian = false;
@@ -88,6 +93,8 @@ int main(int argc, char **argv) {
     else if (a == "--keepDist2") keep_dist2 = std::atoi(need().c_str());
     else if (a == "--keepDist") (void)need();  // distance of the passes before the last: no effect here
     else if (a == "--points4D") points4d = true;
+    else if (a == "--loadBinaryPoints") load_binary = true;
+    else if (a == "--saveBinaryPoints") save_binary = need();
     else if (a == "--hessian") hessian = true;
     else if (a == "--H") H = std::atoi(need().c_str());
     else if (a == "--HC") HC = std::atoi(need().c_str());
@@ -103,10 +110,12 @@ int main(int argc, char **argv) {
     return 1;
   }
   std::vector<float> pts;
-  if (!load_seeds(seeds_file.c_str(), points4d, pts)) {
+  if (!load_seeds(seeds_file.c_str(), points4d, load_binary, pts)) {
     std::cerr << argv[0] << ": could not load file " << seeds_file << "\n";
     return 1;
   }
+  if (!save_binary.empty() && rpd_seeds_save_binary(save_binary.c_str(), pts.data(), int(pts.size() / 4)) != RPD_OK)
+    std::cerr << argv[0] << ": could not save " << save_binary << "\n";
   auto ctx = rpd::Context::create(0);
   if (!ctx) {
     std::cerr << argv[0] << ": no usable sm_100 device\n";
@@ -187,6 +196,8 @@ int main(int argc, char **argv) {
         if (bary[4 * i + 3] <= keep_volume) f << "0 0 0 0\n";
         else f << bary[4 * i] << " " << bary[4 * i + 1] << " " << bary[4 * i + 2] << " " << bary[4 * i + 3] << "\n";
       }
+    } else if (o == "geogram") {
+      write_geogram("gridGPU.geogram_ascii", bary);
     } else if (o == "volume") {
       double vol = 0;
       for (size_t i = 0; i < n; ++i)

@@ -7,9 +7,13 @@
 
 namespace rpd {
 
+// Also flags (nonfinite = 1) a seed with a NaN or infinite coordinate or
+// weight: the caller rejects the input, whose bins would be meaningless.
 __global__ void k_bin_count(const float4 *__restrict__ user, int n, int dim, int *__restrict__ seed_bin,
-                            int *__restrict__ counts) {
+                            int *__restrict__ counts, int *__restrict__ nonfinite) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool bad = i < n && !(isfinite(user[i].x) && isfinite(user[i].y) && isfinite(user[i].z) && isfinite(user[i].w));
+  if (bad) *nonfinite = 1;
   if (i >= n) return;
   const int b = bin_of(user[i], dim);
   seed_bin[i] = b;
@@ -161,16 +165,17 @@ cudaError_t bin_seeds(const float4 *user, int n, int dim, BinWorkspace ws, BinOu
   const int nb = dim * dim * dim;
   cudaError_t e;
   if ((e = cudaMemsetAsync(ws.counts, 0, sizeof(int) * size_t(nb + 1), st)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(ws.max_fill, 0, sizeof(int), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(ws.max_fill, 0, 2 * sizeof(int), st)) != cudaSuccess) return e;
   const int tb = 256;
-  k_bin_count<<<(n + tb - 1) / tb, tb, 0, st>>>(user, n, dim, ws.seed_bin, ws.counts);
+  k_bin_count<<<(n + tb - 1) / tb, tb, 0, st>>>(user, n, dim, ws.seed_bin, ws.counts, ws.max_fill + 1);
   k_max_reduce<<<148 * 4, 256, 0, st>>>(ws.counts, nb, ws.max_fill);
   if ((e = exclusive_scan(ws.counts, out.counters, nb + 1, ws.scan_tiles, st)) != cudaSuccess) return e;
   if (max_fill_host) {
-    if ((e = cudaMemcpyAsync(max_fill_host, ws.max_fill, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(max_fill_host, ws.max_fill, 2 * sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
       return e;
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    if (*max_fill_host > kMaxBinFill) return cudaSuccess;  // caller rejects the input
+    if (max_fill_host[0] > kMaxBinFill || max_fill_host[1]) return cudaSuccess;  // caller rejects the input
   }
   if ((e = cudaMemcpyAsync(ws.cursor, out.counters, sizeof(int) * size_t(nb), cudaMemcpyDeviceToDevice, st)) !=
       cudaSuccess)

@@ -34,7 +34,7 @@ struct BinWorkspace {
   int *counts;      // nb+1
   int *cursor;      // nb+1
   int *scan_tiles;  // scan_workspace_ints(nb+1)
-  int *max_fill;    // 1
+  int *max_fill;    // 2: the largest bin fill, then a non-finite-seed flag
   static size_t bytes(int n, int dim);
 };
 struct BinOutputs {
@@ -47,8 +47,9 @@ struct BinOutputs {
 size_t scan_workspace_ints(int n);
 cudaError_t exclusive_scan(const int *in, int *out, int n, int *tile_ws, cudaStream_t st);
 
-// Bins `user` (device, n seeds).  When max_fill_host is given, the largest
-// bin fill is read back first and, above kMaxBinFill, nothing else runs.
+// Bins `user` (device, n seeds).  When max_fill_host (2 ints) is given, the
+// largest bin fill and a flag for a seed with a non-finite value are read
+// back first and, above kMaxBinFill or with the flag set, nothing else runs.
 cudaError_t bin_seeds(const float4 *user, int n, int dim, BinWorkspace ws, BinOutputs out, cudaStream_t st,
                       int *max_fill_host);
 

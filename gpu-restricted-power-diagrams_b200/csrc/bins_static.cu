@@ -10,8 +10,6 @@
 // device memory instead of allocating it.  The array holds enough for
 // RPD_NOALLOC_MAX_SEEDS seeds; every GPU that loads the library keeps it
 // (about 1.7 MB) until the process exits.
-#include <mutex>
-
 #include "../../include/rpd.h"
 #include "bins.cuh"
 
@@ -32,25 +30,14 @@ constexpr size_t kStaticScratchInts =
 // address from cudaGetSymbolAddress.
 static __device__ __align__(256) int g_bin_scratch[kStaticScratchInts];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-int *g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_bin_scratch on the current device (set up once per
-// device, with that device current).
+// Device address of g_bin_scratch on the current device, looked up on every
+// call (cheap once the module is loaded), so a device reset by the host
+// application between calls never leaves a stale address behind.
 cudaError_t scratch_address(int **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_bin_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_bin_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = static_cast<int *>(p);
-  }
-  *out = g_scratch_addr[dev];
+  *out = static_cast<int *>(p);
   return cudaSuccess;
 }
 
@@ -81,10 +68,11 @@ extern "C" int rpd_bin_seeds_noalloc(const float *xyzw, int n, float *stored, in
   BinOutputs out{reinterpret_cast<float4 *>(stored), perm, counters, nullptr};
   // bin_seeds clears the counts and the max-fill word it accumulates into;
   // the rest of the scratch is fully overwritten before it is read
-  int max_fill = 0;
-  cudaError_t e = bin_seeds(reinterpret_cast<const float4 *>(xyzw), n, dim, ws, out, st, &max_fill);
+  int fill[2] = {0, 0};  // the largest bin fill, a non-finite seed
+  cudaError_t e = bin_seeds(reinterpret_cast<const float4 *>(xyzw), n, dim, ws, out, st, fill);
   if (e != cudaSuccess) return RPD_ERR_CUDA;
-  if (max_fill > kMaxBinFill) return RPD_ERR_DEGENERATE;
+  if (fill[1]) return RPD_ERR_INVALID;
+  if (fill[0] > kMaxBinFill) return RPD_ERR_DEGENERATE;
   if (cudaStreamSynchronize(st) != cudaSuccess) return RPD_ERR_CUDA;
   return RPD_OK;
 }

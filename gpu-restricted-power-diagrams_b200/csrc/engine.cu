@@ -586,7 +586,8 @@ __global__ void k_weight_min(const float4 *__restrict__ stored, int n, int *__re
 
 cudaError_t update_wmin(rpd_solver *s, cudaStream_t st) {
   cudaError_t e;
-  if ((e = s->wmin.ensure(sizeof(int))) != cudaSuccess) return e;
+  // wmin[1]: a flag of rpd_solver_set_weights
+  if ((e = s->wmin.ensure(2 * sizeof(int))) != cudaSuccess) return e;
   static const int highest = INT_MAX;
   if ((e = cudaMemcpyAsync(s->wmin.ptr, &highest, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
   const int blocks = std::min((s->n + 255) / 256, 4 * s->ctx->sm_count);
@@ -625,9 +626,15 @@ int rpd_solver_set_points(rpd_solver *s, const float *xyzw, int n, rpd_mem where
   ws.scan_tiles = ws.cursor + (nb + 1);
   ws.max_fill = ws.scan_tiles + scan_workspace_ints(int(nb + 1));
   BinOutputs out{s->stored.as<float4>(), s->perm.as<int>(), s->counters.as<int>(), s->user_to_stored.as<int>()};
-  int max_fill = 0;
-  if ((e = bin_seeds(s->user.as<float4>(), n, dim, ws, out, st, &max_fill)) != cudaSuccess)
+  int fill[2] = {0, 0};  // the largest bin fill, a non-finite seed
+  if ((e = bin_seeds(s->user.as<float4>(), n, dim, ws, out, st, fill)) != cudaSuccess)
     return map_cuda(ctx, e, "bin seeds");
+  const int max_fill = fill[0];
+  if (fill[1]) {
+    set_error(ctx, "a seed has a NaN or infinite coordinate or weight");
+    s->n = 0;
+    return RPD_ERR_INVALID;
+  }
   if (max_fill > kMaxBinFill) {
     set_error(ctx, "seeds too clustered: " + std::to_string(max_fill) + " in one bin (limit " +
                        std::to_string(kMaxBinFill) + ")");
@@ -653,6 +660,13 @@ __global__ void k_set_weights(const float *w, const int *user_to_stored, int n, 
   stored[user_to_stored[i]].w = x;
 }
 
+// Sets *bad when a value is NaN or infinite.
+__global__ void k_any_nonfinite(const float *__restrict__ v, int n, int *__restrict__ bad) {
+  bool b = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b |= !isfinite(v[i]);
+  if (b) *bad = 1;
+}
+
 int rpd_solver_set_weights(rpd_solver *s, const float *w, rpd_mem where) {
   if (!s || !w || s->n <= 0) return RPD_ERR_INVALID;
   rpd_context *ctx = s->ctx;
@@ -666,6 +680,19 @@ int rpd_solver_set_weights(rpd_solver *s, const float *w, rpd_mem where) {
     if ((e = cudaMemcpyAsync(s->weights.ptr, w, sizeof(float) * n, cudaMemcpyHostToDevice, st)) != cudaSuccess)
       return map_cuda(ctx, e, "copy weights");
     src = s->weights.as<float>();
+  }
+  // a NaN or infinite weight is rejected before any seed changes
+  if ((e = s->wmin.ensure(2 * sizeof(int))) != cudaSuccess) return map_cuda(ctx, e, "alloc flag");
+  int *bad_dev = s->wmin.as<int>() + 1;
+  if ((e = cudaMemsetAsync(bad_dev, 0, sizeof(int), st)) != cudaSuccess) return map_cuda(ctx, e, "clear flag");
+  k_any_nonfinite<<<std::max(1, std::min((n + 255) / 256, 4 * ctx->sm_count)), 256, 0, st>>>(src, n, bad_dev);
+  int bad = 0;
+  if ((e = cudaMemcpyAsync(&bad, bad_dev, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return map_cuda(ctx, e, "read flag");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "check weights");
+  if (bad) {
+    set_error(ctx, "a weight is NaN or infinite");
+    return RPD_ERR_INVALID;
   }
   k_set_weights<<<(n + 255) / 256, 256, 0, st>>>(src, s->user_to_stored.as<int>(), n, s->user.as<float4>(),
                                                  s->stored.as<float4>());

@@ -106,6 +106,22 @@ bool HostGrid::valid(std::string *why) const {
     }
   for (const auto &e : edges)
     if (!edges.count(std::make_pair(e.second, e.first))) return fail("open edge");
+  // no voxel whose 8 corners are all on the border (flag 1): the restriction
+  // could not find a start corner in it (Grid.cpp:147-168; corners past the
+  // last layer count as outside).  The reference's loop adds the offsets to
+  // the grid origin instead of to the voxel, so it only ever inspects voxel
+  // 0; the rule is applied here to every voxel, as its comment states.
+  for (int z = 0; z + 1 < size; ++z)
+    for (int y = 0; y + 1 < size; ++y)
+      for (int x = 0; x + 1 < size; ++x) {
+        int border = 0;
+        for (int c = 0; c < 8; ++c)
+          border += in_domain[size_t(x + (c & 1)) + size_t(y + ((c >> 1) & 1)) * size +
+                              size_t(z + (c >> 2)) * size * size] == 1;
+        if (border == 8)
+          return fail("voxel (" + std::to_string(x) + "," + std::to_string(y) + "," + std::to_string(z) +
+                      ") has only border corners");
+      }
   for (size_t o = 0; o + 1 < offsets.size(); ++o) {
     if (offsets[o] > offsets[o + 1]) return fail("bad offset ordering");
     for (int t = offsets[o]; t + 1 < offsets[o + 1]; ++t)

@@ -111,6 +111,10 @@ def lib():
         L.rpd_batch_launch.argtypes = [C.c_void_p]
         L.rpd_batch_get_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.rpd_batch_destroy.argtypes = [C.c_void_p]
+        L.rpd_seeds_load.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_float)),
+                                     C.POINTER(C.c_int)]
+        L.rpd_seeds_free.argtypes = [C.POINTER(C.c_float)]
+        L.rpd_seeds_save_binary.argtypes = [C.c_char_p, C.c_void_p, C.c_int]
         _lib = L
     return _lib
 
@@ -210,6 +214,31 @@ def default_context() -> Context:
     if _default_ctx is None:
         _default_ctx = Context(0)
     return _default_ctx
+
+
+def load_seeds(path, points4d: bool = False, binary: bool = False) -> np.ndarray:
+    """A seed file through the library's loader (rpd_seeds_load): the
+    reference's text .xyz format (Utils::loadSeedsFile, Utils.cpp:36-79; a
+    weight column with points4d) or its binary format (binary=True,
+    readBinarySeedsFile, Utils.cpp:81-97).  Returns (n, 4) float32 x y z w
+    in the reference frame, not normalised."""
+    p = C.POINTER(C.c_float)()
+    n = C.c_int(0)
+    rc = lib().rpd_seeds_load(os.fsencode(str(path)), int(points4d), int(binary), C.byref(p), C.byref(n))
+    if rc != 0:
+        raise RpdError(rc, f"could not load seeds from {path}")
+    try:
+        return np.ctypeslib.as_array(p, shape=(n.value, 4)).copy()
+    finally:
+        lib().rpd_seeds_free(p)
+
+
+def save_seeds_binary(path, xyzw) -> None:
+    """saveBinarySeedsFile (Utils.cpp:99-113) through rpd_seeds_save_binary."""
+    x = as_xyzw(xyzw)
+    rc = lib().rpd_seeds_save_binary(os.fsencode(str(path)), _ptr(x), len(x))
+    if rc != 0:
+        raise RpdError(rc, f"could not save seeds to {path}")
 
 
 def as_xyzw(points) -> np.ndarray:

@@ -79,7 +79,8 @@ void rpd_solver_destroy(rpd_solver *s);
 /* VoroAlgo::setInputPoints (voronoi.cpp:1088-1107) and the KNearests
  * constructor (knearests.cpp:48-222): copies n seeds (4 floats x y z w each,
  * from host or device memory) and bins them on the device.  The caller may
- * free `xyzw` when this returns. */
+ * free `xyzw` when this returns.  A NaN or infinite coordinate or weight is
+ * RPD_ERR_INVALID (the solver then holds no seeds). */
 int rpd_solver_set_points(rpd_solver *s, const float *xyzw, int n, rpd_mem where);
 /* KNearests::getNumPoints. */
 int rpd_solver_num_points(const rpd_solver *s);
@@ -92,12 +93,28 @@ int rpd_solver_get_permutation(rpd_solver *s, int *perm, rpd_mem where);
    The neighbour table of the last launch with the same K is reused, since
    the reference's neighbours ignore weights (knearests.cl:36-78).  No
    counterpart in the reference, which re-uploads all seeds
-   (voronoi.cpp:1088-1107). */
+   (voronoi.cpp:1088-1107).  A NaN or infinite weight is RPD_ERR_INVALID,
+   with the seeds left unchanged. */
 int rpd_solver_set_weights(rpd_solver *s, const float *w, rpd_mem where);
 /* KNearests::buildKnearests for every seed (knearests.cpp:238-315): the K
  * nearest other seeds, ascending distance, ties by stored index, written as
  * USER indices (-1 where fewer than K exist), n*K ints in user order. */
 int rpd_solver_knn(rpd_solver *s, int K, int *knn_user, rpd_mem where, float *device_ms);
+
+/* -------------------------------------------------------------- seed files */
+
+/* Utils::loadSeedsFile (Utils.cpp:36-79): a count line, then "x y z" per
+ * line ("x y z w" with four_d, --points4D; w = 0 otherwise), not normalised
+ * (test_voronoi.cpp:88).  With binary (--loadBinaryPoints,
+ * readBinarySeedsFile, Utils.cpp:81-97): a 64-bit count N, then 4N floats.
+ * On success *xyzw (4 * *n floats, malloc'ed; free with rpd_seeds_free) and
+ * *n are set.  RPD_ERR_IO when the file cannot be opened, RPD_ERR_FORMAT
+ * when a line does not parse, the count does not match or a value is NaN or
+ * infinite. */
+int rpd_seeds_load(const char *path, int four_d, int binary, float **xyzw, int *n);
+void rpd_seeds_free(float *xyzw);
+/* saveBinarySeedsFile (Utils.cpp:99-113, --saveBinaryPoints). */
+int rpd_seeds_save_binary(const char *path, const float *xyzw, int n);
 
 /* ------------------------------------------------------------------ domain */
 
@@ -428,11 +445,19 @@ int rpd_solver_trace_cell(rpd_solver *s, int user_id, const rpd_params *p, doubl
  *   dim_out   receives dim = round((n / 3.1)^(1/3))
  *   stream    cudaStream_t (null: the default stream)
  *
- * n > RPD_NOALLOC_MAX_SEEDS returns RPD_ERR_CAPACITY.  The first call on a
- * device looks up the array's device address; make that first call before
- * any stream capture.  Every call shares the one array, so calls that
- * overlap on the GPU (other streams, other host threads) race: serialize
- * them.  The call waits for its stream before returning. */
+ * n > RPD_NOALLOC_MAX_SEEDS returns RPD_ERR_CAPACITY; counters_cap below
+ * dim^3 + 1 or a misaligned seed pointer returns RPD_ERR_INVALID (dim_out is
+ * set first when n is in range); more than 4096 seeds in one bin returns
+ * RPD_ERR_DEGENERATE and a NaN or infinite value RPD_ERR_INVALID.  After any
+ * error the contents of stored, perm and counters are unspecified.
+ *
+ * The call is synchronous: it reads two words back from the device and waits
+ * for its stream before returning, so it must never be called on a stream
+ * that is being captured into a CUDA graph.  Every call looks up the array's
+ * device address on the current device (so a device reset between calls is
+ * harmless); the first call on a device also loads the library's device code
+ * there.  Every call shares the one array, so calls that overlap on the GPU
+ * (other streams, other host threads) race: serialize them. */
 #define RPD_NOALLOC_MAX_SEEDS 262144
 int rpd_bin_seeds_noalloc(const float *xyzw, int n, float *stored, int *perm, int *counters, int counters_cap,
                           int *dim_out, void *stream);

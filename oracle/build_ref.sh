@@ -9,10 +9,16 @@
 # ConvexCell.cl:45 (`#define make_real4 (real4)`, an OpenCL vector literal that
 # is not valid C++), for a call of the shim's constructor function.  No copy
 # of the sources is written anywhere.
+#
+# Usage: build_ref.sh REFERENCE_DIR   (or RPD_REFERENCE_DIR in the environment)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${RPD_REFERENCE_DIR:-/root/reference}"
+REF="${1:-${RPD_REFERENCE_DIR:-}}"
 OUT="$HERE/_ref"
+if [ -z "$REF" ]; then
+  echo "build_ref.sh: no reference directory given (argument or RPD_REFERENCE_DIR); skipping" >&2
+  exit 0
+fi
 if [ ! -f "$REF/ConvexCell.cl" ] || [ ! -f "$REF/knearests.cl" ]; then
   echo "build_ref.sh: reference sources not found at $REF; skipping" >&2
   exit 0

@@ -86,3 +86,38 @@ def test_fresh_neighbours_flag_recomputes_the_table(rpd):
     fresh = s.stats()["passes"][0]["knn_ms"]
     assert fresh > reused
     assert np.array_equal(s.moments(), m0)
+
+
+@pytest.mark.parametrize("bad", [float("nan"), float("inf"), -float("inf")])
+def test_nonfinite_seeds_and_weights_rejected(rpd, bad):
+    """A NaN or infinite coordinate or weight is RPD_ERR_INVALID (checked in
+    the binning pass, host or device input); a rejected weight update leaves
+    the seeds as they were."""
+    import ctypes as C
+
+    import torch
+
+    x = jittered(12, seed=3, weights=True)
+    for col in (0, 2, 3):
+        y = x.copy()
+        y[17, col] = bad
+        s = rpd.Solver()
+        with pytest.raises(rpd.RpdError) as e:
+            s.set_points(y)
+        assert e.value.code == -1 and s.n == 0
+        yd = torch.from_numpy(y).cuda()
+        rc = rpd.lib().rpd_solver_set_points(s.h, C.c_void_p(yd.data_ptr()), len(y), rpd.RPD_DEVICE)
+        assert rc == -1 and s.n == 0
+        s.set_points(x)  # the solver stays usable
+        assert s.n == len(x)
+        s.close()
+    s = rpd.Solver().set_points(x)
+    s.launch(K=20, P=30, V=40)
+    m0 = s.moments().copy()
+    w = x[:, 3].copy()
+    w[5] = bad
+    with pytest.raises(rpd.RpdError) as e:
+        s.set_weights(w)
+    assert e.value.code == -1
+    s.launch(K=20, P=30, V=40)
+    assert np.array_equal(s.moments(), m0)
