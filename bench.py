@@ -42,7 +42,7 @@ CONFIGS = {
                        K=20, P=25, V=30, T=100,
                        desc="5M seeds by seeded Poisson-disk dart throwing in [0,1]^3 (min distance 0.7 N^(-1/3)), "
                             "weights 0, unit cube domain at 128^3 (faces inset half a voxel, 2 triangles per face "
-                            "cell), K=20 P=25 V=30 T=100; every predicate in FP64 (escalated fraction 1.0)"),
+                            "cell), K=20 P=25 V=30 T=100"),
     # batched uneven diagrams in one graph (one GPU, or one batch per GPU)
     "batch-256": dict(kind="batch", count=256, nmin=1000, nmax=200_000, gmin=64, gmax=160, ks=(20, 50, 70),
                       nell=5, sseed=4, P=30, V=40, T=100,
@@ -88,6 +88,27 @@ def make_grid(cfg):
     if cfg["grid"] == "cube":
         return rpd.Grid.cube(cfg["gsize"])
     return None
+
+
+# FP64 FMA peak of this pool's B200, measured: 8 independent DFMA chains per
+# thread, 256-thread blocks, 4 and 8 blocks per SM, best of 10 CUDA-event
+# timings (34.17 TFLOP/s; FP32 FFMA the same way: 72.32 TFLOP/s).
+MEASURED_FP64_TFLOPS = 34.17
+SMSP_PER_SM = 4  # warp schedulers per SM: one warp instruction each per cycle
+
+
+def profile_counters(config, kernel="k_cell"):
+    """The per-launch counters of a committed ncu summary
+    (profiles/<kernel>_<config>_counters.txt), or {}."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{config}_counters.txt")
+    if os.path.exists(path):
+        with open(path) as f:
+            for ln in f:
+                if "=" in ln and not ln.startswith("#"):
+                    k, v = ln.split("=", 1)
+                    out[k.strip()] = float(v.strip())
+    return out
 
 
 def measured_peak_hbm():
@@ -146,126 +167,194 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(x, grid, cfg, target_s=10.0):
-    """The reference's own kernels compiled for the host CPU (or, when they
-    were not built here, the oracle restatement) on every host thread, over
-    a bounded sample of the same diagram: every stride-th binned seed."""
+REF_SAMPLE_CELLS = 100_000
+
+
+def ref_sample_stride(n):
+    """The CPU reference's sample of an n-seed diagram: every stride-th
+    binned seed, about REF_SAMPLE_CELLS cells (the whole diagram below)."""
+    return max(1, n // REF_SAMPLE_CELLS)
+
+
+def reference_cpu_step(x, grid, cfg, stride):
+    """One solve of the reference's own kernels compiled for the host CPU
+    (or, when they were not built here, the oracle restatement) on every host
+    thread, over every stride-th binned seed of the diagram, all passes.  The
+    timed work is the neighbour search and the cells of every pass; binning
+    the seed set and converting the grid are excluded, as on the device.
+    Returns (seconds, cells of the first pass, kind)."""
     import oracle
 
     kind = "reference" if oracle.has_reference_kernels() else "port"
     a = grid.arrays() if grid is not None else None
     ga = (oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
           if a is not None else None)
-    xd = x.astype(np.float64)
-    kw = dict(grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2, vhs1=2, use_double=False,
-              kernels=1 if kind == "reference" else 0, knn_mode=0)
+    _, _, st = oracle.solve(x.astype(np.float64), grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2,
+                            vhs1=2, use_double=False, kernels=1 if kind == "reference" else 0, knn_mode=0,
+                            sample_stride=stride, return_stats=True)
+    return st["knn_seconds"] + st["cell_seconds"], st["pass_cells"][0], kind
 
-    def run(stride):
-        # the timed work: neighbour search + cells of every pass (binning of
-        # the seed set and the grid upload are excluded, as on the device)
-        _, _, st = oracle.solve(xd, sample_stride=stride, return_stats=True, **kw)
-        return st["knn_seconds"] + st["cell_seconds"], st
 
+def cpu_baseline(x, grid, cfg, repeats=2):
+    """The reported CPU baseline: the same sample and the same runs as the
+    --impl reference arm (reference_cpu_step), one untimed run, then the mean
+    of `repeats`."""
     n = len(x)
-    stride0 = max(1, n // 20000)
-    t, st = run(stride0)
-    cells0 = st["pass_cells"][0]
-    rate0 = cells0 / max(t, 1e-9)
-    stride = max(1, int(round(n / max(1.0, rate0 * target_s))))
-    t, st = run(stride)
-    cells = st["pass_cells"][0]
+    stride = ref_sample_stride(n)
+    reference_cpu_step(x, grid, cfg, stride)
+    runs = [reference_cpu_step(x, grid, cfg, stride) for _ in range(repeats)]
+    t = sum(r[0] for r in runs) / len(runs)
+    cells, kind = runs[0][1], runs[0][2]
     return {"value": cells / t, "unit": "cells/s", "cores": os.cpu_count(), "kind": kind,
-            "sample": f"{cells} cells (every {stride}th binned seed of the same {n}-seed diagram, all passes), "
-                      f"{t:.2f} s on {os.cpu_count()} host threads"}
+            "sample": f"{cells} cells (every {stride}th binned seed of the same {n}-seed diagram, all passes; "
+                      f"the --impl reference arm's sample), {t:.2f} s per solve on {os.cpu_count()} host threads"}
 
 
-def accuracy(solver, x, grid, cfg, m_gpu, st_gpu, target_s=10.0):
-    """The device results against the FP64 oracle (restated reference, exact
-    neighbour order) on a bounded sample of the same diagram (every stride-th
-    binned seed, all passes): per-cell relative mass error and barycentre
-    error (normalised by the domain extent, 1000), status mismatches, the
-    symmetric difference of the non-empty cells; and the neighbour lists of
-    every seed against the oracle's (mismatching rows)."""
+class OracleSample:
+    """The FP64 oracle (restated reference, exact neighbour order) on a
+    bounded sample of a diagram: every stride-th binned seed (of the
+    oracle's own binning; in FP64 a few seeds near bin faces fall into the
+    next bin), all passes, about target_s seconds of host work."""
+
+    def __init__(self, x, grid, cfg, target_s=10.0):
+        import oracle
+
+        a = grid.arrays() if grid is not None else None
+        ga = (oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+              if a is not None else None)
+        self.xd = x.astype(np.float64)
+        self.cfg = cfg
+        n = len(x)
+        kw = dict(grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], use_double=True, knn_mode=1,
+                  return_stats=True)
+
+        def run(stride):
+            b, s, st = oracle.solve(self.xd, sample_stride=stride, **kw)
+            return b, s, st["knn_seconds"] + st["cell_seconds"], st["pass_cells"][0], st
+
+        stride = max(1, n // 5000)
+        _, _, t, cells, _ = run(stride)
+        stride = max(1, int(round(n / max(1.0, cells / max(t, 1e-9) * target_s))))
+        self.b, self.s, self.t, cells, self.ost = run(stride)
+        self.stride = stride
+        _, perm, _ = oracle.bin_seeds(self.xd, use_double=True)
+        self.u = np.asarray(perm)[::stride]
+
+    def metrics(self, m_gpu, st_gpu):
+        """Per-cell relative mass error and barycentre error (normalised by
+        the domain extent, 1000), status mismatches and the symmetric
+        difference of the non-empty cells on the sample."""
+        u, b, s = self.u, self.b, self.s
+        both = (st_gpu[u] == 4) & (s[u] == 4)
+        m, mr = m_gpu[u, 3], b[u, 3]
+        rel = np.abs(m - mr)[both] / np.maximum(np.abs(mr[both]), 1e-3)
+        nz = both & (np.abs(mr) > 1e-3) & (np.abs(m) > 1e-3)
+        bary = (np.abs(m_gpu[u][nz, :3] / m[nz, None] - b[u][nz, :3] / mr[nz, None]).max(1) / 1000.0
+                if nz.any() else np.zeros(1))
+        ne = (np.abs(m) > 1e-3) & (st_gpu[u] == 4)
+        ner = (np.abs(mr) > 1e-3) & (s[u] == 4)
+        return {"cells": int(len(u)), "status_mismatch": int((st_gpu[u] != s[u]).sum()),
+                "nonempty_symdiff": int((ne != ner).sum()),
+                "mass_max_rel": float(rel.max()) if rel.size else 0.0,
+                "mass_rms_rel": float(np.sqrt((rel ** 2).mean())) if rel.size else 0.0,
+                "bary_max": float(bary.max()), "bary_rms": float(np.sqrt((bary ** 2).mean()))}
+
+
+def accuracy(solver, sample, m_gpu, st_gpu):
+    """The device results against the FP64 oracle sample, and the neighbour
+    lists of every seed against the oracle's (mismatching rows)."""
     import oracle
 
-    a = grid.arrays() if grid is not None else None
-    ga = (oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
-          if a is not None else None)
-    xd = x.astype(np.float64)
-    n = len(x)
-    kw = dict(grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], use_double=True, knn_mode=1,
-              return_stats=True)
-
-    def run(stride):
-        b, s, st = oracle.solve(xd, sample_stride=stride, **kw)
-        return b, s, st["knn_seconds"] + st["cell_seconds"], st["pass_cells"][0], st
-
-    stride = max(1, n // 5000)
-    _, _, t, cells, _ = run(stride)
-    stride = max(1, int(round(n / max(1.0, cells / max(t, 1e-9) * target_s))))
-    b, s, t, cells, ost = run(stride)
-    # the sampled cells: every stride-th seed of the oracle's own binning (in
-    # FP64 a few seeds near bin faces fall into the next bin), as user ids
-    _, perm, _ = oracle.bin_seeds(xd, use_double=True)
-    u = np.asarray(perm)[::stride]
-    both = (st_gpu[u] == 4) & (s[u] == 4)
-    m, mr = m_gpu[u, 3], b[u, 3]
-    rel = np.abs(m - mr)[both] / np.maximum(np.abs(mr[both]), 1e-3)
-    nz = both & (np.abs(mr) > 1e-3) & (np.abs(m) > 1e-3)
-    bary = (np.abs(m_gpu[u][nz, :3] / m[nz, None] - b[u][nz, :3] / mr[nz, None]).max(1) / 1000.0
-            if nz.any() else np.zeros(1))
-    ne = (np.abs(m) > 1e-3) & (st_gpu[u] == 4)
-    ner = (np.abs(mr) > 1e-3) & (s[u] == 4)
+    cfg, ost = sample.cfg, sample.ost
     kg = solver.knn(cfg["K"])
-    ko = oracle.knn(xd, cfg["K"], knn_mode=1)
-    return {"oracle": "FP64 restatement, exact neighbour order", "cells": int(len(u)), "stride": stride,
-            "status_mismatch": int((st_gpu[u] != s[u]).sum()),
-            "nonempty_symdiff": int((ne != ner).sum()),
-            "mass_max_rel": float(rel.max()) if rel.size else 0.0,
-            "mass_rms_rel": float(np.sqrt((rel ** 2).mean())) if rel.size else 0.0,
-            "bary_max": float(bary.max()), "bary_rms": float(np.sqrt((bary ** 2).mean())),
-            "knn_rows_mismatch": int((kg != ko).any(1).sum()), "knn_rows": int(n), "oracle_seconds": round(t, 2),
-            # the reference algorithm's FP64 work on the sample, per cell: 45 flops
-            # per half-space test (det4x4 by cofactors), 41 per vertex from its
-            # three planes, 60 per vertex integrated (restated kernels' counts)
-            "fp64_flops_per_cell": (45.0 * ost["hs_tests"] + 41.0 * ost["vertex_evals"] +
-                                    60.0 * ost["export_vertices"]) / max(1, cells)}
+    ko = oracle.knn(sample.xd, cfg["K"], knn_mode=1)
+    out = {"oracle": "FP64 restatement, exact neighbour order", "stride": sample.stride}
+    out.update(sample.metrics(m_gpu, st_gpu))
+    cells = max(1, ost["pass_cells"][0])
+    out.update({"knn_rows_mismatch": int((kg != ko).any(1).sum()), "knn_rows": int(len(kg)),
+                "oracle_seconds": round(sample.t, 2),
+                # the reference algorithm's FP64 work on the sample, per cell: 45 flops
+                # per half-space test (det4x4 by cofactors), 41 per vertex from its
+                # three planes, 60 per vertex integrated (restated kernels' counts)
+                "fp64_flops_per_cell": (45.0 * ost["hs_tests"] + 41.0 * ost["vertex_evals"] +
+                                        60.0 * ost["export_vertices"]) / cells})
+    return out
+
+
+def precision_modes(solver, cfg, sample, flush, steps=6, warmup=3):
+    """The clipping loop in each arithmetic (rpd_params.precision) on the
+    same resident diagram: device time per solve, cells/s, the escalated
+    fraction of the half-space tests (from one untimed launch with the work
+    counters), and the accuracy against the FP64 oracle sample."""
+    import torch
+
+    import rpd
+
+    out = {}
+    n = solver.n
+    base = None
+    for name, prec in (("fp64", rpd.PRECISION_FP64), ("mixed", rpd.PRECISION_MIXED), ("fp32", rpd.PRECISION_FP32)):
+        p = rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_FRESH_NEIGHBOURS,
+                               precision=prec)
+        for _ in range(warmup):
+            solver.launch(p)
+        ms, cell_ms = [], []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            solver.launch(p)
+            st = solver.stats()
+            ms.append(st["total_ms"])
+            cell_ms.append(st["passes"][0]["cell_kernel_ms"])
+        m, stt = solver.moments().copy(), solver.status().copy()
+        solver.launch(rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_COUNTERS,
+                                         precision=prec))
+        c = solver.stats()["counters"]
+        t = float(np.median(ms))
+        e = {"value": n / (t / 1e3), "unit": "cells/s", "ms_per_step": t,
+             "cell_kernel_ms_first_pass": float(np.median(cell_ms)),
+             "vertex_tests": c["vertex_tests"], "escalated_tests": c["escalated_tests"],
+             "escalated_fraction": c["escalated_tests"] / max(1, c["vertex_tests"]),
+             "escalated_vertices": c["escalated_vertices"], "escalated_radius_tests": c["escalated_radii"],
+             "vs_fp64_oracle": sample.metrics(m, stt) if sample is not None else None}
+        if base is None:
+            base = (m, stt)
+        else:
+            e["bitwise_equal_to_fp64_mode"] = bool(np.array_equal(m, base[0]) and np.array_equal(stt, base[1]))
+        out[name] = e
+    out["mixed_over_fp32"] = out["mixed"]["value"] / out["fp32"]["value"]
+    out["target"] = ("north-star target: the mixed form >= 1.5x the plain FP32 path at <= 1e-5 mass error; " +
+                     ("met" if out["mixed_over_fp32"] >= 1.5 else "missed") +
+                     f" ({out['mixed_over_fp32']:.2f}x)")
+    return out
 
 
 def run_reference(args, cfg, rank, world):
     """--impl reference: the reference's CPU implementation of the path on the
-    host cores (rank 0 only)."""
+    host cores (rank 0 only), on the sample the cpu_baseline of the other arm
+    uses (reference_cpu_step)."""
     if rank != 0:
         return
     x = make_seeds(cfg, 0)
     grid = make_grid(cfg)
-    import oracle
-
-    kind = "reference" if oracle.has_reference_kernels() else "port"
-    a = grid.arrays() if grid is not None else None
-    ga = (oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
-          if a is not None else None)
-    xd = x.astype(np.float64)
     n = len(x)
-    stride = max(1, n // 100000)
-    kw = dict(grid=ga, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2, vhs1=2, use_double=False,
-              kernels=1 if kind == "reference" else 0, knn_mode=0, sample_stride=stride, return_stats=True)
+    stride = ref_sample_stride(n)
     for _ in range(args.warmup):
-        oracle.solve(xd, **kw)
-    times, cells = [], 0
+        reference_cpu_step(x, grid, cfg, stride)
+    times, cells, kind = [], 0, "reference"
     for _ in range(args.steps):
-        _, _, st = oracle.solve(xd, **kw)
-        times.append(st["knn_seconds"] + st["cell_seconds"])
-        cells = st["pass_cells"][0]
+        t, cells, kind = reference_cpu_step(x, grid, cfg, stride)
+        times.append(t)
     t = sum(times) / len(times)
     value = cells / t
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 half-space predicate, VHSAlgo 2)",
-        "data": "synthetic", "config": {"workload": args.config, "description": cfg["desc"], "n_seeds": n},
+        "data": "synthetic", "config": {"workload": args.config, "description": cfg["desc"], "n_seeds_per_gpu": n},
         "cpu_baseline": {"value": value, "unit": "cells/s", "cores": os.cpu_count(), "kind": kind,
-                         "sample": f"{cells} cells per step (every {stride}th binned seed of the {n}-seed diagram)"},
+                         "sample": f"{cells} cells per step (every {stride}th binned seed of the {n}-seed diagram, "
+                                   f"all passes)"},
         "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -380,9 +469,12 @@ def run_ours(args, cfg, rank, world, local):
     e2e_t = sum(e2e_s) / len(e2e_s)
     ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda")
 
-    # roofline of the dominant kernel (the cell kernel of the first pass):
-    # minimal DRAM bytes per launch = the neighbour table and the seeds read
-    # once, the moments and statuses written once, the grid arrays read once
+    # roofline of the dominant kernel (the cell kernel of the first pass),
+    # timed live with CUDA events: it is bound by instruction issue (ncu:
+    # warp-instruction counts and stalls in the committed profile), so the
+    # bound is the issue rate, 4 warp instructions per SM and cycle at the SM
+    # clock sampled during the timed steps; FP64 work against the measured
+    # DFMA peak and DRAM bytes against the measured copy bandwidth beside it
     a = grid.arrays() if grid is not None else None
     grid_bytes = 0 if a is None else int(a["in_domain"].nbytes + a["offsets"].nbytes + a["tri_list"].nbytes +
                                          a["triangles"].nbytes + len(a["points"]) * 16)
@@ -390,17 +482,34 @@ def run_ours(args, cfg, rank, world, local):
     rows = n - probe_out[-1]
     alg_bytes = rows * (4 * cfg["K"] + 16 + 32 + 4) + grid_bytes
     cell_avg_ms = sum(cell_ms) / len(cell_ms)
-    achieved = alg_bytes / (cell_avg_ms / 1e3) / 1e9
-    peak, peak_kind = measured_peak_hbm()
-    # DRAM bytes of one first-pass k_cell launch from the committed ncu summary
-    # of this workload (dram__bytes_read.sum + dram__bytes_write.sum)
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_cell_{args.config}_traffic.txt")
-    if os.path.exists(prof):
-        with open(prof) as f:
-            for ln in f:
-                if ln.startswith("bytes_per_launch"):
-                    traffic = int(ln.split("=")[1].strip())
+    peak_hbm, peak_kind = measured_peak_hbm()
+    prof = profile_counters(args.config)
+    # the profile's counts scaled to this launch's rows (equal for the same workload)
+    scale = rows / prof["rows"] if prof.get("rows") else None
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    issue_peak = 148 * SMSP_PER_SM * sm_mhz * 1e6 / 1e9  # G warp instructions / s
+    roofline = {"kernel": "k_cell (first pass)", "bound": "issue", "unit": "G warp-instructions/s",
+                "peak": issue_peak, "peak_source": f"148 SMs x {SMSP_PER_SM} schedulers x {sm_mhz:.0f} MHz "
+                                                  "(SM clock sampled during the timed steps)",
+                "launch_ms": cell_avg_ms, "rows": rows}
+    if scale:
+        inst = prof["warp_instructions_per_launch"] * scale
+        roofline["achieved"] = inst / (cell_avg_ms / 1e3) / 1e9
+        roofline["frac"] = roofline["achieved"] / issue_peak
+        roofline["warp_instructions_per_launch"] = inst
+        roofline["traffic"] = int(prof["bytes_per_launch"] * scale)
+        fp64 = prof["fp64_flops_per_launch"] * scale
+        roofline["fp64"] = {"achieved": fp64 / (cell_avg_ms / 1e3) / 1e12, "unit": "TFLOP/s",
+                            "peak": MEASURED_FP64_TFLOPS, "peak_source": "measured (DFMA microbenchmark)",
+                            "frac": fp64 / (cell_avg_ms / 1e3) / 1e12 / MEASURED_FP64_TFLOPS,
+                            "flops_per_launch": fp64, "work": "executed FP64 instructions (2 DFMA + DADD + DMUL)"}
+        roofline["counters_source"] = f"profiles/k_cell_{args.config}_counters.txt (ncu, one launch)"
+    else:
+        roofline.update({"achieved": None, "frac": None, "traffic": None,
+                         "note": "no committed ncu counters for this workload"})
+    achieved_hbm = alg_bytes / (cell_avg_ms / 1e3) / 1e9
+    roofline["hbm"] = {"achieved": achieved_hbm, "unit": "GB/s", "peak": peak_hbm, "peak_source": peak_kind,
+                       "frac": achieved_hbm / peak_hbm, "alg_bytes_per_launch": alg_bytes}
     line = {
         "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -413,11 +522,7 @@ def run_ours(args, cfg, rank, world, local):
                 "d2h_bytes_per_step": int(n * 32),
                 "path": "rpd_solver_set_points(host) + rpd_solver_launch + rpd_solver_get_moments(host)"},
         "gpu_launches": int(sum(launches)),
-        "roofline": {"kernel": "k_cell (first pass)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                     "alg_bytes_per_launch": alg_bytes, "launch_ms": cell_avg_ms,
-                     "note": "k_cell of the first pass timed alone with CUDA events; an issue-bound FP64 "
-                             "clipping kernel (ncu: issue active ~48%), so the HBM fraction is low by nature"},
+        "roofline": roofline,
         "clocks": clk,
         "detail": {"probe_ms": sum(probe_ms) / len(probe_ms), "probe_outside": probe_out[-1],
                    "knn_ms": sum(knn_ms) / len(knn_ms), "cell_ms_first_pass": cell_avg_ms, "cell_rows_first_pass": rows,
@@ -428,17 +533,19 @@ def run_ours(args, cfg, rank, world, local):
         "setup": setup,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(x, grid, cfg, target_s=args.cpu_seconds)
-        line["accuracy"] = acc = accuracy(solver, x, grid, cfg, m_gpu, st_gpu, target_s=args.cpu_seconds)
-        # the clipping's own bound is FP64 issue, not HBM: the reference
-        # algorithm's FP64 operations of the whole solve against B200's FP64 rate
-        # (datasheet: not measured on this pool)
+        line["cpu_baseline"] = cpu_baseline(x, grid, cfg)
+        sample = OracleSample(x, grid, cfg, target_s=args.cpu_seconds)
+        line["accuracy"] = acc = accuracy(solver, sample, m_gpu, st_gpu)
+        line["precision_modes"] = precision_modes(solver, cfg, sample, flush)
+        # the reference algorithm's FP64 work (its counts on the oracle
+        # sample) over the whole solve: work this engine mostly does not do
+        # (cached radii, the outside probe), so a reference-equivalent rate
         flops = acc["fp64_flops_per_cell"] * n
-        line["roofline_fp64"] = {"bound": "fp64", "achieved": flops / (ms / 1e3) / 1e12, "unit": "TFLOP/s",
-                                 "peak": 40.0, "peak_source": "nominal B200 FP64 (datasheet; not measured here)",
-                                 "frac": flops / (ms / 1e3) / 1e12 / 40.0, "flops_per_solve": flops,
-                                 "work_unit": "45 per half-space test + 41 per vertex + 60 per integrated vertex, "
-                                              "the reference algorithm's counts (FP64 oracle on the sample)"}
+        line["reference_equivalent_fp64"] = {
+            "achieved": flops / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "peak": MEASURED_FP64_TFLOPS,
+            "peak_source": "measured (DFMA microbenchmark)", "flops_per_solve": flops,
+            "work_unit": "45 per half-space test + 41 per vertex + 60 per integrated vertex, the reference "
+                         "algorithm's counts (FP64 oracle on the sample); not executed work"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     solver.close()
@@ -616,10 +723,14 @@ def run_batch(args, cfg, rank, world, local):
                    "pass0_cell_kernel_ms": cell_avg_ms, "batch": bstats},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        mid = int(np.argsort(sizes)[len(sizes) // 2])
-        cb = cpu_baseline(specs[mid]["xyzw"], grids[mid], dict(K=specs[mid]["K"], P=cfg["P"], V=cfg["V"],
-                                                               T=cfg["T"]), target_s=args.cpu_seconds)
-        cb["sample"] = f"diagram {mid} (the median size, {sizes[mid]} seeds, K={specs[mid]['K']}): " + cb["sample"]
+        # the --impl reference arm's sample and runs: one untimed, the mean of two
+        jobs = batch_reference_jobs(cfg)
+        batch_reference_step(cfg, jobs)
+        runs = [batch_reference_step(cfg, jobs) for _ in range(2)]
+        t_ref = sum(r[0] for r in runs) / 2
+        cb = {"value": runs[0][1] / t_ref, "unit": "cells/s", "cores": os.cpu_count(), "kind": runs[0][2],
+              "sample": f"{runs[0][1]} cells: " + BATCH_REF_SAMPLE.format(len(jobs)) +
+                        f" (the --impl reference arm's sample), {t_ref:.2f} s on {os.cpu_count()} host threads"}
         line["cpu_baseline"] = cb
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -633,40 +744,54 @@ def run_batch(args, cfg, rank, world, local):
         dist.destroy_process_group()
 
 
-def run_batch_reference(args, cfg, rank):
-    """--impl reference for the batch: the reference's CPU implementation over
-    a bounded sample of the same diagrams (every 16th), rank 0 only."""
-    if rank != 0:
-        return
+def batch_reference_jobs(cfg):
+    """The CPU reference's sample of the batch: every 16th diagram, each
+    sampled to about 6000 binned seeds (all passes)."""
     import oracle
     import rpd
 
     specs = batch_specs(cfg, 0)
     sub = [specs[i] for i in range(0, len(specs), 16)]
     grids = batch_grids(rpd, cfg, sub)
-    kind = "reference" if oracle.has_reference_kernels() else "port"
     jobs = []
     for s, g in zip(sub, grids):
         a = g.arrays()
         ga = oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
         n = len(s["xyzw"])
         jobs.append((s["xyzw"].astype(np.float64), ga, s["K"], max(1, n // 6000)))
+    return jobs
 
-    def step():
-        t, cells = 0.0, 0
-        for xd, ga, K, stride in jobs:
-            _, _, st = oracle.solve(xd, grid=ga, K=K, P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2, vhs1=2,
-                                    use_double=False, kernels=1 if kind == "reference" else 0, knn_mode=0,
-                                    sample_stride=stride, return_stats=True)
-            t += st["knn_seconds"] + st["cell_seconds"]
-            cells += st["pass_cells"][0]
-        return t, cells
 
+def batch_reference_step(cfg, jobs):
+    """One pass of the reference's own kernels (host build) over the sampled
+    diagrams: (seconds, cells of the first passes, kind)."""
+    import oracle
+
+    kind = "reference" if oracle.has_reference_kernels() else "port"
+    t, cells = 0.0, 0
+    for xd, ga, K, stride in jobs:
+        _, _, st = oracle.solve(xd, grid=ga, K=K, P=cfg["P"], V=cfg["V"], T=cfg["T"], vhs0=2, vhs1=2,
+                                use_double=False, kernels=1 if kind == "reference" else 0, knn_mode=0,
+                                sample_stride=stride, return_stats=True)
+        t += st["knn_seconds"] + st["cell_seconds"]
+        cells += st["pass_cells"][0]
+    return t, cells, kind
+
+
+BATCH_REF_SAMPLE = "every 16th diagram ({}), each sampled to about 6000 binned seeds, all passes"
+
+
+def run_batch_reference(args, cfg, rank):
+    """--impl reference for the batch: the reference's CPU implementation over
+    a bounded sample of the same diagrams (batch_reference_jobs), rank 0 only."""
+    if rank != 0:
+        return
+    jobs = batch_reference_jobs(cfg)
     for _ in range(args.warmup):
-        step()
-    times, cells = [], 0
+        batch_reference_step(cfg, jobs)
+    times, cells, kind = [], 0, "reference"
     for _ in range(args.steps):
-        t, cells = step()
+        t, cells, kind = batch_reference_step(cfg, jobs)
         times.append(t)
     t = sum(times) / len(times)
     value = cells / t
@@ -676,8 +801,7 @@ def run_batch_reference(args, cfg, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 half-space predicate, VHSAlgo 2)",
         "data": "synthetic", "config": {"workload": args.config, "description": cfg["desc"]},
         "cpu_baseline": {"value": value, "unit": "cells/s", "cores": os.cpu_count(), "kind": kind,
-                         "sample": f"{cells} cells per step: every 16th diagram ({len(jobs)}), each sampled to "
-                                   f"about 6000 binned seeds, all passes"},
+                         "sample": f"{cells} cells per step: " + BATCH_REF_SAMPLE.format(len(jobs))},
         "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

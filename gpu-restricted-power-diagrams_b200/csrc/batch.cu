@@ -411,6 +411,10 @@ int check_params(rpd_context *ctx, const rpd_params &p) {
     set_error(ctx, "batched solves return no Hessian rows (hessian_h > 0): use rpd_solver_launch");
     return RPD_ERR_INVALID;
   }
+  if (p.precision != RPD_PRECISION_FP64) {
+    set_error(ctx, "batched solves clip in FP64 only (precision): use rpd_solver_launch");
+    return RPD_ERR_INVALID;
+  }
   return RPD_OK;
 }
 

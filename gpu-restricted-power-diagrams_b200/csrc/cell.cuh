@@ -38,6 +38,9 @@ enum CellCounter {
   kCtrOutside,            // cells proven outside the domain before the end of clipping
   kCtrConeEmpty,          // boundary triangles whose cone misses the cell
   kCtrConesSkipped,       // boundary triangles dropped: they miss the cell (apex inside it)
+  kCtrEscTests,           // FP32 clipping: sign tests escalated to FP64
+  kCtrEscVertices,        // FP32 clipping: vertices made in FP64 (near-degenerate)
+  kCtrEscRadii,           // FP32 clipping: radius tests escalated to the exact FP64 radius
   kCtrNum
 };
 
@@ -68,6 +71,9 @@ struct CellLaunch {
   const int *ids = nullptr;        // stored ids of the rows (null: row i = seed i)
   int num = 0;
   int P = 0, V = 0, T = 0;         // caps of this pass
+  // clipping precision: 0 FP64; 1 mixed (FP32 with FP64 escalation, the FP64
+  // clipping's decisions); 2 plain FP32 (float planes, no escalation)
+  int precision = 0;
   // first pass: a cell whose clip succeeded and whose range holds more than T
   // but at most T_ahead triangles (with disjoint lists, counted by grid.tsat)
   // is parked now with all of them -- the result the retry passes would give
@@ -126,6 +132,8 @@ size_t defer_slot_bytes(int P, int V, int T);
 // k_cell over the rows; with a domain and a defer queue, also the chunked
 // boundary-triangle kernel and the per-cell reduction (3 launches).
 cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count = 148, int *launches = nullptr);
+// The same for a.precision > 0 (cell_prec.cu).
+cudaError_t cell_launch_prec(const CellLaunch &a, cudaStream_t st, int sm_count, int *launches);
 
 // Outside probe of a first pass with a domain.  The seeds of the 3x3x3 bins
 // around a seed's own are a subset of all seeds, so their bisectors bound a

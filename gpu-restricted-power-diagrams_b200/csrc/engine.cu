@@ -432,6 +432,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
     a.border_d = border_d;
   }
   a.grid = s->grid;
+  a.precision = s->precision;
   a.status = s->status.as<int>();
   a.out = s->out.as<double4>();
   a.counters = ctr;
@@ -769,6 +770,7 @@ void rpd_params_default(rpd_params *p) {
   p->keep_volume = 0.001;
   p->hessian_h = 0;
   p->hessian_hc = 1;
+  p->precision = RPD_PRECISION_FP64;
 }
 
 int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
@@ -910,6 +912,11 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
     set_error(ctx, "hessian_h must be >= 0 and hessian_hc 1 or 4");
     return RPD_ERR_INVALID;
   }
+  if (p.precision < RPD_PRECISION_FP64 || p.precision > RPD_PRECISION_FP32) {
+    set_error(ctx, "precision must be RPD_PRECISION_FP64, _MIXED or _FP32");
+    return RPD_ERR_INVALID;
+  }
+  s->precision = p.precision;
   s->hess_h = 0;
   if (p.hessian_h > 0) {
     if ((e = s->hess.ensure(sizeof(double) * size_t(n) * p.hessian_h * p.hessian_hc)) != cudaSuccess)

@@ -70,7 +70,8 @@ struct rpd_solver {
   rpd::DevBuf perm;            // int[n] stored -> user
   rpd::DevBuf user_to_stored;  // int[n]
   rpd::DevBuf weights;         // float[n]: staging for rpd_solver_set_weights
-  rpd::DevBuf wmin;            // int: the smallest weight of the seeds that are not walls (float_to_ordered)
+  rpd::DevBuf wmin;            // int[2]: the smallest weight of the seeds that are not walls
+                               // (float_to_ordered); a flag of rpd_solver_set_weights
   rpd::DevBuf counters;        // int[dim^3+1]
   rpd::DevBuf bin_ws;
   rpd::DevBuf ring_bound;      // float[dim+2]
@@ -98,6 +99,7 @@ struct rpd_solver {
   bool use_defer = true;       // park heavy boundary cells for the chunked kernel
   bool inner_apex = true;      // cone apex at a grid corner inside the cell
   bool fresh_knn = false;      // recompute the neighbour table at this launch
+  int precision = 0;           // RPD_PRECISION_* of the clipping loop
   // used cells (keep_distance >= 0 with a domain)
   rpd::DevBuf used;            // unsigned char[n], stored order: 0 or the ring distance
   bool used_on = false;

@@ -131,8 +131,12 @@ FLAG_REFERENCE_APEX = 16
 FLAG_FRESH_NEIGHBOURS = 32
 FLAG_NO_PROBE = 64
 FLAG_NO_T_AHEAD = 128
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+PRECISION_FP32 = 2
 COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
-                 "exports", "export_vertices", "outside_early", "cone_empty", "cones_skipped"]
+                 "exports", "export_vertices", "outside_early", "cone_empty", "cones_skipped",
+                 "escalated_tests", "escalated_vertices", "escalated_radii"]
 
 
 class Params(C.Structure):
@@ -141,7 +145,7 @@ class Params(C.Structure):
     _fields_ = [("K", C.c_int), ("P", C.c_int), ("V", C.c_int), ("T", C.c_int), ("max_extra_passes", C.c_int),
                 ("cube_eps", C.c_float), ("out_domain", C.c_int), ("flags", C.c_uint),
                 ("keep_distance", C.c_int), ("keep_volume", C.c_double), ("hessian_h", C.c_int),
-                ("hessian_hc", C.c_int)]
+                ("hessian_hc", C.c_int), ("precision", C.c_int)]
 
     @classmethod
     def default(cls, **kw):
@@ -156,7 +160,7 @@ class Stats(C.Structure):
     _fields_ = [("npasses", C.c_int), ("pass_cells", C.c_int * 8), ("pass_K", C.c_int * 8),
                 ("pass_P", C.c_int * 8), ("pass_V", C.c_int * 8), ("pass_T", C.c_int * 8),
                 ("pass_knn_ms", C.c_float * 8), ("pass_cell_ms", C.c_float * 8), ("status_hist", C.c_int * 11),
-                ("counters", C.c_ulonglong * 11), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
+                ("counters", C.c_ulonglong * 14), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
                 ("kernel_launches", C.c_int), ("pass_cell_kernel_ms", C.c_float * 8), ("probe_outside", C.c_int),
                 ("probe_ms", C.c_float)]
 

@@ -223,7 +223,28 @@ typedef struct rpd_params {
   int hessian_h;        /* --hessian with --H: facets per Hessian row, 0 off (the default;
                            Options.cpp:22,269) */
   int hessian_hc;       /* --HC: 1 (facet area) or 4 (area-weighted facet centroid and area) */
+  int precision;        /* RPD_PRECISION_*: arithmetic of the clipping loop */
 } rpd_params;
+
+/* Arithmetic of the clipping loop (the reference's VHSAlgo / USE_DOUBLE
+ * choice, ConvexCell.cl:400-461, voronoi.cpp:917-923).  Restriction to the
+ * domain and integration are FP64 in every mode.
+ *   FP64:  planes, vertices (cofactors), half-space tests and radius in FP64
+ *          (the reference's FP64 predicate, VHSAlgo 2, everywhere).
+ *   MIXED: the clipping state in float -- planes, vertex cofactors with error
+ *          majorants -- and every half-space test in float; a test whose value
+ *          lies within its rigorous error bound of the threshold (and a vertex
+ *          or radius test as close) is escalated to FP64, recomputed from the
+ *          FP64 planes, so every decision is the FP64 mode's: the same cells,
+ *          statuses and moments.  The reference's filtered FP32 predicate
+ *          (VHSAlgo 1, ConvexCell.cl:415-448) per test instead of per cell.
+ *          Escalations are counted (RPD_CTR_ESCALATED_*).
+ *   FP32:  plain float: planes rounded to float and every test in float with
+ *          no escalation (the reference's float build, VHSAlgo 0); the cells
+ *          are integrated from the float planes.  For comparison. */
+#define RPD_PRECISION_FP64 0
+#define RPD_PRECISION_MIXED 1
+#define RPD_PRECISION_FP32 2
 
 void rpd_params_default(rpd_params *p);
 
@@ -241,6 +262,11 @@ enum {
   RPD_CTR_CONE_EMPTY,   /* boundary triangles whose cone misses the cell */
   RPD_CTR_CONES_SKIPPED, /* boundary triangles dropped because they miss the cell
                             (cone apex at a grid corner inside the cell) */
+  RPD_CTR_ESCALATED_TESTS,    /* RPD_PRECISION_MIXED: vertex half-space tests decided
+                                 in FP64 (of RPD_CTR_VERTEX_TESTS) */
+  RPD_CTR_ESCALATED_VERTICES, /* RPD_PRECISION_MIXED: vertices made in FP64 */
+  RPD_CTR_ESCALATED_RADII,    /* RPD_PRECISION_MIXED: security-radius / outside tests
+                                 decided on the exact FP64 radius */
   RPD_CTR_NUM
 };
 

@@ -1008,7 +1008,7 @@ struct Solver {
 #pragma omp parallel num_threads(nth)
       {
         const int tid = omp_get_thread_num();
-#pragma omp for schedule(dynamic, 256)
+#pragma omp for schedule(dynamic, 1)
         for (int g0 = 0; g0 < num; g0 += 64) {
           const int cnt = std::min(64, num - g0);
           if (prm.knn_mode == 1)
@@ -1102,7 +1102,7 @@ struct Solver {
           hr.ids = hess_ids.data();
         }
         std::vector<int> tr0(std::max(T, 1) + 1), tr1(std::max(T, 1) + 1);
-#pragma omp for schedule(dynamic, 256)
+#pragma omp for schedule(dynamic, 16)
         for (int g = 0; g < num; ++g) {
           if (bordering_d > 0)
             border_cell<R>(cc, ids[g], nn.data() + size_t(g) * K, K, st_out, uc.flags, bordering_d);
