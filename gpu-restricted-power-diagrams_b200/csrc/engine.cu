@@ -379,6 +379,39 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
   return RPD_OK;
 }
 
+// The neighbour-search variant for K rows of this solver (rpd::KnnVariant).
+// RPD_FLAG_KNN_WARP / RPD_FLAG_KNN_THREAD force one.  Otherwise the
+// context's choice for K, made the first time K comes up with enough rows to
+// tell: both variants run on the first rows (one untimed round, one timed
+// with events), into `out`, which the real launch then overwrites; both give
+// the same lists, so only their speed differs.  Too few rows for a trial: a
+// thread per seed up to K = 64.
+int knn_variant_for(rpd_solver *s, const int *ids, int num, int K, unsigned *out, unsigned flags) {
+  if (flags & RPD_FLAG_KNN_WARP) return kKnnWarp;
+  if (flags & RPD_FLAG_KNN_THREAD) return K <= kKnnThreadMaxK ? kKnnThread : kKnnWarp;
+  if (K > kKnnThreadMaxK) return kKnnWarp;
+  rpd_context *ctx = s->ctx;
+  if (ctx->knn_variant[K] >= 0) return ctx->knn_variant[K];
+  constexpr int kTrialRows = 16384;
+  if (num < kTrialRows / 2) return K <= 64 ? kKnnThread : kKnnWarp;
+  const int m = std::min(num, kTrialRows);
+  cudaStream_t st = ctx->stream;
+  Events<4> ev;
+  float ms[2] = {0.f, 0.f};
+  for (int round = 0; round < 2; ++round)
+    for (int v = 0; v < 2; ++v) {
+      if (round) cudaEventRecord(ev[2 * v], st);
+      if (knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, ids, m, K, s->ring_bound.as<float>(),
+                     out, nullptr, st, v) != cudaSuccess)
+        return kKnnWarp;
+      if (round) cudaEventRecord(ev[2 * v + 1], st);
+    }
+  if (cudaEventSynchronize(ev[3]) != cudaSuccess) return kKnnWarp;
+  for (int v = 0; v < 2; ++v) cudaEventElapsedTime(&ms[v], ev[2 * v], ev[2 * v + 1]);
+  ctx->knn_variant[K] = ms[kKnnThread] < ms[kKnnWarp] ? kKnnThread : kKnnWarp;
+  return ctx->knn_variant[K];
+}
+
 // One pass (VoroAlgoComputeData::launch, voronoi.cpp:861-1036): the K
 // nearest of the listed seeds, then their cells with this pass's caps.
 static_assert(int(RPD_CTR_NUM) == int(kCtrNum), "counter enums out of sync");
@@ -401,8 +434,10 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   cudaEventRecord(ev[0], st);
   if (!reuse) {
     if (all_cells) s->knn_full_K = 0;
+    const int variant = knn_variant_for(s, ids, num, K, kb.as<unsigned>(), s->launch_flags);
+    if (pi < 8) S.pass_knn_variant[pi] = variant;
     e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, ids, num, K, s->ring_bound.as<float>(),
-                   kb.as<unsigned>(), ctr ? ctr + RPD_CTR_NUM : nullptr, st);
+                   kb.as<unsigned>(), ctr ? ctr + RPD_CTR_NUM : nullptr, st, variant);
     if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
     if (all_cells) s->knn_full_K = K;
     S.kernel_launches += 1;
@@ -562,6 +597,13 @@ rpd_solver *rpd_solver_create(rpd_context *ctx, int *err) {
   s->ctx = ctx;
   if (err) *err = RPD_OK;
   return s;
+}
+
+int rpd_context_knn_variant(rpd_context *ctx, int K, int variant) {
+  if (!ctx || K < 1 || K > kMaxK || variant < -2 || variant > 1) return RPD_ERR_INVALID;
+  if (variant == kKnnThread && K > kKnnThreadMaxK) return RPD_ERR_CAPACITY;
+  if (variant != -2) ctx->knn_variant[K] = (signed char)variant;
+  return ctx->knn_variant[K];
 }
 
 void rpd_solver_destroy(rpd_solver *s) {
@@ -734,7 +776,7 @@ int rpd_solver_knn(rpd_solver *s, int K, int *knn_user, rpd_mem where, float *de
   cudaEventRecord(ev[0], st);
   s->knn_full_K = 0;
   e = knn_launch(s->stored.as<float4>(), s->counters.as<int>(), s->dim, nullptr, s->n, K, s->ring_bound.as<float>(),
-                 s->knn.as<unsigned>(), nullptr, st);
+                 s->knn.as<unsigned>(), nullptr, st, knn_variant_for(s, nullptr, s->n, K, s->knn.as<unsigned>(), 0));
   cudaEventRecord(ev[1], st);
   if (e != cudaSuccess) return map_cuda(ctx, e, "knn");
   s->knn_full_K = K;
@@ -906,6 +948,7 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   s->use_defer = !(p.flags & RPD_FLAG_NO_DEFER);
   s->inner_apex = !(p.flags & RPD_FLAG_REFERENCE_APEX);
   s->fresh_knn = (p.flags & RPD_FLAG_FRESH_NEIGHBOURS) != 0;
+  s->launch_flags = p.flags;
   // used cells only with a domain (voronoi.cpp:1291)
   s->used_on = grid && p.keep_distance >= 0;
   if (p.hessian_h < 0 || (p.hessian_h > 0 && p.hessian_hc != 1 && p.hessian_hc != 4)) {

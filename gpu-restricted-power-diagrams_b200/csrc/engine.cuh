@@ -1,5 +1,6 @@
 // Engine state behind the C ABI: device context, resident seed sets.
 #pragma once
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -59,6 +60,10 @@ struct rpd_context {
   int sm_count = 0;
   cudaStream_t stream = nullptr;
   std::string error;
+  // neighbour-search variant per K (rpd::KnnVariant), picked by a timed
+  // trial on this device the first time K comes up; -1 not tried yet
+  signed char knn_variant[257];
+  rpd_context() { std::memset(knn_variant, -1, sizeof(knn_variant)); }
 };
 
 struct rpd_solver {
@@ -100,6 +105,7 @@ struct rpd_solver {
   bool inner_apex = true;      // cone apex at a grid corner inside the cell
   bool fresh_knn = false;      // recompute the neighbour table at this launch
   int precision = 0;           // RPD_PRECISION_* of the clipping loop
+  unsigned launch_flags = 0;   // RPD_FLAG_* of the current launch
   // used cells (keep_distance >= 0 with a domain)
   rpd::DevBuf used;            // unsigned char[n], stored order: 0 or the ring distance
   bool used_on = false;

@@ -205,6 +205,139 @@ __global__ void __launch_bounds__(256) k_knn(const float4 *__restrict__ stored, 
              lane);
 }
 
+// ---- one thread per seed ----
+//
+// The same search with one seed per thread: the thread walks its shells row
+// by row and keeps its K best keys in a max-heap in shared memory (root = the
+// K-th best so far; a closer candidate replaces the root and sifts down),
+// then heap-sorts them.  Far fewer instructions per seed than the warp's
+// merges for small K; the keys, the shells scanned and so the lists are the
+// same bit for bit.  Threads of a warp take consecutive stored seeds, whose
+// shells overlap, so their candidate loads hit L1.  The heap of thread t is
+// heap[i * kHeapStride + t], i < K: every thread owns one bank pair, and the
+// coalesced output pass (a warp per row, lanes over i) is conflict-free.
+constexpr int kThreadRows = 128;                 // seeds (threads) per block
+constexpr int kHeapStride = kThreadRows + 1;
+
+struct Heap {
+  unsigned long long *h;  // h[i * kHeapStride]
+  __device__ __forceinline__ unsigned long long &at(int i) const { return h[i * kHeapStride]; }
+  // key into a heap of n < K keys (grows by one)
+  __device__ __forceinline__ void push(int n, unsigned long long key) const {
+    int i = n;
+    while (i > 0) {
+      const int parent = (i - 1) >> 1;
+      const unsigned long long kp = at(parent);
+      if (kp >= key) break;
+      at(i) = kp;
+      i = parent;
+    }
+    at(i) = key;
+  }
+  // key into the root's place of a heap of n keys, sifted down
+  __device__ __forceinline__ void replace_root(int n, unsigned long long key) const {
+    int i = 0;
+    for (;;) {
+      const int l = 2 * i + 1;
+      if (l >= n) break;
+      int c = l;
+      unsigned long long kc = at(l);
+      if (l + 1 < n) {
+        const unsigned long long kr = at(l + 1);
+        if (kr > kc) {
+          c = l + 1;
+          kc = kr;
+        }
+      }
+      if (kc <= key) break;
+      at(i) = kc;
+      i = c;
+    }
+    at(i) = key;
+  }
+};
+
+__global__ void __launch_bounds__(kThreadRows) k_knn_thread(const float4 *__restrict__ stored,
+                                                           const int *__restrict__ counters, int dim,
+                                                           const int *__restrict__ ids, int num, int K,
+                                                           const float *__restrict__ ring_bound,
+                                                           unsigned *__restrict__ out,
+                                                           unsigned long long *__restrict__ candidates) {
+  extern __shared__ unsigned long long heap_smem[];
+  const int t = threadIdx.x;
+  const int row0 = blockIdx.x * kThreadRows;
+  const int row = row0 + t;
+  const Heap H{heap_smem + t};
+  unsigned long long ncand = 0;
+  if (row < num) {
+    const int pin = ids ? __ldg(&ids[row]) : row;
+    const float4 p = __ldg(&stored[pin]);
+    const int cin = bin_of(p, dim);
+    ShellRows sh;
+    sh.cx = cin % dim;
+    sh.cy = (cin / dim) % dim;
+    sh.cz = cin / (dim * dim);
+    sh.dim = dim;
+    int n = 0;
+    unsigned long long root = kEmptyKey;  // the K-th best once the heap is full
+    for (int ring = 0; ring <= dim; ring = ring == 0 ? 2 : ring + 1) {
+      if (ring >= 2) {
+        // whole-shell exit: the K-th best beats the shell bound
+        const float kd = __uint_as_float(unsigned(root >> 32));
+        if (kd < __ldg(&ring_bound[ring])) break;
+        if (sh.cx - ring < 0 && sh.cy - ring < 0 && sh.cz - ring < 0 && sh.cx + ring >= dim &&
+            sh.cy + ring >= dim && sh.cz + ring >= dim)
+          break;  // the shell lies outside the grid
+      }
+      sh.ring = ring;
+      const int nrows = sh.rows();
+      for (int q = 0; q < nrows; ++q) {
+        int a[2], l[2];
+        sh.ranges(q, counters, a[0], l[0], a[1], l[1]);
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+          for (int ptr = a[part], end = a[part] + l[part]; ptr < end; ++ptr) {
+            if (ptr == pin) continue;
+            const float4 qv = __ldg(&stored[ptr]);
+            const float dx = __fsub_rn(qv.x, p.x), dy = __fsub_rn(qv.y, p.y), dz = __fsub_rn(qv.z, p.z);
+            const float d = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(d)) << 32) | unsigned(ptr);
+            ++ncand;
+            if (n < K) {
+              H.push(n, key);
+              ++n;
+              if (n == K) root = H.at(0);
+            } else if (key < root) {
+              H.replace_root(K, key);
+              root = H.at(0);
+            }
+          }
+        }
+      }
+    }
+    // ascending order: the root (largest) to the back, one by one
+    for (int end = n - 1; end > 0; --end) {
+      const unsigned long long last = H.at(end);
+      H.at(end) = H.at(0);
+      H.replace_root(end, last);
+    }
+    for (int i = n; i < K; ++i) H.at(i) = kEmptyKey;
+  }
+  __syncthreads();
+  // coalesced rows: a warp per row, lanes over the row's entries
+  const int lane = t & 31, warp = t >> 5;
+  const int rows_here = min(kThreadRows, num - row0);
+  for (int r = warp; r < rows_here; r += kThreadRows / 32) {
+    unsigned *o = out + size_t(row0 + r) * K;
+    for (int i = lane; i < K; i += 32) o[i] = unsigned(heap_smem[i * kHeapStride + r] & 0xffffffffull);
+  }
+  if (candidates) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(kFull, ncand, o);
+    if (lane == 0) atomicAdd(candidates, ncand);
+  }
+}
+
 // Rows of many diagrams (batched solves): the diagrams of slot class S own
 // rows start[d] .. start[d+1] of this launch; warps stride over them.
 template <int S>
@@ -265,8 +398,20 @@ cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int 
 }
 
 cudaError_t knn_launch(const float4 *stored, const int *counters, int dim, const int *ids, int num, int K,
-                       const float *ring_bound, unsigned *out, unsigned long long *candidates, cudaStream_t st) {
+                       const float *ring_bound, unsigned *out, unsigned long long *candidates, cudaStream_t st,
+                       int variant) {
   if (num <= 0) return cudaSuccess;
+  if (variant == kKnnThread) {
+    if (K < 1 || K > kKnnThreadMaxK) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(unsigned long long) * size_t(K) * kHeapStride;
+    // the dynamic shared memory limit of the current device (a cheap host call)
+    cudaError_t e = cudaFuncSetAttribute(k_knn_thread, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(sizeof(unsigned long long) * kKnnThreadMaxK * kHeapStride));
+    if (e != cudaSuccess) return e;
+    const int blocks = (num + kThreadRows - 1) / kThreadRows;
+    k_knn_thread<<<blocks, kThreadRows, smem, st>>>(stored, counters, dim, ids, num, K, ring_bound, out, candidates);
+    return cudaGetLastError();
+  }
   const int threads = kKnnThreads;
   const long warps = num;
   const int blocks = int((warps * 32 + threads - 1) / threads);

@@ -18,8 +18,14 @@ void ring_bounds(int dim, float *bound);
 // other seeds as stored indices, ascending (distance, index); 0xffffffff
 // pads when fewer exist.  `candidates` (optional) accumulates the number of
 // distance evaluations.
+// variant: kKnnWarp (a warp per seed, bitonic merges) or kKnnThread (a
+// thread per seed, a shared-memory heap; K <= kKnnThreadMaxK); the lists
+// are the same bit for bit.
+enum KnnVariant { kKnnWarp = 0, kKnnThread = 1 };
+constexpr int kKnnThreadMaxK = 128;
 cudaError_t knn_launch(const float4 *stored, const int *counters, int dim, const int *ids, int num, int K,
-                       const float *ring_bound, unsigned *out, unsigned long long *candidates, cudaStream_t st);
+                       const float *ring_bound, unsigned *out, unsigned long long *candidates, cudaStream_t st,
+                       int variant = kKnnWarp);
 
 // One diagram of a batched neighbour launch: rows are ids[0..) (null: the
 // seeds 0..), row i written to out + i*K.

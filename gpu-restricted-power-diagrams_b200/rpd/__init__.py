@@ -55,6 +55,7 @@ def lib():
         L.rpd_context_stream.restype = C.c_void_p
         L.rpd_context_stream.argtypes = [C.c_void_p]
         L.rpd_version.restype = C.c_char_p
+        L.rpd_context_knn_variant.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.rpd_solver_create.restype = C.c_void_p
         L.rpd_solver_create.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
         L.rpd_solver_destroy.argtypes = [C.c_void_p]
@@ -131,6 +132,8 @@ FLAG_REFERENCE_APEX = 16
 FLAG_FRESH_NEIGHBOURS = 32
 FLAG_NO_PROBE = 64
 FLAG_NO_T_AHEAD = 128
+FLAG_KNN_WARP = 256
+FLAG_KNN_THREAD = 512
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRECISION_FP32 = 2
@@ -162,7 +165,7 @@ class Stats(C.Structure):
                 ("pass_knn_ms", C.c_float * 8), ("pass_cell_ms", C.c_float * 8), ("status_hist", C.c_int * 11),
                 ("counters", C.c_ulonglong * 14), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
                 ("kernel_launches", C.c_int), ("pass_cell_kernel_ms", C.c_float * 8), ("probe_outside", C.c_int),
-                ("probe_ms", C.c_float)]
+                ("probe_ms", C.c_float), ("pass_knn_variant", C.c_int * 8)]
 
     def as_dict(self):
         n = self.npasses
@@ -170,7 +173,8 @@ class Stats(C.Structure):
             "npasses": n,
             "passes": [{"cells": self.pass_cells[i], "K": self.pass_K[i], "P": self.pass_P[i], "V": self.pass_V[i],
                         "T": self.pass_T[i], "knn_ms": self.pass_knn_ms[i], "cell_ms": self.pass_cell_ms[i],
-                        "cell_kernel_ms": self.pass_cell_kernel_ms[i]}
+                        "cell_kernel_ms": self.pass_cell_kernel_ms[i],
+                        "knn_variant": ("warp", "thread")[self.pass_knn_variant[i]]}
                        for i in range(min(n, 8))],
             "status": {STATUS_NAMES[i]: v for i, v in enumerate(self.status_hist) if v},
             "counters": {COUNTER_NAMES[i]: int(v) for i, v in enumerate(self.counters)},
@@ -193,6 +197,14 @@ class Context:
 
     def error(self) -> str:
         return lib().rpd_context_error(self.h).decode()
+
+    def knn_variant(self, K: int, variant: int = -2) -> int:
+        """rpd_context_knn_variant: pin (0 warp, 1 thread per seed), forget
+        (-1) or read (-2) the neighbour-search variant for K."""
+        rc = lib().rpd_context_knn_variant(self.h, K, variant)
+        if rc < -1:
+            self.check(rc)
+        return rc
 
     def check(self, rc):
         if rc != RPD_OK:

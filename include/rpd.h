@@ -70,6 +70,12 @@ const char *rpd_context_error(const rpd_context *ctx);
 void *rpd_context_stream(rpd_context *ctx);
 /* Library version string. */
 const char *rpd_version(void);
+/* The neighbour-search variant the context uses for K (0: a warp per seed,
+ * 1: a thread per seed, K <= 128): variant 0 or 1 pins it, -1 forgets it
+ * (the next search with K times both again), -2 only reads it.  Returns the
+ * variant for K afterwards, -1 when not chosen yet, or an rpd_error.  No
+ * counterpart in the reference (one kernel, knearests.cl:36-78). */
+int rpd_context_knn_variant(rpd_context *ctx, int K, int variant);
 
 /* ------------------------------------------------------ seeds + neighbours */
 
@@ -202,6 +208,13 @@ rpd_grid *rpd_solver_export_grid(rpd_solver *s, int *err);
                                        to the retry passes instead of restricting at
                                        once the cells the retries would settle (same
                                        results) */
+#define RPD_FLAG_KNN_WARP 256u      /* neighbour search with a warp per seed (bitonic
+                                       merges) for every K (same results) */
+#define RPD_FLAG_KNN_THREAD 512u    /* neighbour search with a thread per seed (a
+                                       shared-memory heap) for K <= 128 (same results).
+                                       Without either flag each context picks the
+                                       faster for each K by a timed trial the first
+                                       time K comes up (rpd_stats.pass_knn_variant) */
 
 /* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
 typedef struct rpd_params {
@@ -292,6 +305,8 @@ typedef struct rpd_stats {
    * keep. */
   int probe_outside;
   float probe_ms;
+  int pass_knn_variant[8];         /* neighbour search of each pass: 0 a warp per seed,
+                                      1 a thread per seed */
 } rpd_stats;
 
 /* VoroAlgo::setGrid (voronoi.cpp:1079-1082): uploads the domain; null
