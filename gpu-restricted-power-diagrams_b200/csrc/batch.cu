@@ -43,6 +43,7 @@ struct DiagStatic {
   int early_out, inner_apex;
   const int *wmin;  // the smallest weight of the seeds that are not walls (float_to_ordered)
   int T_ahead;      // first pass: triangle overflows up to this count parked at once (0: off)
+  int probe;        // 1: the outside probe settles the seeds it can before the first pass
   float cube_eps;
   DevGrid grid;
   int *status;
@@ -64,6 +65,7 @@ struct DiagState {
   int rc_cond;        // 1: empty cells are not re-solved
   int hist[16];       // status histogram of the failing cells of the last recompute
   int ahead_max;      // the largest triangle count the first pass parked ahead
+  int probe_outside;  // seeds the outside probe proved empty
   int final_hist[16]; // status histogram of every cell at the end
   int pass_cells[kPassRecord], pass_K[kPassRecord], pass_P[kPassRecord], pass_V[kPassRecord], pass_T[kPassRecord];
 };
@@ -77,7 +79,9 @@ struct Plan {
   int *start_grid;   // ndiag+1
   int *start_plain;  // ndiag+1
   int *rc_start;     // ndiag+1
-  const int *s0, *s1;  // exclusive scans of the last recompute's flags
+  const int *s0, *s1;  // exclusive scans of the last recompute's flags (before the first
+                       // pass: of the probe's misses, over every cell)
+  const int *all_start;  // ndiag+1: every cell's row prefix
 };
 
 struct PassArgs {
@@ -134,7 +138,10 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
       s.A = g.ids_a;
       s.B = g.ids_b;
       s.C = g.ids_c;
-      s.num = g.n;
+      // with the probe, the first pass runs the seeds it left (their stored
+      // ids in C, scattered before this kernel)
+      s.num = g.probe ? pl.s0[pl.all_start[d + 1]] - pl.s0[pl.all_start[d]] : g.n;
+      s.probe_outside = g.n - s.num;
       s.rc_ids = nullptr;
       s.rc_cond = 0;
       s.rc_num = g.n;
@@ -233,7 +240,7 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     if (!s.active) continue;
     const int pi = s.npasses;
     if (pi < kPassRecord) {
-      s.pass_cells[pi] = s.num;
+      s.pass_cells[pi] = pa.pass == 0 ? g.n : s.num;  // the reference's first pass: every seed
       s.pass_K[pi] = s.K;
       s.pass_P[pi] = s.P;
       s.pass_V[pi] = s.V;
@@ -241,7 +248,7 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     }
     s.npasses++;
     for (int k = 0; k < 16; ++k) s.hist[k] = 0;
-    const int *ids = pa.pass == 0 ? nullptr : s.C;
+    const int *ids = pa.pass == 0 && !g.probe ? nullptr : s.C;
     unsigned *kout = pa.pass == 0 ? g.knn_full : pl.knn[d].out;
     KnnDiag &kd = pl.knn[d];
     kd.stored = g.stored;
@@ -328,6 +335,33 @@ __global__ void k_fail_scatter_batch(DiagState *__restrict__ st, const int *__re
   }
 }
 
+// The seeds the outside probe left (status kProbeMiss) in the probed
+// diagrams: flags over every cell (f[total] = 0), then their stored ids into
+// each diagram's C list in stored order.
+__global__ void k_probe_flags_batch(const DiagStatic *__restrict__ ds, const int *__restrict__ all_start, int ndiag,
+                                    int *__restrict__ f) {
+  const int total = all_start[ndiag];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= total; i += gridDim.x * blockDim.x) {
+    if (i == total) {
+      f[i] = 0;
+      continue;
+    }
+    const int d = owner_of_row(all_start, ndiag, i);
+    f[i] = ds[d].probe && ds[d].status[i - all_start[d]] == kProbeMiss;
+  }
+}
+
+__global__ void k_probe_scatter_batch(const DiagStatic *__restrict__ ds, const int *__restrict__ all_start, int ndiag,
+                                      const int *__restrict__ f, const int *__restrict__ pos) {
+  const int total = all_start[ndiag];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    if (!f[i]) continue;
+    const int d = owner_of_row(all_start, ndiag, i);
+    const int r = all_start[d];
+    ds[d].ids_c[pos[i] - pos[r]] = i - r;
+  }
+}
+
 // Final status histogram of every diagram.
 __global__ void k_final_hist(const DiagStatic *__restrict__ ds, DiagState *__restrict__ st,
                              const int *__restrict__ all_start, int ndiag) {
@@ -368,6 +402,9 @@ struct rpd_batch {
   DevBuf d_statics, d_states, d_descs, d_descs_inline, d_knn, d_kstart, d_start_grid, d_start_plain, d_rc_start,
       d_all_start;
   DevBuf f0, f1, s0, s1, scan_tiles;
+  DevBuf d_probes, d_probe_start;  // outside probe records of the probed diagrams, row prefixes
+  bool probed = false;             // the capture runs the outside probe
+  cudaEvent_t ev_probe = nullptr;  // after the probe and its compaction
   DevBuf retry_knn, defer_slots, defer_part, defer_fail, defer_ctr, defer_chunk_slot, work;
   DiagState *host_states = nullptr;  // pinned
   cudaGraph_t graph = nullptr;
@@ -386,6 +423,7 @@ struct rpd_batch {
       if (e) cudaEventDestroy(e);
     for (auto &e : ev_pass)
       if (e) cudaEventDestroy(e);
+    if (ev_probe) cudaEventDestroy(ev_probe);
   }
   void drop_graph() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -465,6 +503,22 @@ int describe(rpd_batch *b, std::vector<DiagStatic> &out) {
     if (g.T_ahead <= p.T) g.T_ahead = 0;
     g.inner_apex = (p.flags & RPD_FLAG_REFERENCE_APEX) ? 0 : 1;
     g.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
+    // the outside probe, as rpd_solver_launch runs it on a launch with fresh
+    // neighbours (every replay computes its neighbours afresh): with a domain
+    // that leaves plainly-outside voxels to prove
+    g.probe = 0;
+    if (grid && g.early_out && s->grid.sat && !(p.flags & RPD_FLAG_NO_PROBE)) {
+      const long long S = s->grid.size, S1 = S + 1;
+      if (s->grid_nonplain < 0) {
+        int v = 0;
+        if ((e = cudaMemcpyAsync(&v, s->grid.sat + (S1 * S1 * S1 - 1), sizeof(int), cudaMemcpyDeviceToHost,
+                                 ctx->stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+          return map_cuda(ctx, e, "read grid table");
+        s->grid_nonplain = v;
+      }
+      g.probe = s->grid_nonplain < 0.95 * double(S * S * S) ? 1 : 0;
+    }
     g.grid = s->grid;
     g.status = s->status.as<int>();
     g.out = s->out.as<double4>();
@@ -518,6 +572,32 @@ int capture(rpd_batch *b) {
     set_error(ctx, "batch: more than 2^31 cells");
     return RPD_ERR_INVALID;
   }
+  // outside probe records of the probed diagrams (the single solve's, run_probe)
+  std::vector<ProbeLaunch> probes;
+  std::vector<int> probe_start(1, 0);
+  for (int d = 0; d < nd; ++d) {
+    const DiagStatic &g = G[d];
+    if (!g.probe) continue;
+    ProbeLaunch pr;
+    pr.stored = g.stored;
+    pr.n = g.n;
+    pr.bins = g.bins;
+    pr.dim = g.dim;
+    pr.grid = g.grid;
+    pr.P = g.P0;
+    pr.V = g.V0;
+    pr.cube_eps = g.cube_eps;
+    const double spacing = 1000.0 / std::cbrt(double(g.n));
+    pr.min_plain_cage = 1.0 * spacing;
+    pr.min_plain = 1.5 * spacing;
+    pr.wmin = g.wmin;
+    pr.status = g.status;
+    pr.out = g.out;
+    probes.push_back(pr);
+    probe_start.push_back(probe_start.back() + g.n);
+  }
+  const int nprobe = int(probes.size());
+  const long probe_rows = probe_start.back();
   all_start[nd] = int(cells);
   b->cells = cells;
   // caps the launches of pass j hold: the first-pass maxima grown j times
@@ -547,7 +627,9 @@ int capture(rpd_batch *b) {
       (e = b->d_start_grid.ensure(sizeof(int) * stride)) != cudaSuccess ||
       (e = b->d_start_plain.ensure(sizeof(int) * stride)) != cudaSuccess ||
       (e = b->d_rc_start.ensure(sizeof(int) * stride)) != cudaSuccess ||
-      (e = b->d_all_start.ensure(sizeof(int) * stride)) != cudaSuccess)
+      (e = b->d_all_start.ensure(sizeof(int) * stride)) != cudaSuccess ||
+      (e = b->d_probes.ensure(sizeof(ProbeLaunch) * std::max(1, nprobe))) != cudaSuccess ||
+      (e = b->d_probe_start.ensure(sizeof(int) * (size_t(nprobe) + 1))) != cudaSuccess)
     return map_cuda(ctx, e, "alloc batch");
   const int nscan = int(cells) + 1;
   if ((e = b->f0.ensure(sizeof(int) * nscan)) != cudaSuccess || (e = b->f1.ensure(sizeof(int) * nscan)) != cudaSuccess ||
@@ -582,10 +664,15 @@ int capture(rpd_batch *b) {
     if (!x && (e = cudaEventCreate(&x)) != cudaSuccess) return map_cuda(ctx, e, "batch events");
   for (auto &x : b->ev_pass)
     if (!x && (e = cudaEventCreate(&x)) != cudaSuccess) return map_cuda(ctx, e, "batch events");
+  if (!b->ev_probe && (e = cudaEventCreate(&b->ev_probe)) != cudaSuccess) return map_cuda(ctx, e, "batch events");
   if ((e = cudaMemcpyAsync(b->d_statics.ptr, G.data(), sizeof(DiagStatic) * nd, cudaMemcpyHostToDevice, st)) !=
           cudaSuccess ||
       (e = cudaMemcpyAsync(b->d_all_start.ptr, all_start.data(), sizeof(int) * stride, cudaMemcpyHostToDevice, st)) !=
           cudaSuccess ||
+      (nprobe && (e = cudaMemcpyAsync(b->d_probes.ptr, probes.data(), sizeof(ProbeLaunch) * nprobe,
+                                      cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+      (e = cudaMemcpyAsync(b->d_probe_start.ptr, probe_start.data(), sizeof(int) * (nprobe + 1),
+                           cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->d_states.ptr, 0, sizeof(DiagState) * nd, st)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->f0.ptr, 0, sizeof(int) * nscan, st)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->f1.ptr, 0, sizeof(int) * nscan, st)) != cudaSuccess ||
@@ -604,6 +691,7 @@ int capture(rpd_batch *b) {
   pl.rc_start = b->d_rc_start.as<int>();
   pl.s0 = b->s0.as<int>();
   pl.s1 = b->s1.as<int>();
+  pl.all_start = b->d_all_start.as<int>();
   // persistent neighbour launches: a full SM of 256-thread blocks each
   const int knn_blocks = ctx->sm_count * (2048 / kKnnThreads);
   const int flat_blocks = ctx->sm_count * 8;
@@ -645,6 +733,20 @@ int capture(rpd_batch *b) {
     }
     pa.defer = dq;
     if (j < kPassRecord && (e = mark(b->ev_pass[j])) != cudaSuccess) return fail(e, "batch event");
+    if (j == 0 && nprobe) {
+      // the outside probe over every seed of the probed diagrams, then the
+      // stored ids of the seeds it left (the first pass's rows)
+      if ((e = probe_batch_launch(b->d_probes.as<ProbeLaunch>(), b->d_probe_start.as<int>(), nprobe, probe_rows,
+                                  Pb[0], Vb[0], st)) != cudaSuccess)
+        return fail(e, "batch probe");
+      k_probe_flags_batch<<<flat_blocks, 256, 0, st>>>(ds, b->d_all_start.as<int>(), nd, b->f0.as<int>());
+      if ((e = exclusive_scan(b->f0.as<int>(), b->s0.as<int>(), nscan, b->scan_tiles.as<int>(), st)) != cudaSuccess)
+        return fail(e, "batch scan");
+      k_probe_scatter_batch<<<flat_blocks, 256, 0, st>>>(ds, b->d_all_start.as<int>(), nd, b->f0.as<int>(),
+                                                         b->s0.as<int>());
+      launches += 6;  // probe, flags, scan (3), scatter
+      if ((e = mark(b->ev_probe)) != cudaSuccess) return fail(e, "batch event");
+    }
     k_plan<<<1, 1024, 0, st>>>(ds, sts, nd, pl, pa);
     ++launches;
     if (j == 0 && (e = mark(b->ev[0])) != cudaSuccess) return fail(e, "batch event");
@@ -653,8 +755,8 @@ int capture(rpd_batch *b) {
       const int S = kKnnClassSlots[c];
       const bool want = j == 0 ? class_used[c] : (S >= knn_slots(Kmin) && S <= knn_slots(Kb[j]));
       if (!want) continue;
-      if ((e = knn_batch_launch(S, pl.knn, pl.kstart + c * stride, nd, knn_blocks, st, j == 0 ? class_rows[c] : -1)) !=
-          cudaSuccess)
+      if ((e = knn_batch_launch(S, pl.knn, pl.kstart + c * stride, nd, knn_blocks, st,
+                                j == 0 && !nprobe ? class_rows[c] : -1)) != cudaSuccess)
         return fail(e, "batch knn");
       ++launches;
     }
@@ -675,7 +777,7 @@ int capture(rpd_batch *b) {
     cb.after_cell = j == 0 ? b->ev[2] : nullptr;
     // the first pass's rows are every cell: one warp per row; the retries'
     // rows are known on the device only: persistent, rows from a counter
-    cb.rows_grid = j == 0 ? rows_grid0 : -1;
+    cb.rows_grid = j == 0 && !nprobe ? rows_grid0 : -1;
     cb.rows_plain = j == 0 ? rows_plain0 : -1;
     cb.work = b->work.as<int>();
     if ((e = cell_batch_launch(cb, st, ctx->sm_count, &launches)) != cudaSuccess) return fail(e, "batch cells");
@@ -710,6 +812,7 @@ int capture(rpd_batch *b) {
   }
   b->passes = passes;
   b->launches = launches;
+  b->probed = nprobe > 0;
   b->captures++;
   return RPD_OK;
 }
@@ -791,6 +894,7 @@ int rpd_batch_launch(rpd_batch *b) {
   cudaEventElapsedTime(&S.pass0_cell_kernel_ms, b->ev[1], b->ev[2]);
   const int rec = std::min(b->passes, kPassRecord);
   for (int j = 0; j < rec; ++j) cudaEventElapsedTime(&S.pass_ms[j], b->ev_pass[j], b->ev_pass[j + 1]);
+  if (b->probed) cudaEventElapsedTime(&S.probe_ms, b->ev_pass[0], b->ev_probe);
   std::vector<int> again;
   for (int d = 0; d < b->ndiag; ++d) {
     const DiagState &h = b->host_states[d];
@@ -813,8 +917,11 @@ int rpd_batch_launch(rpd_batch *b) {
     for (int i = 0; i < kStatusNum; ++i) T.status_hist[i] = h.final_hist[i];
     T.total_ms = ms;
     T.kernel_launches = b->launches;
+    T.probe_outside = h.probe_outside;
+    S.probe_outside += h.probe_outside;
     S.max_passes = std::max(S.max_passes, h.npasses);
-    s->knn_full_K = b->params[d].K;
+    // with the probe the table holds the first pass's rows only
+    s->knn_full_K = b->statics[d].probe ? 0 : b->params[d].K;
     s->used_on = false;
     s->used_count = -1;
     s->hess_h = 0;

@@ -41,6 +41,36 @@ cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count, int 
   return launch_vs<8>(a, L, st, sm_count, launches);
 }
 
+cudaError_t probe_batch_launch(const ProbeLaunch *probes, const int *start, int ndiag, long rows, int P, int V,
+                               cudaStream_t st) {
+  if (rows <= 0) return cudaSuccess;
+  if (P > kMaxP || V > kMaxV || P < 7 || V < 8) return cudaErrorInvalidValue;
+  const Layout L = make_layout(P, V, 0, false);
+  const int wpb = warps_per_block_for(L);
+  if (wpb == 0) return cudaErrorInvalidValue;
+  const size_t smem = size_t(L.total) * wpb;
+  const int blocks = int((rows + wpb - 1) / wpb);
+  const int vs = L.Vc / 32;
+  cudaError_t e;
+#define RPD_PROBE_BATCH(VSN)                                                        \
+  e = allow_smem(reinterpret_cast<const void *>(k_probe_batch<VSN>), smem);         \
+  if (e != cudaSuccess) return e;                                                   \
+  k_probe_batch<VSN><<<blocks, wpb * 32, smem, st>>>(probes, start, ndiag, L);
+  if (vs <= 2) {
+    RPD_PROBE_BATCH(2)
+  } else if (vs <= 3) {
+    RPD_PROBE_BATCH(3)
+  } else if (vs <= 4) {
+    RPD_PROBE_BATCH(4)
+  } else if (vs <= 6) {
+    RPD_PROBE_BATCH(6)
+  } else {
+    RPD_PROBE_BATCH(8)
+  }
+#undef RPD_PROBE_BATCH
+  return cudaGetLastError();
+}
+
 cudaError_t probe_launch(const ProbeLaunch &p, cudaStream_t st) {
   if (p.n <= 0) return cudaSuccess;
   if (p.P > kMaxP || p.V > kMaxV || p.P < 7 || p.V < 8 || !p.grid.sat || !p.wmin) return cudaErrorInvalidValue;

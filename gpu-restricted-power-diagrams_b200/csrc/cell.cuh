@@ -159,6 +159,12 @@ struct ProbeLaunch {
   double4 *out = nullptr;          // n, stored order
 };
 cudaError_t probe_launch(const ProbeLaunch &p, cudaStream_t st);
+// The probe over every seed of many diagrams (batched solves): diagram d's
+// record probes[d] (device) and rows start[d] .. start[d+1] (device; `rows`
+// of them in all, known when the launch is made); P and V at least every
+// diagram's first-pass caps.
+cudaError_t probe_batch_launch(const ProbeLaunch *probes, const int *start, int ndiag, long rows, int P, int V,
+                               cudaStream_t st);
 
 // Whether one warp's layout for these caps fits a block's shared memory.
 bool cell_caps_fit(int P, int V, int T, bool grid);

@@ -2541,14 +2541,13 @@ __device__ __forceinline__ unsigned cage_bits(float nx, float ny, float nz, floa
 // with a ball of at least min_plain, the 32 nearest candidates (warp
 // bitonic merges) clip the box in distance order until the cell fits the
 // ball.
+// vc: the vertex capacity the warp works with (the layout's, or a batched
+// diagram's own, vertex_capacity).
 template <int VS>
-__global__ void __launch_bounds__(128, 6) k_probe(const __grid_constant__ ProbeLaunch p,
-                                                  const __grid_constant__ Layout L) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int lane = threadIdx.x & 31;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (row >= p.n) return;
-  WarpCell w = bind(smem + size_t(threadIdx.x >> 5) * L.total, L);
+__device__ __forceinline__ void probe_row(const ProbeLaunch &p, const Layout &L, unsigned char *wsmem, int row,
+                                          int vc, int lane) {
+  WarpCell w = bind(wsmem, L);
+  w.vc = vc;
   const float4 s = p.stored[row];
   const double plain2 = s.w <= kNoCellLimits ? -1.0 : plain_radius2(p.grid, s, lane);
   bool proven = false;
@@ -2654,6 +2653,33 @@ __global__ void __launch_bounds__(128, 6) k_probe(const __grid_constant__ ProbeL
     p.status[row] = proven ? kSuccess : kProbeMiss;
     if (proven) p.out[row] = make_double4(0.0, 0.0, 0.0, 0.0);
   }
+}
+
+template <int VS>
+__global__ void __launch_bounds__(128, 6) k_probe(const __grid_constant__ ProbeLaunch p,
+                                                  const __grid_constant__ Layout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= p.n) return;
+  probe_row<VS>(p, L, smem + size_t(threadIdx.x >> 5) * L.total, row, L.Vc, lane);
+}
+
+// The outside probe over the rows of many diagrams (batched solves):
+// diagram d owns rows start[d] .. start[d+1] (all its seeds) and its own
+// record probes[d]; one warp per row.  The layout holds every diagram's
+// caps; each works with its own vertex capacity.
+template <int VS>
+__global__ void __launch_bounds__(128, 6) k_probe_batch(const ProbeLaunch *__restrict__ probes,
+                                                        const int *__restrict__ start, int ndiag,
+                                                        const __grid_constant__ Layout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (r >= start[ndiag]) return;
+  const int d = owner_of_row(start, ndiag, r);
+  const ProbeLaunch &p = probes[d];
+  probe_row<VS>(p, L, smem + size_t(threadIdx.x >> 5) * L.total, r - start[d], min(L.Vc, (p.V + 31) & ~31), lane);
 }
 
 // Rows of many diagrams in one persistent launch (batched solves): diagram

@@ -440,7 +440,8 @@ class BatchStats(C.Structure):
     _fields_ = [("diagrams", C.c_int), ("cells", C.c_longlong), ("graph_ms", C.c_float),
                 ("passes_captured", C.c_int), ("max_passes", C.c_int), ("kernel_launches", C.c_int),
                 ("captures", C.c_int), ("solved_alone", C.c_int), ("pass0_knn_ms", C.c_float),
-                ("pass0_cell_kernel_ms", C.c_float), ("pass_ms", C.c_float * 8), ("pass_cells", C.c_longlong * 8)]
+                ("pass0_cell_kernel_ms", C.c_float), ("pass_ms", C.c_float * 8), ("pass_cells", C.c_longlong * 8),
+                ("probe_ms", C.c_float), ("probe_outside", C.c_longlong)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pass_ms", "pass_cells")}

@@ -451,6 +451,8 @@ typedef struct rpd_batch_stats {
   float pass0_cell_kernel_ms; /* of graph_ms: the first pass's cell kernel (no cone kernels) */
   float pass_ms[8];     /* of graph_ms: each captured pass (plan, neighbours, cells, compaction) */
   long long pass_cells[8]; /* cells of each pass, all diagrams */
+  float probe_ms;       /* of pass_ms[0]: the outside probe and its compaction (0: no diagram probed) */
+  long long probe_outside; /* seeds the probe proved empty outside their domains, all diagrams */
 } rpd_batch_stats;
 
 rpd_batch *rpd_batch_create(rpd_context *ctx, rpd_solver *const *solvers, const rpd_params *params, int count,

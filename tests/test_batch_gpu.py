@@ -36,16 +36,15 @@ def build(rpd, sp, with_grid):
 
 
 def alone(rpd, x, g, p):
-    """The diagram solved on its own, without the outside probe (which
-    batches do not run): its per-pass cell counts are the batch's too (the
-    probe can settle in the first pass an empty cell outside the domain
-    that a full clip would retry).  Both settle triangle overflows ahead."""
+    """The diagram solved on its own: a first launch after its seeds were
+    set, so with the outside probe as in every batch replay (the probe can
+    settle in the first pass an empty cell outside the domain that a full
+    clip would retry, so per-pass cell counts depend on it).  Both settle
+    triangle overflows ahead."""
     s = rpd.Solver().set_points(x)
     if g is not None:
         s.set_grid(g)
-    q = rpd.Params.from_buffer_copy(p)
-    q.flags |= rpd.FLAG_NO_PROBE
-    s.launch(q)
+    s.launch(p)
     return s
 
 
@@ -55,6 +54,7 @@ def assert_same(got, ref):
     a, b = got.stats(), ref.stats()
     assert a["npasses"] == b["npasses"]
     assert a["status"] == b["status"]
+    assert a["probe_outside"] == b["probe_outside"]
     for pa, pb in zip(a["passes"], b["passes"]):
         assert (pa["cells"], pa["K"], pa["P"], pa["V"], pa["T"]) == (pb["cells"], pb["K"], pb["P"], pb["V"], pb["T"])
 
@@ -72,12 +72,16 @@ def test_batch_equals_solves_alone(rpd):
             p.flags |= rpd.FLAG_FIRST_PASS_ONLY
         if i == 7:
             p.flags |= rpd.FLAG_REFERENCE_APEX
+        if i == 9:
+            p.flags |= rpd.FLAG_NO_PROBE
         params.append(p)
     b = rpd.Batch(solvers, params)
     b.launch()
     st = b.stats()
     assert st["diagrams"] == 12 and st["cells"] == sum(len(s["xyzw"]) for s in sp)
     assert st["max_passes"] >= 3 and st["captures"] == 1
+    assert st["probe_outside"] > 0  # the domains leave plainly-outside seeds to prove
+    assert solvers[9].stats()["probe_outside"] == 0
     for i, s in enumerate(sp):
         assert_same(solvers[i], alone(rpd, s["xyzw"], grids[i], params[i]))
 
@@ -132,3 +136,5 @@ def test_batch_rejects_unsupported(rpd):
         rpd.Batch(solvers, rpd.Params.default(flags=rpd.FLAG_COUNTERS))
     with pytest.raises(rpd.RpdError):
         rpd.Batch(solvers, rpd.Params.default(keep_distance=1)).launch()
+    with pytest.raises(rpd.RpdError):
+        rpd.Batch(solvers, rpd.Params.default(precision=rpd.PRECISION_MIXED))
