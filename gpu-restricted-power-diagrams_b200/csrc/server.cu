@@ -239,6 +239,11 @@ struct rpd_server {
         r->info.device_ms = st.total_ms;
         r->info.npasses = st.npasses;
         r->info.failed_cells = rc == RPD_OK ? r->n - st.status_hist[RPD_SUCCESS] - st.status_hist[RPD_EMPTY_CELL] : r->n;
+        for (int k = 0; k < RPD_STATUS_NUM; ++k) r->info.status_hist[k] = rc == RPD_OK ? st.status_hist[k] : 0;
+        r->info.last_caps[0] = st.npasses > 0 ? st.pass_K[std::min(st.npasses, 8) - 1] : 0;
+        r->info.last_caps[1] = st.npasses > 0 ? st.pass_P[std::min(st.npasses, 8) - 1] : 0;
+        r->info.last_caps[2] = st.npasses > 0 ? st.pass_V[std::min(st.npasses, 8) - 1] : 0;
+        r->info.last_caps[3] = st.npasses > 0 ? st.pass_T[std::min(st.npasses, 8) - 1] : 0;
         if (rc != RPD_OK) {
           const char *msg = rpd_context_error(c);
           std::snprintf(r->info.error, sizeof(r->info.error), "%s", msg ? msg : "");

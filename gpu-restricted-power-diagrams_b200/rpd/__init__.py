@@ -683,11 +683,14 @@ class RequestInfo(C.Structure):
     _fields_ = [("status", C.c_int), ("session", C.c_int), ("n", C.c_int), ("slot", C.c_int),
                 ("queue_ms", C.c_double), ("latency_ms", C.c_double), ("device_ms", C.c_double),
                 ("npasses", C.c_int), ("admitted_at_ms", C.c_double), ("done_at_ms", C.c_double),
-                ("failed_cells", C.c_int), ("error", C.c_char * 160)]
+                ("failed_cells", C.c_int), ("error", C.c_char * 160), ("status_hist", C.c_int * 11),
+                ("last_caps", C.c_int * 4)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["error"] = self.error.decode(errors="replace")
+        d["status_hist"] = {STATUS_NAMES[i]: v for i, v in enumerate(self.status_hist) if v}
+        d["last_caps"] = dict(zip("KPVT", list(self.last_caps)))
         return d
 
 

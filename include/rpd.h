@@ -362,6 +362,8 @@ typedef struct rpd_request_info {
   double done_at_ms;      /* since the server was created */
   int failed_cells;   /* cells whose final status is neither success nor empty */
   char error[160];    /* the context's error text when status != RPD_OK */
+  int status_hist[RPD_STATUS_NUM]; /* final status of every cell of the request */
+  int last_caps[4];   /* K, P, V, T of the request's last pass */
 } rpd_request_info;
 
 rpd_server *rpd_server_create(int device, int slots, size_t mem_budget, int *err);

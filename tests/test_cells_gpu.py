@@ -234,3 +234,15 @@ def test_bench_workloads_full_size(rpd, workload):
     g = bench.make_grid(cfg)
     met, got, gst, *_ = run_case(rpd, x, grid=g, K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"])
     assert_parity(met)
+
+
+def test_cell_in_the_box_margin_has_no_start_corner(rpd):
+    """A weighted cell entirely in the box's margin past the grid (x >
+    1000.05): the reference's find_another_beginning_vertex, as the oracle
+    gives it; every other cell as the oracle."""
+    import test_oracle
+
+    g, _, x = test_oracle._margin_cell_case()
+    met, got, gst, ref, rst, _ = run_case(rpd, x.astype(np.float32), grid=g, K=30, P=30, V=40, T=100)
+    assert gst[-1] == 7 and rst[-1] == 7
+    assert_parity(met)
