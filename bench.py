@@ -282,6 +282,39 @@ def accuracy(solver, sample, m_gpu, st_gpu):
     return out
 
 
+def safe_radius_check(solver, cfg, grid, flush, steps=4):
+    """The weighted security-radius guard (RPD_FLAG_SAFE_RADIUS) against
+    the reference's stop test on the same diagram: the cells whose results
+    differ, each solve's total mass against the domain volume (the cells of
+    a correct diagram partition it), and the solve time of both."""
+    import torch
+
+    import rpd
+
+    out = {}
+    res = {}
+    for name, flags in (("reference_test", 0), ("guard", rpd.FLAG_SAFE_RADIUS)):
+        p = rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"],
+                               flags=rpd.FLAG_FRESH_NEIGHBOURS | flags)
+        solver.launch(p)
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            solver.launch(p)
+            ms.append(solver.stats()["total_ms"])
+        m, st = solver.moments().copy(), solver.status().copy()
+        res[name] = (m, st)
+        e = {"ms_per_step": float(np.median(ms)), "failed_cells": int(((st != 4) & (st != 6)).sum())}
+        if grid is not None:
+            e["total_mass_rel_err_vs_domain"] = float(abs(m[st == 4, 3].sum() / grid.getVolume() - 1.0))
+        out[name] = e
+    (m0, s0), (m1, s1) = res["reference_test"], res["guard"]
+    out["cells_that_differ"] = int(((m0 != m1).any(1) | (s0 != s1)).sum())
+    out["status_differ"] = int((s0 != s1).sum())
+    return out
+
+
 def precision_modes(solver, cfg, sample, flush, steps=6, warmup=3):
     """The clipping loop in each arithmetic (rpd_params.precision) on the
     same resident diagram: device time per solve, cells/s, the escalated
@@ -538,6 +571,7 @@ def run_ours(args, cfg, rank, world, local):
         sample = OracleSample(x, grid, cfg, target_s=args.cpu_seconds)
         line["accuracy"] = acc = accuracy(solver, sample, m_gpu, st_gpu)
         line["precision_modes"] = precision_modes(solver, cfg, sample, flush)
+        line["safe_radius"] = safe_radius_check(solver, cfg, grid, flush)
         # the reference algorithm's FP64 work (its counts on the oracle
         # sample) over the whole solve: work this engine mostly does not do
         # (cached radii, the outside probe), so a reference-equivalent rate

@@ -55,6 +55,8 @@ void usage(const char *argv0) {
             << "\t--keepVolume=v: cells with volume below v are empty (default 1)\n"
             << "\t--keepDist2=d: with --grid, keep the used cells and d rings around them (default 0; -1 all)\n"
             << "\t--hessian: compute the facet-area rows (--H=h facets per row, default 50; --HC=1|4)\n"
+            << "\t--safeRadius: stop clipping on the weighted security-radius guard\n"
+            << "\t--precision=fp64|mixed|fp32: arithmetic of the clipping loop (default fp64)\n"
             << "\t--printInvariants --checkGrid --debug\n";
 }
 
@@ -68,7 +70,8 @@ int main(int argc, char **argv) {
   std::string save_binary;
   double keep_volume = 1;
   int keep_dist2 = 0;  // test_voronoi's final keep distance (Options.cpp:42, test_voronoi.cpp:38)
-  bool hessian = false;
+  bool hessian = false, safe_radius = false;
+  int precision = RPD_PRECISION_FP64;
   int H = 50, HC = 1;  // Options.cpp:22-23
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i], val;
@@ -96,6 +99,11 @@ int main(int argc, char **argv) {
     else if (a == "--loadBinaryPoints") load_binary = true;
     else if (a == "--saveBinaryPoints") save_binary = need();
     else if (a == "--hessian") hessian = true;
+    else if (a == "--safeRadius") safe_radius = true;
+    else if (a == "--precision") {
+      const std::string v = need();
+      precision = v == "mixed" ? RPD_PRECISION_MIXED : (v == "fp32" ? RPD_PRECISION_FP32 : RPD_PRECISION_FP64);
+    }
     else if (a == "--H") H = std::atoi(need().c_str());
     else if (a == "--HC") HC = std::atoi(need().c_str());
     else if (a == "--printInvariants") invariants = true;
@@ -138,6 +146,8 @@ int main(int argc, char **argv) {
   algo.m_keepVolume = keep_volume;
   algo.m_H = hessian ? H : 0;  // Options.cpp:269-270
   algo.m_HC = HC;
+  algo.m_safeRadius = safe_radius;
+  algo.m_precision = precision;
   algo.setInputPoints(pts);
   if (has_grid) algo.setGrid(grid);
   std::vector<double> bary;

@@ -44,6 +44,7 @@ struct DiagStatic {
   const int *wmin;  // the smallest weight of the seeds that are not walls (float_to_ordered)
   int T_ahead;      // first pass: triangle overflows up to this count parked at once (0: off)
   int probe;        // 1: the outside probe settles the seeds it can before the first pass
+  int safe_radius;  // the weighted security-radius guard (RPD_FLAG_SAFE_RADIUS)
   float cube_eps;
   DevGrid grid;
   int *status;
@@ -278,6 +279,7 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     a.early_out = g.early_out;
     a.wmin = g.wmin;
     a.inner_apex = g.inner_apex;
+    a.safe_radius = g.safe_radius;
     a.grid = g.grid;
     a.status = g.status;
     a.out = g.out;
@@ -502,6 +504,7 @@ int describe(rpd_batch *b, std::vector<DiagStatic> &out) {
                     : 0;
     if (g.T_ahead <= p.T) g.T_ahead = 0;
     g.inner_apex = (p.flags & RPD_FLAG_REFERENCE_APEX) ? 0 : 1;
+    g.safe_radius = (p.flags & RPD_FLAG_SAFE_RADIUS) ? 1 : 0;
     g.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
     // the outside probe, as rpd_solver_launch runs it on a launch with fresh
     // neighbours (every replay computes its neighbours afresh): with a domain
@@ -543,7 +546,7 @@ int capture(rpd_batch *b) {
   const std::vector<DiagStatic> &G = b->statics;
   long long cells = 0, table = 0;
   int Kmin = kMaxK, Kmax = 0, Pmax = 0, Vmax = 0, Tmax = 0, J = 0;
-  bool any_grid = false, any_plain = false, defer = true;
+  bool any_grid = false, any_plain = false, defer = true, any_safe = false;
   bool class_used[kKnnClasses] = {};
   long class_rows[kKnnClasses] = {};
   long rows_grid0 = 0, rows_plain0 = 0;  // the first pass's rows
@@ -560,6 +563,7 @@ int capture(rpd_batch *b) {
     Tmax = std::max(Tmax, g.T0);
     J = std::max(J, g.max_extra);
     (g.grid.size > 0 ? any_grid : any_plain) = true;
+    if (g.safe_radius) any_safe = true;
     if (b->params[d].flags & RPD_FLAG_NO_DEFER) defer = false;
     for (int c = 0; c < kKnnClasses; ++c)
       if (knn_slots(g.K0) == kKnnClassSlots[c]) {
@@ -780,6 +784,7 @@ int capture(rpd_batch *b) {
     cb.rows_grid = j == 0 && !nprobe ? rows_grid0 : -1;
     cb.rows_plain = j == 0 ? rows_plain0 : -1;
     cb.work = b->work.as<int>();
+    cb.safe = any_safe;
     if ((e = cell_batch_launch(cb, st, ctx->sm_count, &launches)) != cudaSuccess) return fail(e, "batch cells");
     // failing cells of the pass's diagrams
     k_fail_flags_batch<<<flat_blocks, 256, 0, st>>>(ds, sts, pl.rc_start, nd, b->f0.as<int>(), b->f1.as<int>());

@@ -10,6 +10,7 @@ bool cell_caps_fit(int P, int V, int T, bool grid) { return warps_per_block_for(
 
 cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches) {
   if (b.ndiag <= 0) return cudaSuccess;
+  if (b.safe) return cell_batch_launch_safe(b, st, sm_count, launches);
   if (b.P > kMaxP || b.V > kMaxV || b.T > kMaxT || b.P < 7 || b.V < 8) return cudaErrorInvalidValue;
   const Layout Lg = make_layout(b.P, b.V, b.T, true, 0, b.T_slot), Lp = make_layout(b.P, b.V, b.T, false);
   if (b.defer.slots && (b.defer.slot_bytes < slot_bytes_for(Lg, Lg.T) || b.defer.max_chunks * b.defer.chunk < Lg.T))
@@ -27,6 +28,7 @@ size_t defer_slot_bytes(int P, int V, int T) { return slot_bytes_for(make_layout
 cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count, int *launches) {
   if (a.num <= 0) return cudaSuccess;
   if (a.precision != 0) return cell_launch_prec(a, st, sm_count, launches);
+  if (a.safe_radius) return cell_launch_safe(a, st, sm_count, launches);
   if (a.P > kMaxP || a.V > kMaxV || a.T > kMaxT || a.P < 7 || a.V < 8) return cudaErrorInvalidValue;
   if (a.hess && (a.defer.slots || a.H < 1 || (a.HC != 1 && a.HC != 4))) return cudaErrorInvalidValue;
   if (a.T_ahead > kMaxT || (a.T_ahead > a.T && (!a.defer.slots || a.hess))) return cudaErrorInvalidValue;

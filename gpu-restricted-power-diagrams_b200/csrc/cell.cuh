@@ -87,6 +87,7 @@ struct CellLaunch {
   const int *wmin = nullptr;       // the smallest weight of the seeds that are not walls
                                    // (float_to_ordered); null: no early exit
   int inner_apex = 1;              // cone apex at a grid corner inside the cell when there is one
+  int safe_radius = 0;             // the weighted security-radius guard instead of the reference's test
   DevGrid grid;                    // grid.size == 0: no domain
   int *status = nullptr;           // n, stored order
   double4 *out = nullptr;          // n, stored order: (m*x, m*y, m*z, m)
@@ -132,8 +133,10 @@ size_t defer_slot_bytes(int P, int V, int T);
 // k_cell over the rows; with a domain and a defer queue, also the chunked
 // boundary-triangle kernel and the per-cell reduction (3 launches).
 cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count = 148, int *launches = nullptr);
-// The same for a.precision > 0 (cell_prec.cu).
+// The same for a.precision > 0 (cell_prec.cu), and for FP64 clipping with
+// the weighted security-radius guard (a.safe_radius; cell_safe.cu).
 cudaError_t cell_launch_prec(const CellLaunch &a, cudaStream_t st, int sm_count, int *launches);
+cudaError_t cell_launch_safe(const CellLaunch &a, cudaStream_t st, int sm_count, int *launches);
 
 // Outside probe of a first pass with a domain.  The seeds of the 3x3x3 bins
 // around a seed's own are a subset of all seeds, so their bisectors bound a
@@ -187,7 +190,10 @@ struct CellBatch {
   // is made (one warp per row), else -1 (persistent launches)
   long rows_grid = -1, rows_plain = -1;
   int *work = nullptr;  // one device int: the row counter of persistent launches (optional)
+  bool safe = false;    // a diagram uses the weighted security-radius guard (its launch record decides)
 };
 cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches = nullptr);
+// The same with the guard compiled in (cell_safe.cu).
+cudaError_t cell_batch_launch_safe(const CellBatch &b, cudaStream_t st, int sm_count, int *launches);
 
 }  // namespace rpd

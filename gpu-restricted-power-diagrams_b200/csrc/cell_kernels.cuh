@@ -2240,6 +2240,24 @@ __device__ __forceinline__ bool nonempty_cell(float4 s, unsigned vmask, double d
   return (vmask & 1u) && double(s.w) - double(ordered_to_float(__ldg(wmin))) < 0.999 * d2_nearest;
 }
 
+// The security-radius test: no neighbour past the j-th (at squared distance
+// d2j, the neighbours sorted by distance) can cut the cell of squared radius
+// R2.  The reference's test is the Voronoi one, d2j > 4 R2
+// (ConvexCell.cl:364-382).  With safe_dw >= 0 (CellLaunch::safe_radius; it
+// is w_s - min w, the weights added to the squared distances as the
+// reference adds them) the weighted guard instead: a neighbour at distance
+// d' >= d_j with weight >= min w has its bisector at offset
+// (d'^2 + w' - w_s) / (2 d') >= R -- so it cannot cut the ball of radius R
+// around the seed, which holds the cell -- once d_j > R and
+// d_j^2 - 2 R d_j > w_s - min w (the left side grows with d' past R).
+// Squared, without roots: d_j > R and 2 R d_j < d_j^2 - c hold together when
+// d2j > R2, d2j > c and 4 R2 d2j < (d2j - c)^2 (c = safe_dw >= 0).
+__device__ __forceinline__ bool radius_reached(double d2j, double R2, double safe_dw) {
+  if (!(safe_dw >= 0.0)) return d2j > 4.0 * R2;
+  const double e = d2j - safe_dw;
+  return d2j > R2 && e > 0.0 && 4.0 * R2 * d2j < e * e;
+}
+
 // The vertex capacity a cell of this launch works with.  A batched launch's
 // layout may hold more vertices than a diagram's cap (it is sized for every
 // diagram); capacity-dependent choices follow the diagram's own cap, so a
@@ -2251,7 +2269,10 @@ __device__ __forceinline__ int vertex_capacity(const CellLaunch &a, const Layout
 // One row of a cell launch (one warp): clip, restrict, integrate, write.
 // `only_status` >= 0: skip the row unless its cell has that status; vc:
 // the vertex capacity (vertex_capacity).
-template <int VS, bool GRID, bool INL, int PREC = 0>
+// SAFE: 1 -- the launch record's safe_radius selects the weighted
+// security-radius guard (radius_reached); 0 -- the reference's test, compiled
+// without the guard (its code costs the default clipping loop ~5%).
+template <int VS, bool GRID, bool INL, int PREC = 0, int SAFE = 0>
 __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, unsigned char *wsmem, int row,
                                          int only_status, int vc, int lane) {
   WarpCell w = bind(wsmem, L);
@@ -2299,6 +2320,15 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
   bool reached = false, exhausted = false, outside = false;
   const bool early = GRID && a.early_out && a.grid.sat != nullptr && a.wmin != nullptr && a.border_d == 0;
   double plain2 = early ? plain_radius2(a.grid, s, lane) : -1.0;
+  // the weighted security-radius guard (radius_reached): w_s - min w when
+  // on (computed where used, so the default loop carries nothing), else -1
+  auto safe_dw = [&]() -> double {
+    if constexpr (SAFE) {
+      return a.safe_radius && a.wmin ? fmax(0.0, double(s.w) - double(ordered_to_float(__ldg(a.wmin)))) : -1.0;
+    } else {
+      return -1.0;
+    }
+  };
   for (int i0 = 0; i0 < a.K && status == kSuccess && !reached && !exhausted && !outside; i0 += 32) {
     // every lane builds the bisector of one neighbour, in double
     const int i = i0 + lane;
@@ -2360,7 +2390,7 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
             break;
           }
         }
-        if (d2j > 4.0 * R2) {
+        if (radius_reached(d2j, R2, safe_dw())) {
           reached = true;
           break;
         }
@@ -2385,17 +2415,19 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
             }
           }
         }
+        // the test is monotone in R2: reached at the upper bound means
+        // reached, not reached at the lower bound means not
         bool done;
-        if (PREC == 2 || d2j > 4.0 * double(R2hi)) {
-          done = d2j > 4.0 * double(R2hi);
-        } else if (d2j <= 4.0 * double(R2lo)) {
+        if (PREC == 2 || radius_reached(d2j, double(R2hi), safe_dw())) {
+          done = radius_reached(d2j, double(R2hi), safe_dw());
+        } else if (!radius_reached(d2j, double(R2lo), safe_dw())) {
           done = false;
         } else {
           if (R2 < 0.0) {
             R2 = radius2_exact<VS>(w, lane);
             ++esc[kEscRadii];
           }
-          done = d2j > 4.0 * R2;
+          done = radius_reached(d2j, R2, safe_dw());
         }
         if (done) {
           reached = true;
@@ -2489,13 +2521,14 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
   }
 }
 
-template <int VS, bool GRID, bool INL, int PREC = 0>
+template <int VS, bool GRID, bool INL, int PREC = 0, int SAFE = 0>
 __global__ void __launch_bounds__(128, 5) k_cell(const __grid_constant__ CellLaunch a, const __grid_constant__ Layout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= a.num) return;
-  cell_row<VS, GRID, INL, PREC>(a, L, smem + size_t(threadIdx.x >> 5) * L.total, row, a.only_status, L.Vc, lane);
+  cell_row<VS, GRID, INL, PREC, SAFE>(a, L, smem + size_t(threadIdx.x >> 5) * L.total, row, a.only_status, L.Vc,
+                                      lane);
 }
 
 // Cage test of the outside probe: bit i of the result is set when the
@@ -2691,7 +2724,7 @@ __global__ void __launch_bounds__(128, 6) k_probe_batch(const ProbeLaunch *__res
 // time from this counter (persistent launches of unknown row counts, so a
 // warp that drew heavy rows does not hold the launch back); null: warp w
 // takes rows w, w + warps, ... (a grid of one warp per row takes one each).
-template <int VS, bool GRID, bool INL>
+template <int VS, bool GRID, bool INL, int SAFE = 0>
 __global__ void __launch_bounds__(128, 5)
     k_cell_batch(const CellLaunch *__restrict__ descs, const int *__restrict__ start, int ndiag,
                  const __grid_constant__ Layout L, int only_status, const int *__restrict__ park_counter,
@@ -2710,7 +2743,7 @@ __global__ void __launch_bounds__(128, 5)
   while (r < total) {
     const int d = owner_of_row(start, ndiag, r);
     const CellLaunch &a = descs[d];
-    cell_row<VS, GRID, INL>(a, L, wsmem, r - start[d], only_status, vertex_capacity(a, L), lane);
+    cell_row<VS, GRID, INL, 0, SAFE>(a, L, wsmem, r - start[d], only_status, vertex_capacity(a, L), lane);
     __syncwarp();  // the warp's shared memory is reused by its next row
     if (work) {
       r = lane == 0 ? atomicAdd(work, 1) : 0;
@@ -2911,7 +2944,7 @@ int warps_per_block_for(const Layout &L) {
   return w;
 }
 
-template <int VS, int PREC = 0>
+template <int VS, int PREC = 0, int SAFE = 0>
 cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int sm_count, int *launches) {
   const int warps_per_block = warps_per_block_for(L);
   if (warps_per_block == 0) return cudaErrorInvalidValue;
@@ -2920,9 +2953,9 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
   cudaError_t e;
   if (a.grid.size > 0 && a.defer.slots) {
     // every boundary cell parks; the chunked kernel does the triangles
-    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, false, PREC>), smem);
+    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, false, PREC, SAFE>), smem);
     if (e != cudaSuccess) return e;
-    k_cell<VS, true, false, PREC><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    k_cell<VS, true, false, PREC, SAFE><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (a.after_cell) cudaEventRecord(a.after_cell, st);
     e = allow_smem(reinterpret_cast<const void *>(k_cone<VS>), smem);
     if (e != cudaSuccess) return e;
@@ -2930,15 +2963,15 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
     k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a, L);
     if (launches) *launches += 3;
   } else if (a.grid.size > 0) {
-    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, true, PREC>), smem);
+    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, true, PREC, SAFE>), smem);
     if (e != cudaSuccess) return e;
-    k_cell<VS, true, true, PREC><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    k_cell<VS, true, true, PREC, SAFE><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (a.after_cell) cudaEventRecord(a.after_cell, st);
     if (launches) ++*launches;
   } else {
-    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, false, true, PREC>), smem);
+    e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, false, true, PREC, SAFE>), smem);
     if (e != cudaSuccess) return e;
-    k_cell<VS, false, true, PREC><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
+    k_cell<VS, false, true, PREC, SAFE><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (a.after_cell) cudaEventRecord(a.after_cell, st);
     if (launches) ++*launches;
   }
@@ -2957,14 +2990,14 @@ int resident_blocks(Kernel k, int threads, size_t smem, int sm_count) {
 // rows >= 0: the launch's row count is known: one warp per row.  Else a
 // persistent launch; with `work`, rows are taken from that counter (zeroed
 // here, on the stream).
-template <int VS, bool GRID, bool INL>
+template <int VS, bool GRID, bool INL, int SAFE = 0>
 cudaError_t batch_cells(const CellLaunch *descs, const int *start, int ndiag, const Layout &L, int only_status,
                         const int *park_counter, int park_capacity, long rows, int *work, cudaStream_t st,
                         int sm_count) {
   const int wpb = warps_per_block_for(L);
   if (wpb == 0) return cudaErrorInvalidValue;
   const size_t smem = size_t(L.total) * wpb;
-  auto k = k_cell_batch<VS, GRID, INL>;
+  auto k = k_cell_batch<VS, GRID, INL, SAFE>;
   cudaError_t e = allow_smem(reinterpret_cast<const void *>(k), smem);
   if (e != cudaSuccess) return e;
   int blocks;
@@ -2984,19 +3017,19 @@ cudaError_t record_after_cell(const CellBatch &b, cudaStream_t st) {
   return b.after_cell ? cudaEventRecordWithFlags(b.after_cell, st, cudaEventRecordExternal) : cudaSuccess;
 }
 
-template <int VS>
+template <int VS, int SAFE = 0>
 cudaError_t launch_batch_vs(const CellBatch &b, const Layout &Lg, const Layout &Lp, cudaStream_t st, int sm_count,
                             int *launches) {
   cudaError_t e;
   if (b.start_plain) {
-    if ((e = batch_cells<VS, false, true>(b.descs_inline, b.start_plain, b.ndiag, Lp, -1, nullptr, 0, b.rows_plain,
+    if ((e = batch_cells<VS, false, true, SAFE>(b.descs_inline, b.start_plain, b.ndiag, Lp, -1, nullptr, 0, b.rows_plain,
                                           b.work, st, sm_count)) != cudaSuccess)
       return e;
     if (launches) ++*launches;
   }
   if (!b.start_grid) return record_after_cell(b, st);
   if (!b.defer.slots) {
-    if ((e = batch_cells<VS, true, true>(b.descs_inline, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, b.rows_grid,
+    if ((e = batch_cells<VS, true, true, SAFE>(b.descs_inline, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, b.rows_grid,
                                          b.work, st, sm_count)) != cudaSuccess)
       return e;
     if (launches) ++*launches;
@@ -3004,7 +3037,7 @@ cudaError_t launch_batch_vs(const CellBatch &b, const Layout &Lg, const Layout &
   }
   // every boundary cell parks; the chunked kernel does the triangles, then
   // the cells that found the queue full run again inline
-  if ((e = batch_cells<VS, true, false>(b.descs, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, b.rows_grid, b.work, st,
+  if ((e = batch_cells<VS, true, false, SAFE>(b.descs, b.start_grid, b.ndiag, Lg, -1, nullptr, 0, b.rows_grid, b.work, st,
                                         sm_count)) != cudaSuccess)
     return e;
   if ((e = record_after_cell(b, st)) != cudaSuccess) return e;
@@ -3014,7 +3047,7 @@ cudaError_t launch_batch_vs(const CellBatch &b, const Layout &Lg, const Layout &
   if ((e = allow_smem(reinterpret_cast<const void *>(kc), smem)) != cudaSuccess) return e;
   kc<<<resident_blocks(kc, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(b.descs, b.defer, Lg);
   k_cone_finish_batch<<<sm_count * 4, 128, 0, st>>>(b.descs, b.defer, Lg);
-  if ((e = batch_cells<VS, true, true>(b.descs_inline, b.start_grid, b.ndiag, Lg, kParkOverflow, b.defer.counters,
+  if ((e = batch_cells<VS, true, true, SAFE>(b.descs_inline, b.start_grid, b.ndiag, Lg, kParkOverflow, b.defer.counters,
                                        b.defer.capacity, -1, b.work, st, sm_count)) != cudaSuccess)
     return e;
   if (launches) *launches += 4;

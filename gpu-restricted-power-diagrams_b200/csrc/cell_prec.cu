@@ -7,13 +7,14 @@ namespace rpd {
 
 namespace {
 
+// (the weighted security-radius guard is decided per launch record here)
 template <int PREC>
 cudaError_t launch_prec(const CellLaunch &a, const Layout &L, int vs, cudaStream_t st, int sm_count, int *launches) {
-  if (vs <= 2) return launch_vs<2, PREC>(a, L, st, sm_count, launches);
-  if (vs <= 3) return launch_vs<3, PREC>(a, L, st, sm_count, launches);
-  if (vs <= 4) return launch_vs<4, PREC>(a, L, st, sm_count, launches);
-  if (vs <= 6) return launch_vs<6, PREC>(a, L, st, sm_count, launches);
-  return launch_vs<8, PREC>(a, L, st, sm_count, launches);
+  if (vs <= 2) return launch_vs<2, PREC, 1>(a, L, st, sm_count, launches);
+  if (vs <= 3) return launch_vs<3, PREC, 1>(a, L, st, sm_count, launches);
+  if (vs <= 4) return launch_vs<4, PREC, 1>(a, L, st, sm_count, launches);
+  if (vs <= 6) return launch_vs<6, PREC, 1>(a, L, st, sm_count, launches);
+  return launch_vs<8, PREC, 1>(a, L, st, sm_count, launches);
 }
 
 }  // namespace

@@ -460,6 +460,7 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   a.early_out = early_out && !(s->used_on && s->keep_volume <= 0.0) ? 1 : 0;
   a.wmin = s->wmin.as<int>();
   a.inner_apex = s->inner_apex ? 1 : 0;
+  a.safe_radius = (s->launch_flags & RPD_FLAG_SAFE_RADIUS) ? 1 : 0;
   if (s->used_on) {
     a.used = s->used.as<unsigned char>();
     a.keep_volume = s->keep_volume;

@@ -133,6 +133,7 @@ FLAG_FRESH_NEIGHBOURS = 32
 FLAG_NO_PROBE = 64
 FLAG_NO_T_AHEAD = 128
 FLAG_KNN_WARP = 256
+FLAG_SAFE_RADIUS = 1024
 FLAG_KNN_THREAD = 512
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1

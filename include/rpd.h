@@ -208,6 +208,14 @@ rpd_grid *rpd_solver_export_grid(rpd_solver *s, int *err);
                                        to the retry passes instead of restricting at
                                        once the cells the retries would settle (same
                                        results) */
+#define RPD_FLAG_SAFE_RADIUS 1024u  /* --safeRadius: stop clipping on the weighted security-radius
+                                       guard instead of the reference's Voronoi test d^2 > 4 R^2
+                                       (ConvexCell.cl:364-382): with the neighbours sorted by
+                                       distance d and the weights added to squared distances, no
+                                       later neighbour cuts the cell once d_j > R and
+                                       d_j^2 - 2 R d_j > w_s - min w.  A cell the reference's test
+                                       stops early on comes out exact (different from the
+                                       reference's); equal weights give the reference's test */
 #define RPD_FLAG_KNN_WARP 256u      /* neighbour search with a warp per seed (bitonic
                                        merges) for every K (same results) */
 #define RPD_FLAG_KNN_THREAD 512u    /* neighbour search with a thread per seed (a

@@ -157,6 +157,8 @@ class VoroAlgo {
     p.keep_volume = m_keepVolume;
     p.hessian_h = m_H;
     p.hessian_hc = m_HC;
+    p.precision = m_precision;
+    if (m_safeRadius) p.flags |= RPD_FLAG_SAFE_RADIUS;
     if (rpd_solver_launch(s_, &p) != RPD_OK) {
       if (m_debug) fprintf(stderr, "VoroAlgo::launch: %s\n", ctx_->error().c_str());
       return false;
@@ -248,6 +250,11 @@ class VoroAlgo {
   // values per facet (1 or 4)
   int m_H = 0;
   int m_HC = 1;
+  // no counterparts in VoroAlgo: the clipping arithmetic (RPD_PRECISION_*, in
+  // place of the compile-time VHSAlgo / USE_DOUBLE choice) and the weighted
+  // security-radius guard (RPD_FLAG_SAFE_RADIUS)
+  int m_precision = RPD_PRECISION_FP64;
+  bool m_safeRadius = false;
 
  private:
   std::shared_ptr<Context> ctx_;

@@ -74,6 +74,8 @@ def test_batch_equals_solves_alone(rpd):
             p.flags |= rpd.FLAG_REFERENCE_APEX
         if i == 9:
             p.flags |= rpd.FLAG_NO_PROBE
+        if i == 10:
+            p.flags |= rpd.FLAG_SAFE_RADIUS
         params.append(p)
     b = rpd.Batch(solvers, params)
     b.launch()

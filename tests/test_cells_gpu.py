@@ -246,3 +246,35 @@ def test_cell_in_the_box_margin_has_no_start_corner(rpd):
     met, got, gst, ref, rst, _ = run_case(rpd, x.astype(np.float32), grid=g, K=30, P=30, V=40, T=100)
     assert gst[-1] == 7 and rst[-1] == 7
     assert_parity(met)
+
+
+def test_safe_radius_guard(rpd):
+    """RPD_FLAG_SAFE_RADIUS: with weights the reference's Voronoi stop test
+    (d^2 > 4 R^2) can end a cell before a lighter far neighbour cuts it, so
+    the cells overlap and their masses over-count the domain; with the
+    weighted guard they partition it to FP64 rounding.  Without weights the
+    guard is the reference's test."""
+    g = rpd.Grid.blob(40, 5, 2)
+    vol = g.getVolume()
+    x = jittered(24, seed=12, weights=True)
+    h = 1000.0 / 24
+    x[:, 3] = np.random.default_rng(3).uniform(0, 0.6 * h * h, len(x)).astype(np.float32)
+    kw = dict(K=50, P=40, V=60, T=100)
+    m0, s0, _ = solve_gpu(rpd, x, g, **kw)
+    m1, s1, _ = solve_gpu(rpd, x, g, flags=rpd.FLAG_SAFE_RADIUS, **kw)
+    assert (s0 == 4).all() and (s1 == 4).all()
+    err0 = abs(m0[:, 3].sum() / vol - 1)
+    err1 = abs(m1[:, 3].sum() / vol - 1)
+    differ = int((m0 != m1).any(1).sum())
+    print("reference test", err0, "guard", err1, "cells that differ", differ)
+    assert err1 < 1e-12 and err0 > 100 * err1 and differ > 0
+    # the reference's test equals the oracle (the reference algorithm)
+    ref, rst = oracle.solve(x.astype(np.float64), grid=oracle_grid(g), use_double=True, knn_mode=1, **kw)
+    assert_parity(compare(m0, s0, ref, rst))
+    # equal weights: the same cells
+    y = x.copy()
+    y[:, 3] = 0
+    ma, sa, _ = solve_gpu(rpd, y, g, **kw)
+    mb, sb, _ = solve_gpu(rpd, y, g, flags=rpd.FLAG_SAFE_RADIUS, **kw)
+    assert np.array_equal(sa, sb)
+    assert np.abs(ma - mb).max() <= 1e-9 * np.abs(ma).max()
