@@ -384,17 +384,17 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
 // context's choice for K, made the first time K comes up with enough rows to
 // tell: both variants run on the first rows (one untimed round, one timed
 // with events), into `out`, which the real launch then overwrites; both give
-// the same lists, so only their speed differs.  Too few rows for a trial: a
-// thread per seed up to K = 64.
+// the same lists, so only their speed differs.  Fewer rows than a trial
+// takes (retry passes): a warp per seed -- a thread per seed leaves most of
+// the GPU idle there and each row's search serial (0.45 ms for 144 rows).
 int knn_variant_for(rpd_solver *s, const int *ids, int num, int K, unsigned *out, unsigned flags) {
   if (flags & RPD_FLAG_KNN_WARP) return kKnnWarp;
   if (flags & RPD_FLAG_KNN_THREAD) return K <= kKnnThreadMaxK ? kKnnThread : kKnnWarp;
-  if (K > kKnnThreadMaxK) return kKnnWarp;
+  constexpr int kTrialRows = 16384;
+  if (K > kKnnThreadMaxK || num < kTrialRows) return kKnnWarp;
   rpd_context *ctx = s->ctx;
   if (ctx->knn_variant[K] >= 0) return ctx->knn_variant[K];
-  constexpr int kTrialRows = 16384;
-  if (num < kTrialRows / 2) return K <= 64 ? kKnnThread : kKnnWarp;
-  const int m = std::min(num, kTrialRows);
+  const int m = kTrialRows;
   cudaStream_t st = ctx->stream;
   Events<4> ev;
   float ms[2] = {0.f, 0.f};

@@ -220,9 +220,10 @@ rpd_grid *rpd_solver_export_grid(rpd_solver *s, int *err);
                                        merges) for every K (same results) */
 #define RPD_FLAG_KNN_THREAD 512u    /* neighbour search with a thread per seed (a
                                        shared-memory heap) for K <= 128 (same results).
-                                       Without either flag each context picks the
-                                       faster for each K by a timed trial the first
-                                       time K comes up (rpd_stats.pass_knn_variant) */
+                                       Without either flag, searches of at least 16K
+                                       rows use the variant each context picks for K by
+                                       a timed trial the first time K comes up, smaller
+                                       ones a warp per seed (rpd_stats.pass_knn_variant) */
 
 /* VoroAlgo's knobs (voronoi.h:199-246; defaults of Options.cpp:22-28). */
 typedef struct rpd_params {
