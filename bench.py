@@ -394,11 +394,12 @@ def run_reference(args, cfg, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def aggregate_over_ranks(ms, e2e_s, n, world, device):
+def aggregate_over_ranks(ms, e2e_s, n, world, device, diagrams=None):
     """Whole-job numbers of one timed run: each rank solved its own n-seed
-    diagram; the job's step time is the slowest rank's (max over ranks), and
-    the throughput counts the cells of all ranks.  Returns (ms, e2e_s,
-    cells_per_s, e2e_cells_per_s)."""
+    diagram (or, with diagrams=1, the ranks split one); the job's step time
+    is the slowest rank's (max over ranks), and the throughput counts the
+    cells of every diagram.  Returns (ms, e2e_s, cells_per_s,
+    e2e_cells_per_s)."""
     if world > 1:
         import torch
         import torch.distributed as dist
@@ -406,7 +407,8 @@ def aggregate_over_ranks(ms, e2e_s, n, world, device):
         t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, e2e_s = float(t[0].item()), float(t[1].item())
-    return ms, e2e_s, n * world / (ms / 1e3), n * world / e2e_s
+    d = world if diagrams is None else diagrams
+    return ms, e2e_s, n * d / (ms / 1e3), n * d / e2e_s
 
 
 def run_ours(args, cfg, rank, world, local):
@@ -423,7 +425,8 @@ def run_ours(args, cfg, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     ctx = rpd.Context(local)
-    x = make_seeds(cfg, rank)
+    split = args.split and world > 1
+    x = make_seeds(cfg, 0 if split else rank)  # --split: one diagram over the ranks
     t0 = time.perf_counter()
     grid = make_grid(cfg)
     setup = {"grid_host_build_s": time.perf_counter() - t0}
@@ -459,15 +462,33 @@ def run_ours(args, cfg, rank, world, local):
 
     clocks = ClockSampler(local)
     step_ms, cell_ms, knn_ms, launches, npasses, probe_ms, probe_out = [], [], [], [], [], [], []
+    if split:
+        from rpd import split as rsplit
+
+        # device events on the engine's stream around the whole split step
+        # (part solve, per-pass reductions, the gather and the install)
+        eng = torch.cuda.ExternalStream(rpd.lib().rpd_context_stream(ctx.h))
+        for _ in range(args.warmup):
+            rsplit.solve_split(solver, params=params)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
-        solver.launch(params)
-        st = solver.stats()
-        step_ms.append(st["total_ms"])
+        if split:
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(eng)
+            rsplit.solve_split(solver, params=params)
+            e1.record(eng)
+            e1.synchronize()
+            st = solver.stats()
+            step_ms.append(e0.elapsed_time(e1))
+        else:
+            solver.launch(params)
+            st = solver.stats()
+            step_ms.append(st["total_ms"])
         cell_ms.append(st["passes"][0]["cell_kernel_ms"])
         knn_ms.append(st["passes"][0]["knn_ms"])
         probe_ms.append(st["probe_ms"])
@@ -497,11 +518,14 @@ def run_ours(args, cfg, rank, world, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ctx.check(rpd.lib().rpd_solver_set_points(solver.h, rpd._ptr(xa), n, rpd.RPD_HOST))
-        solver.launch(params)
+        if split:
+            rsplit.solve_split(solver, params=params)
+        else:
+            solver.launch(params)
         ctx.check(rpd.lib().rpd_solver_get_moments(solver.h, rpd._ptr(oa), rpd.RPD_HOST))
         e2e_s.append(time.perf_counter() - t0)
     e2e_t = sum(e2e_s) / len(e2e_s)
-    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda")
+    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda", 1 if split else None)
 
     # roofline of the dominant kernel (the cell kernel of the first pass),
     # timed live with CUDA events: it is bound by instruction issue (ncu:
@@ -546,11 +570,14 @@ def run_ours(args, cfg, rank, world, local):
                        "frac": achieved_hbm / peak_hbm, "alg_bytes_per_launch": alg_bytes}
     line = {
         "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "f64 geometry on f32 seeds (FP64 cofactor predicates and integration)",
         "data": "synthetic",
         "config": {"workload": args.config, "description": cfg["desc"], "n_seeds_per_gpu": n,
-                   "parallelism": f"{world} independent diagrams, one per GPU",
+                   "parallelism": (f"one diagram split over {world} GPUs (stored-seed ranges, per-pass "
+                                   "all-reduce of the retry counts, one all-gather of the results)") if split
+                                  else f"{world} independent diagrams, one per GPU",
                    "l2": "flushed between steps (256 MB write, untimed)"},
         "e2e": {"value": e2e_value, "unit": "cells/s", "h2d_bytes_per_step": int(x.nbytes),
                 "d2h_bytes_per_step": int(n * 32),
@@ -706,7 +733,7 @@ def run_batch(args, cfg, rank, world, local):
         e2e_s.append(time.perf_counter() - t0)
     e2e_t = sum(e2e_s) / len(e2e_s)
     recaptured = batch.stats()["captures"] - bstats["captures"]
-    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda")
+    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda", 1 if split else None)
     seq_rate = n / min(seq_wall)
     seq_dev_rate = n / (min(seq_dev) / 1e3)
 
@@ -1048,6 +1075,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--split", action="store_true",
+                    help="single-diagram configs with --gpus N > 1: the ranks split one diagram (strong scaling) "
+                         "instead of solving one each")
     ap.add_argument("--slots", type=int, default=None, help="serving configs: concurrent slots (default: the config's)")
     ap.add_argument("--diagrams", type=int, default=None,
                     help="batch configs: solve only the first N diagrams (small cases for profiling)")

@@ -149,7 +149,8 @@ cudaError_t cell_launch_safe(const CellLaunch &a, cudaStream_t st, int sm_count,
 // solved by the full pass.
 struct ProbeLaunch {
   const float4 *stored = nullptr;  // n seeds in stored (bin) order
-  int n = 0;
+  int n = 0;                       // rows: the stored seeds first .. first + n - 1
+  int first = 0;
   const int *bins = nullptr;       // dim^3 + 1 bin starts of the stored order
   int dim = 0;
   DevGrid grid;                    // with its summed-volume table (grid.sat)

@@ -2577,10 +2577,11 @@ __device__ __forceinline__ unsigned cage_bits(float nx, float ny, float nz, floa
 // vc: the vertex capacity the warp works with (the layout's, or a batched
 // diagram's own, vertex_capacity).
 template <int VS>
-__device__ __forceinline__ void probe_row(const ProbeLaunch &p, const Layout &L, unsigned char *wsmem, int row,
+__device__ __forceinline__ void probe_row(const ProbeLaunch &p, const Layout &L, unsigned char *wsmem, int r,
                                           int vc, int lane) {
   WarpCell w = bind(wsmem, L);
   w.vc = vc;
+  const int row = p.first + r;  // the seed's stored index
   const float4 s = p.stored[row];
   const double plain2 = s.w <= kNoCellLimits ? -1.0 : plain_radius2(p.grid, s, lane);
   bool proven = false;

@@ -132,16 +132,24 @@ struct Events {
   cudaEvent_t operator[](int i) const { return ev[i]; }
 };
 
-// Rows the outside probe left: f[i] = 1 where status is kProbeMiss; f[n] = 0.
-__global__ void k_probe_flags(const int *__restrict__ status, int n, int *__restrict__ f) {
+// Rows the outside probe left among stored seeds first .. first + n - 1:
+// f[i] = 1 where status is kProbeMiss; f[n] = 0.
+__global__ void k_probe_flags(const int *__restrict__ status, int first, int n, int *__restrict__ f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) f[i] = status[i] == kProbeMiss;
+  if (i < n) f[i] = status[first + i] == kProbeMiss;
   else if (i == n) f[i] = 0;
 }
 
-__global__ void k_probe_scatter(int n, const int *__restrict__ f, const int *__restrict__ pos, int *__restrict__ ids) {
+__global__ void k_probe_scatter(int first, int n, const int *__restrict__ f, const int *__restrict__ pos,
+                                int *__restrict__ ids) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && f[i]) ids[pos[i]] = i;
+  if (i < n && f[i]) ids[pos[i]] = first + i;
+}
+
+// ids[i] = first + i (a contiguous range of stored ids).
+__global__ void k_iota(int first, int n, int *__restrict__ ids) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ids[i] = first + i;
 }
 
 template <class T>
@@ -337,11 +345,10 @@ int count_used(rpd_solver *s) {
 // stored ids of the seeds it left into `ids`, ascending; synchronous.  The
 // cage test runs where the plainly-outside ball is at least one mean seed
 // spacing wide, clipping where it is at least 1.5.
-int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
+int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss, int first, int n) {
   rpd_context *ctx = s->ctx;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
-  const int n = s->n;
   const size_t nsc = scan_workspace_ints(n + 1);
   if ((e = s->fail_ws.ensure(sizeof(int) * (2 * size_t(n + 1) + nsc))) != cudaSuccess)
     return map_cuda(ctx, e, "alloc probe ws");
@@ -351,13 +358,14 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
   ProbeLaunch pr;
   pr.stored = s->stored.as<float4>();
   pr.n = n;
+  pr.first = first;
   pr.bins = s->counters.as<int>();
   pr.dim = s->dim;
   pr.grid = s->grid;
   pr.P = P;
   pr.V = V;
   pr.cube_eps = eps;
-  const double spacing = 1000.0 / std::cbrt(double(n));
+  const double spacing = 1000.0 / std::cbrt(double(s->n));
   pr.min_plain_cage = 1.0 * spacing;
   pr.min_plain = 1.5 * spacing;
   pr.wmin = s->wmin.as<int>();
@@ -365,9 +373,9 @@ int run_probe(rpd_solver *s, int P, int V, float eps, int *ids, int &nmiss) {
   pr.out = s->out.as<double4>();
   if ((e = probe_launch(pr, st)) != cudaSuccess) return map_cuda(ctx, e, "probe");
   const int tb = 256;
-  k_probe_flags<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(s->status.as<int>(), n, f);
+  k_probe_flags<<<(n + 1 + tb - 1) / tb, tb, 0, st>>>(s->status.as<int>(), first, n, f);
   if ((e = exclusive_scan(f, pos, n + 1, tiles, st)) != cudaSuccess) return map_cuda(ctx, e, "scan");
-  k_probe_scatter<<<(n + tb - 1) / tb, tb, 0, st>>>(n, f, pos, ids);
+  k_probe_scatter<<<(n + tb - 1) / tb, tb, 0, st>>>(first, n, f, pos, ids);
   cudaEventRecord(ev[1], st);
   int cnt = 0;
   cudaMemcpyAsync(&cnt, pos + n, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -909,7 +917,37 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *gh) {
   return RPD_OK;
 }
 
-int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
+}  // extern "C"
+
+// One part of a diagram split over several solvers (rpd_solver_launch_part):
+// the stored seeds first .. first + count - 1, and the reduction that makes
+// every part's retry schedule the whole diagram's.
+struct PartSpec {
+  int first, count;
+  rpd_part_reduce_fn reduce;
+  void *user;
+};
+
+// The pass schedule's counts combined over the parts: sums (the failing
+// statuses' histogram, the failing cells) and maxima (the largest triangle
+// count parked ahead).  Without parts nothing changes.
+static int reduce_schedule(rpd_solver *s, const PartSpec *part, int hist[kStatusNum], int &n0) {
+  if (!part) return RPD_OK;
+  long long sums[kStatusNum + 1], maxes[1];
+  for (int i = 0; i < kStatusNum; ++i) sums[i] = hist[i];
+  sums[kStatusNum] = n0;
+  maxes[0] = s->ahead_max;
+  if (part->reduce(sums, kStatusNum + 1, maxes, 1, part->user) != 0) {
+    set_error(s->ctx, "part reduction failed");
+    return RPD_ERR_INVALID;
+  }
+  for (int i = 0; i < kStatusNum; ++i) hist[i] = int(sums[i]);
+  n0 = int(sums[kStatusNum]);
+  s->ahead_max = int(maxes[0]);
+  return RPD_OK;
+}
+
+static int launch_impl(rpd_solver *s, const rpd_params *pp, const PartSpec *part) {
   if (!s || s->n <= 0) return RPD_ERR_INVALID;
   rpd_params p;
   if (pp) p = *pp;
@@ -1013,24 +1051,35 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
       !(p.flags & (RPD_FLAG_FIRST_PASS_ONLY | RPD_FLAG_NO_T_AHEAD)))
     T_ahead = t_ahead_cap(p.P, p.K, p.T, p.max_extra_passes);
   int rc;
+  // the cells of this launch: every seed, or a part's stored range
+  const int first = part ? part->first : 0, count = part ? part->count : n;
+  const int *range = nullptr;  // the part's stored ids (null: every seed)
+  if (part) {
+    if ((e = s->ids_range.ensure(sizeof(int) * size_t(std::max(count, 1)))) != cudaSuccess)
+      return map_cuda(ctx, e, "alloc range");
+    if (count > 0) k_iota<<<(count + 255) / 256, 256, 0, st>>>(first, count, s->ids_range.as<int>());
+    range = s->ids_range.as<int>();
+  }
   if (probe) {
     int nmiss = 0;
     int *miss = s->ids_b.as<int>();
-    if ((rc = run_probe(s, p.P, p.V, eps, miss, nmiss)) != RPD_OK) return rc;
+    if ((rc = run_probe(s, p.P, p.V, eps, miss, nmiss, first, count)) != RPD_OK) return rc;
     rc = run_pass(s, miss, nmiss, p.K, p.P, p.V, T0, eps, 0, counters, early, 0, T_ahead, out_domain);
-    s->stats.pass_cells[0] = n;  // the reference's first pass: every seed
+    s->stats.pass_cells[0] = count;  // the reference's first pass: every seed (of the part)
   } else {
-    rc = run_pass(s, nullptr, n, p.K, p.P, p.V, T0, eps, 0, counters, early, 0, T_ahead, out_domain);
+    rc = run_pass(s, range, count, p.K, p.P, p.V, T0, eps, 0, counters, early, 0, T_ahead, out_domain);
   }
   if (rc != RPD_OK) return rc;
   int K = p.K, P = p.P, V = p.V, T = p.T;
   if (!(p.flags & RPD_FLAG_FIRST_PASS_ONLY)) {
     int hist[kStatusNum];
-    int n0 = 0, n1 = 0;
+    int n0 = 0, n1 = 0, n0_all = 0;  // n0: this part's failing cells; n0_all: every part's
     int *A = s->ids_a.as<int>(), *B = s->ids_b.as<int>(), *Cc = s->ids_c.as<int>();
     // extra passes (voronoi.cpp:1311-1376): caps grow x1.5 by failing status
-    if ((rc = recompute_ids(s, nullptr, n, 0, A, Cc, n0, n1, hist)) != RPD_OK) return rc;
-    for (int step = 0; step < p.max_extra_passes && n0 > 0; ++step) {
+    if ((rc = recompute_ids(s, range, count, 0, A, Cc, n0, n1, hist)) != RPD_OK) return rc;
+    n0_all = n0;
+    if ((rc = reduce_schedule(s, part, hist, n0_all)) != RPD_OK) return rc;
+    for (int step = 0; step < p.max_extra_passes && n0_all > 0; ++step) {
       bool relaunch = false;
       if (hist[kVertexOverflow]) { relaunch = true; V = int(V * 1.5); }
       if (hist[kPlaneOverflow]) { relaunch = true; P = int(P * 1.5); }
@@ -1045,6 +1094,8 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
       if ((rc = run_pass(s, Cc, n1, K, P, V, T, eps, out_domain, counters, early)) != RPD_OK) return rc;
       if ((rc = recompute_ids(s, A, n0, 1, B, Cc, n0, n1, hist)) != RPD_OK) return rc;
       std::swap(A, B);
+      n0_all = n0;
+      if ((rc = reduce_schedule(s, part, hist, n0_all)) != RPD_OK) return rc;
     }
   }
   if (s->used_on) {
@@ -1061,7 +1112,7 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   cudaEventRecord(t1, st);
   int *h = s->hist.as<int>();
   cudaMemsetAsync(h, 0, sizeof(int) * 16, st);
-  k_status_hist<<<s->ctx->sm_count, 256, 0, st>>>(s->status.as<int>(), n, h);
+  k_status_hist<<<s->ctx->sm_count, 256, 0, st>>>(s->status.as<int>() + first, count, h);
   s->stats.kernel_launches += 1;
   int hh[16];
   cudaMemcpyAsync(hh, h, sizeof(hh), cudaMemcpyDeviceToHost, st);
@@ -1072,8 +1123,72 @@ int rpd_solver_launch(rpd_solver *s, const rpd_params *pp) {
   for (int i = 0; i < kStatusNum; ++i) s->stats.status_hist[i] = hh[i];
   for (int i = 0; i < RPD_CTR_NUM; ++i) s->stats.counters[i] = c64[i];
   s->stats.knn_candidates = c64[RPD_CTR_NUM];
-  s->have_results = true;
+  s->have_results = !part;  // a part's results are complete once gathered (rpd_solver_set_stored)
   s->launches_since_points++;
+  return RPD_OK;
+}
+
+extern "C" {
+
+int rpd_solver_launch(rpd_solver *s, const rpd_params *p) { return launch_impl(s, p, nullptr); }
+
+int rpd_solver_part_range(int n, int part, int parts, int *first, int *count) {
+  if (n < 0 || parts < 1 || part < 0 || part >= parts || !first || !count) return RPD_ERR_INVALID;
+  const long long per = (static_cast<long long>(n) + parts - 1) / parts;
+  const long long a = std::min<long long>(n, per * part), b = std::min<long long>(n, per * (part + 1));
+  *first = int(a);
+  *count = int(b - a);
+  return RPD_OK;
+}
+
+int rpd_solver_launch_part(rpd_solver *s, const rpd_params *pp, int part, int parts, rpd_part_reduce_fn reduce,
+                           void *user) {
+  if (!s || s->n <= 0 || !reduce) return RPD_ERR_INVALID;
+  rpd_params p;
+  if (pp) p = *pp;
+  else rpd_params_default(&p);
+  if (p.hessian_h > 0 || (s->grid.size > 0 && p.keep_distance >= 0)) {
+    set_error(s->ctx, "a diagram split over parts returns no Hessian rows or used cells");
+    return RPD_ERR_INVALID;
+  }
+  PartSpec spec{0, 0, reduce, user};
+  int rc = rpd_solver_part_range(s->n, part, parts, &spec.first, &spec.count);
+  if (rc != RPD_OK) return rc;
+  return launch_impl(s, &p, &spec);
+}
+
+int rpd_solver_get_stored(rpd_solver *s, double *out4, int *status, int first, int count, rpd_mem where) {
+  if (!s || first < 0 || count < 0 || first + count > s->n || (!out4 && !status)) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const cudaMemcpyKind kind = where == RPD_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  cudaError_t e = cudaSuccess;
+  if (out4 && count)
+    e = cudaMemcpyAsync(out4, s->out.as<double4>() + first, sizeof(double4) * count, kind, st);
+  if (e == cudaSuccess && status && count)
+    e = cudaMemcpyAsync(status, s->status.as<int>() + first, sizeof(int) * count, kind, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return map_cuda(ctx, e, "get stored results");
+}
+
+int rpd_solver_set_stored(rpd_solver *s, const double *out4, const int *status, rpd_mem where) {
+  if (!s || s->n <= 0 || !out4 || !status) return RPD_ERR_INVALID;
+  rpd_context *ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const int n = s->n;
+  if ((e = s->out.ensure(sizeof(double4) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc out");
+  if ((e = s->status.ensure(sizeof(int) * n)) != cudaSuccess) return map_cuda(ctx, e, "alloc status");
+  const cudaMemcpyKind kind = where == RPD_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if ((e = cudaMemcpyAsync(s->out.ptr, out4, sizeof(double4) * n, kind, st)) == cudaSuccess &&
+      (e = cudaMemcpyAsync(s->status.ptr, status, sizeof(int) * n, kind, st)) == cudaSuccess)
+    e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return map_cuda(ctx, e, "set stored results");
+  s->used_count = -1;
+  s->hess_h = 0;
+  s->have_results = true;
   return RPD_OK;
 }
 

@@ -39,6 +39,19 @@ class RpdError(RuntimeError):
 
 _lib = None
 
+# rpd_part_reduce_fn: (sums, nsum, maxes, nmax, user) -> 0
+PART_REDUCE = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_longlong), C.c_int, C.POINTER(C.c_longlong), C.c_int, C.c_void_p)
+
+
+def part_range(n: int, part: int, parts: int):
+    """rpd_solver_part_range: (first, count) of part `part` of `parts` of an
+    n-seed diagram's stored seeds."""
+    a, b = C.c_int(0), C.c_int(0)
+    rc = lib().rpd_solver_part_range(n, part, parts, C.byref(a), C.byref(b))
+    if rc != 0:
+        raise RpdError(rc, "part range")
+    return a.value, b.value
+
 
 def lib():
     """Loads librpd.so (raises when it was not built)."""
@@ -112,6 +125,10 @@ def lib():
         L.rpd_batch_launch.argtypes = [C.c_void_p]
         L.rpd_batch_get_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.rpd_batch_destroy.argtypes = [C.c_void_p]
+        L.rpd_solver_part_range.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.rpd_solver_launch_part.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, PART_REDUCE, C.c_void_p]
+        L.rpd_solver_get_stored.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.rpd_solver_set_stored.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.rpd_seeds_load.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_float)),
                                      C.POINTER(C.c_int)]
         L.rpd_seeds_free.argtypes = [C.POINTER(C.c_float)]
@@ -353,6 +370,56 @@ class Solver:
     def launch(self, params=None, **kw):
         p = params if params is not None else Params.default(**kw)
         self.ctx.check(lib().rpd_solver_launch(self.h, C.byref(p)))
+        return self
+
+    def launch_part(self, part: int, parts: int, reduce, params=None, **kw):
+        """rpd_solver_launch_part: the cells of this part's stored range, with
+        the retry schedule of the whole diagram.  reduce(sums, maxes) gets this
+        part's counts (int64 arrays) and returns them summed (maximised) over
+        every part."""
+        p = params if params is not None else Params.default(**kw)
+        err = []
+
+        def cb(sums, nsum, maxes, nmax, user):
+            try:
+                s = np.ctypeslib.as_array(sums, shape=(nsum,))
+                m = np.ctypeslib.as_array(maxes, shape=(nmax,))
+                rs, rm = reduce(s.copy(), m.copy())
+                s[:] = rs
+                m[:] = rm
+                return 0
+            except Exception as exc:  # reported after the launch returns
+                err.append(exc)
+                return 1
+
+        fn = PART_REDUCE(cb)
+        rc = lib().rpd_solver_launch_part(self.h, C.byref(p), part, parts, fn, None)
+        if err:
+            raise err[0]
+        self.ctx.check(rc)
+        return self
+
+    def stored(self, first: int, count: int, out=None, status=None, device: bool = False):
+        """rpd_solver_get_stored: results of stored seeds first .. first+count-1
+        ((count, 4) doubles, (count,) statuses); with device=True, out and
+        status are device pointers (ints) filled in place."""
+        if device:
+            self.ctx.check(lib().rpd_solver_get_stored(self.h, C.c_void_p(out), C.c_void_p(status), first, count,
+                                                      RPD_DEVICE))
+            return None
+        o = np.zeros((count, 4), np.float64)
+        st = np.zeros(count, np.int32)
+        self.ctx.check(lib().rpd_solver_get_stored(self.h, _ptr(o), _ptr(st), first, count, RPD_HOST))
+        return o, st
+
+    def set_stored(self, out, status, device: bool = False):
+        """rpd_solver_set_stored: installs every stored seed's results."""
+        if device:
+            self.ctx.check(lib().rpd_solver_set_stored(self.h, C.c_void_p(out), C.c_void_p(status), RPD_DEVICE))
+        else:
+            o = np.ascontiguousarray(out, np.float64)
+            st = np.ascontiguousarray(status, np.int32)
+            self.ctx.check(lib().rpd_solver_set_stored(self.h, _ptr(o), _ptr(st), RPD_HOST))
         return self
 
     def moments(self) -> np.ndarray:

@@ -328,6 +328,37 @@ int rpd_solver_set_grid(rpd_solver *s, const rpd_grid *g);
  * next launch or set_points. */
 int rpd_solver_launch(rpd_solver *s, const rpd_params *p);
 
+/* ---------------------------------------------------- one diagram, several GPUs */
+
+/* A diagram split over several solvers, e.g. one per GPU (no counterpart in
+ * the reference, which solves one id batch after another on one device,
+ * voronoi.cpp:960-973; this cuts the diagram at those batches).  Every part
+ * holds all seeds and the domain (rpd_solver_set_points / _set_grid with the
+ * same inputs) and solves the cells of its range of stored (binned) seeds,
+ * part p of `parts`: rpd_solver_part_range gives first and count.  The retry
+ * schedule is the whole diagram's: after every pass the launch calls
+ * `reduce` with this part's counts -- sums[0 .. RPD_STATUS_NUM) the failing
+ * cells' status histogram, sums[RPD_STATUS_NUM] their number, maxes[0] the
+ * largest triangle count settled ahead -- and the callback must replace each
+ * with its sum (maximum) over all parts (an all-reduce over the parts'
+ * processes, e.g. NCCL; every part calls it the same number of times) and
+ * return 0.  Then every part holds its range's results in stored order:
+ * gather the ranges (rpd_solver_get_stored, then e.g. an all-gather) and
+ * install them on a solver with rpd_solver_set_stored, whose getters then
+ * give the whole diagram -- the results rpd_solver_launch gives, bit for bit.
+ * Not with Hessian rows or used cells. */
+typedef int (*rpd_part_reduce_fn)(long long *sums, int nsum, long long *maxes, int nmax, void *user);
+int rpd_solver_part_range(int n, int part, int parts, int *first, int *count);
+int rpd_solver_launch_part(rpd_solver *s, const rpd_params *p, int part, int parts, rpd_part_reduce_fn reduce,
+                           void *user);
+/* Results of stored seeds first .. first + count - 1 (4 doubles and a status
+ * each; either pointer may be null); stored order = the binned order of
+ * rpd_solver_get_permutation. */
+int rpd_solver_get_stored(rpd_solver *s, double *out4, int *status, int first, int count, rpd_mem where);
+/* Installs every stored seed's results (n of each), e.g. gathered from the
+ * parts, as this solver's last results. */
+int rpd_solver_set_stored(rpd_solver *s, const double *out4, const int *status, rpd_mem where);
+
 /* Per seed in USER order: (m*x, m*y, m*z, m) in the reference frame, as
  * getBarycenters + getPermutationToUser give them (voronoi.cpp:1165-1209);
  * zeros for failed cells; the seed itself for w <= RPD_NO_CELL_LIMITS. */
