@@ -733,7 +733,7 @@ def run_batch(args, cfg, rank, world, local):
         e2e_s.append(time.perf_counter() - t0)
     e2e_t = sum(e2e_s) / len(e2e_s)
     recaptured = batch.stats()["captures"] - bstats["captures"]
-    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda", 1 if split else None)
+    ms, e2e_t, value, e2e_value = aggregate_over_ranks(ms, e2e_t, n, world, "cuda")
     seq_rate = n / min(seq_wall)
     seq_dev_rate = n / (min(seq_dev) / 1e3)
 

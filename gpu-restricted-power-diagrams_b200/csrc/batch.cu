@@ -406,6 +406,8 @@ struct rpd_batch {
   DevBuf f0, f1, s0, s1, scan_tiles;
   DevBuf d_probes, d_probe_start;  // outside probe records of the probed diagrams, row prefixes
   bool probed = false;             // the capture runs the outside probe
+  int stats_variant[kKnnClasses] = {};       // first pass's neighbour variant per slot class (-1: unused)
+  float stats_trial_ms[kKnnClasses][2] = {};  // the capture's trial: warp, thread (0: no trial)
   cudaEvent_t ev_probe = nullptr;  // after the probe and its compaction
   DevBuf retry_knn, defer_slots, defer_part, defer_fail, defer_ctr, defer_chunk_slot, work;
   DiagState *host_states = nullptr;  // pinned
@@ -700,6 +702,66 @@ int capture(rpd_batch *b) {
   const int knn_blocks = ctx->sm_count * (2048 / kKnnThreads);
   const int flat_blocks = ctx->sm_count * 8;
   int launches = 0;
+  // The first pass's neighbour-search variant per slot class (the
+  // autotuner): the probe and the first pass's plan run once outside the
+  // graph, so the records and rows exist, then each class large enough to
+  // tell (16K rows) is searched both ways on its own rows, timed with events
+  // (one untimed round first); the graph takes the faster.  Retry passes
+  // (few rows) take a warp per seed.
+  int variant[kKnnClasses];
+  for (int c = 0; c < kKnnClasses; ++c) {
+    variant[c] = kKnnWarp;
+    b->stats_trial_ms[c][0] = b->stats_trial_ms[c][1] = 0.f;
+  }
+  {
+    bool trial = false;
+    for (int c = 0; c < kKnnClasses; ++c)
+      trial |= class_used[c] && 32 * kKnnClassSlots[c] <= kKnnThreadMaxK && class_rows[c] >= 16384;
+    if (trial) {
+      if (nprobe) {
+        if ((e = probe_batch_launch(b->d_probes.as<ProbeLaunch>(), b->d_probe_start.as<int>(), nprobe, probe_rows,
+                                    Pb[0], Vb[0], st)) != cudaSuccess)
+          return map_cuda(ctx, e, "batch probe");
+        k_probe_flags_batch<<<flat_blocks, 256, 0, st>>>(ds, b->d_all_start.as<int>(), nd, b->f0.as<int>());
+        if ((e = exclusive_scan(b->f0.as<int>(), b->s0.as<int>(), nscan, b->scan_tiles.as<int>(), st)) != cudaSuccess)
+          return map_cuda(ctx, e, "batch scan");
+        k_probe_scatter_batch<<<flat_blocks, 256, 0, st>>>(ds, b->d_all_start.as<int>(), nd, b->f0.as<int>(),
+                                                           b->s0.as<int>());
+      }
+      PassArgs pa0;
+      pa0.pass = 0;
+      pa0.final_ = 0;
+      pa0.retry_knn = b->retry_knn.as<unsigned>();
+      pa0.retry_cap = retry_cap;
+      pa0.Pb = Pb[0];
+      pa0.Vb = Vb[0];
+      pa0.Tb = Tb[0];
+      pa0.Kb = Kb[0];
+      pa0.defer = DeferQueue();
+      k_plan<<<1, 1024, 0, st>>>(ds, sts, nd, pl, pa0);
+      cudaEvent_t te[3];
+      for (auto &x : te) cudaEventCreate(&x);
+      for (int c = 0; c < kKnnClasses; ++c) {
+        const int S = kKnnClassSlots[c];
+        if (!class_used[c] || 32 * S > kKnnThreadMaxK || class_rows[c] < 16384) continue;
+        for (int round = 0; round < 2 && e == cudaSuccess; ++round) {
+          if (round) cudaEventRecord(te[0], st);
+          e = knn_batch_launch(S, pl.knn, pl.kstart + c * stride, nd, knn_blocks, st, -1, kKnnWarp);
+          if (round) cudaEventRecord(te[1], st);
+          if (e == cudaSuccess) e = knn_batch_launch(S, pl.knn, pl.kstart + c * stride, nd, knn_blocks, st, -1, kKnnThread);
+          if (round) cudaEventRecord(te[2], st);
+        }
+        if (e == cudaSuccess) e = cudaEventSynchronize(te[2]);
+        if (e != cudaSuccess) break;
+        cudaEventElapsedTime(&b->stats_trial_ms[c][0], te[0], te[1]);
+        cudaEventElapsedTime(&b->stats_trial_ms[c][1], te[1], te[2]);
+        variant[c] = b->stats_trial_ms[c][1] < b->stats_trial_ms[c][0] ? kKnnThread : kKnnWarp;
+      }
+      for (auto &x : te) cudaEventDestroy(x);
+      if (e != cudaSuccess || (e = cudaStreamSynchronize(st)) != cudaSuccess) return map_cuda(ctx, e, "batch trial");
+    }
+  }
+  for (int c = 0; c < kKnnClasses; ++c) b->stats_variant[c] = class_used[c] ? variant[c] : -1;
   if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return map_cuda(ctx, e, "begin capture");
   auto fail = [&](cudaError_t err, const char *what) {
@@ -760,7 +822,8 @@ int capture(rpd_batch *b) {
       const bool want = j == 0 ? class_used[c] : (S >= knn_slots(Kmin) && S <= knn_slots(Kb[j]));
       if (!want) continue;
       if ((e = knn_batch_launch(S, pl.knn, pl.kstart + c * stride, nd, knn_blocks, st,
-                                j == 0 && !nprobe ? class_rows[c] : -1)) != cudaSuccess)
+                                j == 0 && !nprobe ? class_rows[c] : -1, j == 0 ? variant[c] : kKnnWarp)) !=
+          cudaSuccess)
         return fail(e, "batch knn");
       ++launches;
     }
@@ -900,6 +963,11 @@ int rpd_batch_launch(rpd_batch *b) {
   const int rec = std::min(b->passes, kPassRecord);
   for (int j = 0; j < rec; ++j) cudaEventElapsedTime(&S.pass_ms[j], b->ev_pass[j], b->ev_pass[j + 1]);
   if (b->probed) cudaEventElapsedTime(&S.probe_ms, b->ev_pass[0], b->ev_probe);
+  for (int c = 0; c < kKnnClasses; ++c) {
+    S.knn_variant[c] = b->stats_variant[c];
+    S.knn_trial_warp_ms[c] = b->stats_trial_ms[c][0];
+    S.knn_trial_thread_ms[c] = b->stats_trial_ms[c][1];
+  }
   std::vector<int> again;
   for (int d = 0; d < b->ndiag; ++d) {
     const DiagState &h = b->host_states[d];

@@ -14,6 +14,8 @@
 // shell's bound ((shell-1) * bin width)^2, checked at shell granularity
 // after every pending candidate is merged -- the exact rule of the oracle's
 // exact mode, so lists agree bit for bit.
+#include <algorithm>
+
 #include "knn.cuh"
 #include "select.cuh"
 
@@ -257,20 +259,14 @@ struct Heap {
   }
 };
 
-__global__ void __launch_bounds__(kThreadRows) k_knn_thread(const float4 *__restrict__ stored,
-                                                           const int *__restrict__ counters, int dim,
-                                                           const int *__restrict__ ids, int num, int K,
-                                                           const float *__restrict__ ring_bound,
-                                                           unsigned *__restrict__ out,
-                                                           unsigned long long *__restrict__ candidates) {
-  extern __shared__ unsigned long long heap_smem[];
-  const int t = threadIdx.x;
-  const int row0 = blockIdx.x * kThreadRows;
-  const int row = row0 + t;
-  const Heap H{heap_smem + t};
+// The K nearest of stored seed pin into the heap of this thread, sorted
+// ascending and padded with kEmptyKey to K; returns the candidates read.
+__device__ __forceinline__ unsigned long long knn_thread_row(const float4 *__restrict__ stored,
+                                                             const int *__restrict__ counters, int dim, int pin,
+                                                             int K, const float *__restrict__ ring_bound,
+                                                             const Heap &H) {
   unsigned long long ncand = 0;
-  if (row < num) {
-    const int pin = ids ? __ldg(&ids[row]) : row;
+  {
     const float4 p = __ldg(&stored[pin]);
     const int cin = bin_of(p, dim);
     ShellRows sh;
@@ -323,6 +319,22 @@ __global__ void __launch_bounds__(kThreadRows) k_knn_thread(const float4 *__rest
     }
     for (int i = n; i < K; ++i) H.at(i) = kEmptyKey;
   }
+  return ncand;
+}
+
+__global__ void __launch_bounds__(kThreadRows) k_knn_thread(const float4 *__restrict__ stored,
+                                                           const int *__restrict__ counters, int dim,
+                                                           const int *__restrict__ ids, int num, int K,
+                                                           const float *__restrict__ ring_bound,
+                                                           unsigned *__restrict__ out,
+                                                           unsigned long long *__restrict__ candidates) {
+  extern __shared__ unsigned long long heap_smem[];
+  const int t = threadIdx.x;
+  const int row0 = blockIdx.x * kThreadRows;
+  const int row = row0 + t;
+  const Heap H{heap_smem + t};
+  unsigned long long ncand = 0;
+  if (row < num) ncand = knn_thread_row(stored, counters, dim, ids ? __ldg(&ids[row]) : row, K, ring_bound, H);
   __syncthreads();
   // coalesced rows: a warp per row, lanes over the row's entries
   const int lane = t & 31, warp = t >> 5;
@@ -335,6 +347,25 @@ __global__ void __launch_bounds__(kThreadRows) k_knn_thread(const float4 *__rest
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(kFull, ncand, o);
     if (lane == 0) atomicAdd(candidates, ncand);
+  }
+}
+
+// Rows of many diagrams (batched solves) with a thread per seed: the
+// diagrams of one slot class own rows start[d] .. start[d+1]; threads stride
+// over them, each writing its own row (K of its diagram, at most kmax).
+__global__ void __launch_bounds__(kThreadRows) k_knn_thread_batch(const KnnDiag *__restrict__ diags,
+                                                                 const int *__restrict__ start, int ndiag) {
+  extern __shared__ unsigned long long heap_smem[];
+  const Heap H{heap_smem + threadIdx.x};
+  const int total = start[ndiag];
+  const int nthreads = gridDim.x * blockDim.x;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < total; r += nthreads) {
+    const int d = owner_of_row(start, ndiag, r);
+    const KnnDiag &g = diags[d];
+    const int i = r - start[d];
+    knn_thread_row(g.stored, g.counters, g.dim, g.ids ? g.ids[i] : i, g.K, g.ring_bound, H);
+    unsigned *o = g.out + size_t(i) * g.K;
+    for (int k = 0; k < g.K; ++k) o[k] = unsigned(H.at(k) & 0xffffffffull);
   }
 }
 
@@ -383,7 +414,26 @@ void ring_bounds(int dim, float *bound) {
 }
 
 cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st,
-                             long rows) {
+                             long rows, int variant) {
+  if (variant == kKnnThread) {
+    // a thread per row, the heap sized for the class's largest K (32 S)
+    if (32 * S > kKnnThreadMaxK) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(unsigned long long) * size_t(32 * S) * kHeapStride;
+    cudaError_t e = cudaFuncSetAttribute(k_knn_thread_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(sizeof(unsigned long long) * kKnnThreadMaxK * kHeapStride));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_thread_batch, kThreadRows, smem) !=
+            cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int tb = per_sm * sms;
+    if (rows >= 0) tb = int(std::min<long>(tb, (rows + kThreadRows - 1) / kThreadRows + 1));
+    k_knn_thread_batch<<<tb, kThreadRows, smem, st>>>(diags, start, ndiag);
+    return cudaGetLastError();
+  }
   if (rows >= 0) blocks = int(rows * 32 / kKnnThreads + 1);
   switch (S) {
     case 1: k_knn_batch<1><<<blocks, kKnnThreads, 0, st>>>(diags, start, ndiag); break;

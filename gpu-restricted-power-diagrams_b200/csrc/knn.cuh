@@ -47,6 +47,6 @@ constexpr int kKnnClassSlots[kKnnClasses] = {1, 2, 3, 4, 6, 8};
 // rows >= 0: the class's row count, known when the launch is made: one warp
 // per row; else `blocks` persistent blocks.
 cudaError_t knn_batch_launch(int S, const KnnDiag *diags, const int *start, int ndiag, int blocks, cudaStream_t st,
-                             long rows = -1);
+                             long rows = -1, int variant = 0);
 
 }  // namespace rpd

@@ -509,12 +509,17 @@ class BatchStats(C.Structure):
                 ("passes_captured", C.c_int), ("max_passes", C.c_int), ("kernel_launches", C.c_int),
                 ("captures", C.c_int), ("solved_alone", C.c_int), ("pass0_knn_ms", C.c_float),
                 ("pass0_cell_kernel_ms", C.c_float), ("pass_ms", C.c_float * 8), ("pass_cells", C.c_longlong * 8),
-                ("probe_ms", C.c_float), ("probe_outside", C.c_longlong)]
+                ("probe_ms", C.c_float), ("probe_outside", C.c_longlong), ("knn_variant", C.c_int * 6),
+                ("knn_trial_warp_ms", C.c_float * 6), ("knn_trial_thread_ms", C.c_float * 6)]
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pass_ms", "pass_cells")}
+        arrays = ("pass_ms", "pass_cells", "knn_variant", "knn_trial_warp_ms", "knn_trial_thread_ms")
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in arrays}
         n = min(self.passes_captured, 8)
         d["passes"] = [{"cells": int(self.pass_cells[i]), "ms": self.pass_ms[i]} for i in range(n)]
+        d["knn_classes"] = [{"K_max": 32 * s, "variant": ("warp", "thread")[v] if v >= 0 else None,
+                             "trial_warp_ms": self.knn_trial_warp_ms[c], "trial_thread_ms": self.knn_trial_thread_ms[c]}
+                            for c, (s, v) in enumerate(zip((1, 2, 3, 4, 6, 8), self.knn_variant)) if v >= 0]
         return d
 
 

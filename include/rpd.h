@@ -495,6 +495,12 @@ typedef struct rpd_batch_stats {
   long long pass_cells[8]; /* cells of each pass, all diagrams */
   float probe_ms;       /* of pass_ms[0]: the outside probe and its compaction (0: no diagram probed) */
   long long probe_outside; /* seeds the probe proved empty outside their domains, all diagrams */
+  /* The first pass's neighbour search per K class (K <= 32, 64, 96, 128, 192,
+   * 256): 0 a warp per seed, 1 a thread per seed, -1 no diagram in the
+   * class; chosen at capture by timing both on the class's own rows (0 ms:
+   * no trial, too few rows or K too large for a thread per seed). */
+  int knn_variant[6];
+  float knn_trial_warp_ms[6], knn_trial_thread_ms[6];
 } rpd_batch_stats;
 
 rpd_batch *rpd_batch_create(rpd_context *ctx, rpd_solver *const *solvers, const rpd_params *params, int count,
