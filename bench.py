@@ -433,7 +433,8 @@ def run_ours(args, cfg, rank, world, local):
     n = len(x)
     # every timed step is a full solve: neighbours included (repeated launches
     # on unchanged seeds would otherwise reuse the neighbour table)
-    params = rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_FRESH_NEIGHBOURS)
+    params = rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"],
+                                flags=rpd.FLAG_FRESH_NEIGHBOURS | probe_flag(args))
     solver = rpd.Solver(ctx).set_points(x)
     t0 = time.perf_counter()
     solver.set_points(x)  # again, timed: upload from host memory + binning
@@ -502,7 +503,8 @@ def run_ours(args, cfg, rank, world, local):
     m_gpu, st_gpu = solver.moments(), solver.status()
     nonempty = int(((st_gpu == 4) & (m_gpu[:, 3] > 0)).sum())
     # one untimed launch with the work counters on
-    solver.launch(rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=rpd.FLAG_COUNTERS))
+    solver.launch(rpd.Params.default(K=cfg["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"],
+                                     flags=rpd.FLAG_COUNTERS | probe_flag(args)))
     work = solver.stats()["counters"]
     ms = sum(step_ms) / len(step_ms)
 
@@ -575,6 +577,7 @@ def run_ours(args, cfg, rank, world, local):
         "vs_baseline": None, "dtype": "f64 geometry on f32 seeds (FP64 cofactor predicates and integration)",
         "data": "synthetic",
         "config": {"workload": args.config, "description": cfg["desc"], "n_seeds_per_gpu": n,
+                   "outside_probe": bool(args.outside_probe),
                    "parallelism": (f"one diagram split over {world} GPUs (stored-seed ranges, per-pass "
                                    "all-reduce of the retry counts, one all-gather of the results)") if split
                                   else f"{world} independent diagrams, one per GPU",
@@ -618,6 +621,12 @@ def run_ours(args, cfg, rank, world, local):
         dist.destroy_process_group()
 
 
+def probe_flag(args):
+    import rpd
+
+    return rpd.FLAG_OUTSIDE_PROBE if getattr(args, "outside_probe", False) else 0
+
+
 def batch_specs(cfg, rank, count=None):
     """The batch's diagrams; `count` < cfg["count"] keeps the first ones (the
     same specs: the generator draws them in order)."""
@@ -658,7 +667,7 @@ def run_batch(args, cfg, rank, world, local):
         v = rpd.Solver(ctx).set_points(s["xyzw"])
         v.set_grid(g)
         solvers.append(v)
-    params = [rpd.Params.default(K=s["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"]) for s in specs]
+    params = [rpd.Params.default(K=s["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], flags=probe_flag(args)) for s in specs]
     n = sum(len(s["xyzw"]) for s in specs)
     batch = rpd.Batch(solvers, params, ctx)
     for _ in range(args.warmup):
@@ -691,7 +700,7 @@ def run_batch(args, cfg, rank, world, local):
     got = [(v.status().copy(), v.moments().copy()) for v in solvers]
     # the same diagrams one after another (fresh neighbours, as in the batch)
     seq_params = [rpd.Params.default(K=s["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"],
-                                     flags=rpd.FLAG_FRESH_NEIGHBOURS) for s in specs]
+                                     flags=rpd.FLAG_FRESH_NEIGHBOURS | probe_flag(args)) for s in specs]
     for v, p in zip(solvers[:8], seq_params):
         v.launch(p)
     seq_wall, seq_dev = [], []
@@ -763,6 +772,7 @@ def run_batch(args, cfg, rank, world, local):
         "vs_baseline": None, "dtype": "f64 geometry on f32 seeds (FP64 cofactor predicates and integration)",
         "data": "synthetic",
         "config": {"workload": args.config, "description": cfg["desc"], "diagrams": len(specs),
+                   "outside_probe": bool(args.outside_probe),
                    "n_seeds_per_gpu": n, "n_min": min(sizes), "n_max": max(sizes),
                    "parallelism": f"{world} independent batches, one per GPU",
                    "l2": "flushed between steps (256 MB write, untimed)"},
@@ -794,6 +804,34 @@ def run_batch(args, cfg, rank, world, local):
               "sample": f"{runs[0][1]} cells: " + BATCH_REF_SAMPLE.format(len(jobs)) +
                         f" (the --impl reference arm's sample), {t_ref:.2f} s on {os.cpu_count()} host threads"}
         line["cpu_baseline"] = cb
+        # every 32nd diagram of the batch against the FP64 oracle, every cell
+        # of its batched solve (statuses, non-empty set, mass, barycentre)
+        import oracle
+
+        checks = []
+        for i in range(0, len(specs), 32):
+            a = grids[i].arrays()
+            ga = oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"],
+                                   a["offsets"])
+            x = specs[i]["xyzw"].astype(np.float64)
+            ref, rst = oracle.solve(x, grid=ga, K=specs[i]["K"], P=cfg["P"], V=cfg["V"], T=cfg["T"], use_double=True,
+                                    knn_mode=1)
+            st_b, m_b = got[i]
+            ok = (st_b == 4) & (rst == 4)
+            rel = np.abs(m_b[ok, 3] - ref[ok, 3]) / np.maximum(np.abs(ref[ok, 3]), 1e-3)
+            nz = ok & (np.abs(ref[:, 3]) > 1e-3) & (np.abs(m_b[:, 3]) > 1e-3)
+            bary = (np.abs(m_b[nz, :3] / m_b[nz, 3:] - ref[nz, :3] / ref[nz, 3:]).max(1) / 1000.0
+                    if nz.any() else np.zeros(1))
+            ne, ner = (np.abs(m_b[:, 3]) > 1e-3) & (st_b == 4), (np.abs(ref[:, 3]) > 1e-3) & (rst == 4)
+            checks.append({"diagram": i, "n": len(x), "K": specs[i]["K"], "grid": specs[i]["grid_size"],
+                           "status_mismatch": int((st_b != rst).sum()), "nonempty_symdiff": int((ne != ner).sum()),
+                           "mass_max_rel": float(rel.max()) if rel.size else 0.0, "bary_max": float(bary.max())})
+        line["accuracy"] = {"oracle": "FP64 restatement, exact neighbour order; every cell of every 32nd diagram",
+                            "diagrams": checks,
+                            "status_mismatch": sum(c["status_mismatch"] for c in checks),
+                            "nonempty_symdiff": sum(c["nonempty_symdiff"] for c in checks),
+                            "mass_max_rel": max(c["mass_max_rel"] for c in checks),
+                            "bary_max": max(c["bary_max"] for c in checks)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     batch.close()
@@ -1079,6 +1117,9 @@ def main():
                     help="single-diagram configs with --gpus N > 1: the ranks split one diagram (strong scaling) "
                          "instead of solving one each")
     ap.add_argument("--slots", type=int, default=None, help="serving configs: concurrent slots (default: the config's)")
+    ap.add_argument("--outside-probe", action="store_true",
+                    help="solve with RPD_FLAG_OUTSIDE_PROBE: cells proven outside the domain are settled before "
+                         "the first pass (moments equal; a cell the reference never settles reads success)")
     ap.add_argument("--diagrams", type=int, default=None,
                     help="batch configs: solve only the first N diagrams (small cases for profiling)")
     args = ap.parse_args()

@@ -508,11 +508,12 @@ int describe(rpd_batch *b, std::vector<DiagStatic> &out) {
     g.inner_apex = (p.flags & RPD_FLAG_REFERENCE_APEX) ? 0 : 1;
     g.safe_radius = (p.flags & RPD_FLAG_SAFE_RADIUS) ? 1 : 0;
     g.cube_eps = p.cube_eps >= 0 ? p.cube_eps : (grid ? 0.1f : 0.f);
-    // the outside probe, as rpd_solver_launch runs it on a launch with fresh
-    // neighbours (every replay computes its neighbours afresh): with a domain
-    // that leaves plainly-outside voxels to prove
+    // the outside probe (RPD_FLAG_OUTSIDE_PROBE), as rpd_solver_launch runs
+    // it on a launch with fresh neighbours (every replay computes its
+    // neighbours afresh): with a domain that leaves plainly-outside voxels to
+    // prove
     g.probe = 0;
-    if (grid && g.early_out && s->grid.sat && !(p.flags & RPD_FLAG_NO_PROBE)) {
+    if (grid && g.early_out && s->grid.sat && (p.flags & RPD_FLAG_OUTSIDE_PROBE) && !(p.flags & RPD_FLAG_NO_PROBE)) {
       const long long S = s->grid.size, S1 = S + 1;
       if (s->grid_nonplain < 0) {
         int v = 0;

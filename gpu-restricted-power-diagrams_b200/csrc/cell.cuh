@@ -41,6 +41,7 @@ enum CellCounter {
   kCtrEscTests,           // FP32 clipping: sign tests escalated to FP64
   kCtrEscVertices,        // FP32 clipping: vertices made in FP64 (near-degenerate)
   kCtrEscRadii,           // FP32 clipping: radius tests escalated to the exact FP64 radius
+  kCtrStartCorner,        // boundary cells with cones from the reference's start corner
   kCtrNum
 };
 

@@ -1254,6 +1254,66 @@ __device__ int cone_triangles(WarpCell &w, const CellLaunch &a, float4 s, const 
   return kSuccess;
 }
 
+// Whether the cone clipping from the start corner p0 (cone_triangles, the
+// reference's) surely overflows no cap on this cell, so that an apex inside
+// the cell, which clips nothing, gives the reference's status.  Per triangle
+// of the union: a cone plane with every vertex beyond it (margin included)
+// empties the piece and the triangle clips nothing; otherwise the planes
+// that may cut a vertex number c, and no part of the cell that one of them
+// misses can it cut later, so np + c < P keeps every plane check before a
+// clip below P and nv + 2c <= V every clip within V (a clip adds at most
+// one face; f faces make 2f - 4 vertices).  The margin, 1e-9 of the plane
+// offset plus the cell radius R, covers the rounding of the planes (built
+// here as cone_triangles builds them) and of later vertices; a triangle
+// nearly flat from p0 counts as a failure.  One triangle per lane.
+__device__ bool ref_cones_fit(const WarpCell &w, const DevGrid &g, float4 s, const int *tids, int ntri,
+                              const double p0[3], int P, int V, double R, int lane) {
+  if (w.np >= P) return false;  // the check before each triangle's cone
+  bool bad = false;
+  for (int b0 = 0; b0 < ntri; b0 += 32) {
+    const int ti = b0 + lane;
+    if (ti < ntri && !bad) {
+      const int tri = tids[ti];
+      const int i1 = __ldg(&g.tris[3 * tri]), i2 = __ldg(&g.tris[3 * tri + 1]), i3 = __ldg(&g.tris[3 * tri + 2]);
+      const float4 r1 = __ldg(&g.points[i1]), r2 = __ldg(&g.points[i2]), r3 = __ldg(&g.points[i3]);
+      const double P1[3] = {double(r1.x) - s.x, double(r1.y) - s.y, double(r1.z) - s.z};
+      const double P2[3] = {double(r2.x) - s.x, double(r2.y) - s.y, double(r2.z) - s.z};
+      const double P3[3] = {double(r3.x) - s.x, double(r3.y) - s.y, double(r3.z) - s.z};
+      const double ax = P1[0] - p0[0], ay = P1[1] - p0[1], az = P1[2] - p0[2];
+      const double bx = P2[0] - p0[0], by = P2[1] - p0[1], bz = P2[2] - p0[2];
+      const double cx = P3[0] - p0[0], cy = P3[1] - p0[1], cz = P3[2] - p0[2];
+      const double det = ax * (by * cz - bz * cy) - bx * (ay * cz - az * cy) + cx * (ay * bz - az * by);
+      const double scale = sqrt((ax * ax + ay * ay + az * az) * (bx * bx + by * by + bz * bz) *
+                                (cx * cx + cy * cy + cz * cz));
+      if (!(fabs(det) > 1e-9 * scale)) {
+        bad = true;
+      } else {
+        const bool go_out = det > 0;
+        const double *q1 = P1, *q2 = go_out ? P2 : P3, *q3 = go_out ? P3 : P2;
+        const Plane f[4] = {plane_from_points(p0, q1, q2), plane_from_points(p0, q3, q1),
+                            plane_from_points(p0, q2, q3), plane_from_points(q2, q3, q1)};
+        int c = 0;
+        bool empty = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double m = 1e-9 * (fabs(f[k].w) + R);
+          bool any = false, all = true;
+          for (int v = 0; v < w.nv; ++v) {
+            const double cw = w.cw[v], ps = plane_side(w.cx[v], w.cy[v], w.cz[v], cw, f[k]);
+            any |= ps > (kTieEps - m) * fabs(cw);
+            all &= ps > (kTieEps + m) * fabs(cw);
+          }
+          empty |= all;
+          c += any ? 1 : 0;
+        }
+        bad = !empty && c > 0 && !(w.np + c < P && w.nv + 2 * c <= V);
+      }
+    }
+    if (__any_sync(kFull, bad)) return false;
+  }
+  return true;
+}
+
 // Apex inside the cell.  The signed cone decomposition holds for any apex on
 // a known side of the surface.  From a point inside the convex cell, the
 // segment to any point of the cell stays in the cell, so a triangle that
@@ -2147,7 +2207,18 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
     count(ctr, kCtrTriangles, nuniq, lane);
   }
   bool inner = false;
-  if (nuniq > 0 && a.inner_apex) {
+  // The facet pieces of an inner apex clip nothing, so they cannot overflow
+  // a cap; the reference's cones clip the cell by up to 4 planes each (its
+  // status is plane_overflow when a plane check before one finds P planes,
+  // vertex_overflow past V vertices).  A clip adds at most one face, and a
+  // closed cell of f faces has 2f - 4 vertices, so with P >= planes + 4 and
+  // V >= vertices + 8 no cone can overflow and the inner apex gives the
+  // reference's status; else a count of the cuts per cone (ref_cones_fit)
+  // may still show it.  Otherwise the cones run from the start corner and
+  // fail where the reference's fail.
+  if (nuniq > 0 && a.inner_apex &&
+      ((w.np + 4 <= a.P && w.nv + 8 <= a.V) ||
+       ref_cones_fit(w, g, s, tl, nuniq, pt0, a.P, a.V, sqrt(cell_radius2<VS>(w, lane)), lane))) {
     double ap[3];
     const int f = inner_apex(w, g, s, vmin, vmax, tl, nuniq, ap, lane);
     if (f >= 0) {
@@ -2159,6 +2230,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
       nuniq = kept;
     }
   }
+  if (nuniq > 0 && !inner) count(ctr, kCtrStartCorner, 1, lane);
   trace_rec(tr, trcap, lane, 5, pt0[0], pt0[1], pt0[2], in_domain, nuniq);
   if (in_domain == 2) integrate<VS, INL>(w, 1.0, acc, lane, ctr, tr, trcap);
   if (nuniq == 0 && !ahead) return kSuccess;
@@ -2258,6 +2330,84 @@ __device__ __forceinline__ bool radius_reached(double d2j, double R2, double saf
   return d2j > R2 && e > 0.0 && 4.0 * R2 * d2j < e * e;
 }
 
+// Squared distance between two seeds, as the clipping loop computes it.
+__device__ __forceinline__ double seed_dist2(float4 b, float4 s) {
+  const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
+  return bx * bx + by * by + bz * bz;
+}
+
+// A cell proven outside the domain (its squared radius at most r_plain^2)
+// has the reference's result mass 0 and status success only if the
+// reference's clipping of it, which goes on through the neighbours, ends in
+// success.  How far it goes at most: the cell's radius only shrinks, so past
+// neighbour j (clipped, squared radius R2) the first neighbour z >= j that
+// reaches the security radius at R2 ends it (the last neighbour clipped: z),
+// as does the end of the list at z (z - 1: every other seed clipped).
+// Returns that index, or -1 when neither comes within K.  R2 carries a
+// relative margin of 1e-9 for the rounding of the later cells' vertices.
+__device__ int last_clip(const CellLaunch &a, const unsigned *nrow, float4 s, int j, double R2, double dw, int lane) {
+  const double R2m = R2 * (1.0 + 1e-9);
+  for (int c0 = j & ~31; c0 < a.K; c0 += 32) {
+    const int i = c0 + lane;
+    bool stop = false, none = false;
+    if (i >= j && i < a.K) {
+      const unsigned z = __ldg(&nrow[i]);
+      none = z == kNone;
+      stop = none || radius_reached(seed_dist2(__ldg(&a.stored[z]), s), R2m, dw);
+    }
+    const unsigned m = __ballot_sync(kFull, stop);
+    if (m) {
+      const int src = __ffs(m) - 1;
+      return c0 + src - (__shfl_sync(kFull, none, src) ? 1 : 0);
+    }
+  }
+  return -1;
+}
+
+// How many of the neighbours j+1 .. e may cut the current cell: their plane
+// (built as the clipping loop builds it) has a vertex of the cell on its far
+// side, with a margin of 1e-9 of the plane offset plus the cell radius R.
+// Every later cell lies in the current one, whose farthest point beyond a
+// plane is a vertex, so a neighbour that cuts none of its vertices cuts no
+// later cell either; the margin covers the rounding of the later cells'
+// vertices.  One neighbour per lane, every vertex in turn.
+template <int PREC>
+__device__ int cutters_ahead(const WarpCell &w, const CellLaunch &a, const unsigned *nrow, float4 s, int j, int e,
+                             double R, int lane) {
+  int cnt = 0;
+  for (int c0 = (j + 1) & ~31; c0 <= e; c0 += 32) {
+    const int i = c0 + lane;
+    bool cut = false;
+    if (i > j && i <= e) {
+      const float4 b = __ldg(&a.stored[__ldg(&nrow[i])]);
+      const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
+      const double nd2 = bx * bx + by * by + bz * bz;
+      const double len = sqrt(nd2), inv = 1.0 / len;
+      const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) * (0.5 * inv);
+      Plane pl{-bx * inv, -by * inv, -bz * inv, off};
+      if constexpr (PREC == 2) pl = Plane{double(float(pl.x)), double(float(pl.y)), double(float(pl.z)), double(float(pl.w))};
+      const double tol = kTieEps - 1e-9 * (fabs(off) + R);
+      for (int v = 0; v < w.nv && !cut; ++v) {
+        const double cw = w.cw[v];
+        cut = plane_side(w.cx[v], w.cy[v], w.cz[v], cw, pl) > tol * fabs(cw);
+      }
+    }
+    cnt += __popc(__ballot_sync(kFull, cut));
+  }
+  return cnt;
+}
+
+// Whether clipping the neighbours after j up to e, of which c may cut the
+// cell, surely overflows no cap: the plane count grows by one per cut
+// (np + c < P keeps every plane check before a clip below P), and a cut adds
+// at most one face to the closed cell, whose f faces make 2f - 4 vertices
+// (nv + 2c <= V).  The cell cannot become empty either (nonempty_cell gates
+// the exits).  A later clip that meets a degenerate cavity
+// (inconsistent_boundary) is the one failure this cannot foresee.
+__device__ __forceinline__ bool caps_hold(int e, int j, int c, int np, int nv, int P, int V) {
+  return e >= 0 && (e == j || (np + c < P && nv + 2 * c <= V));
+}
+
 // The vertex capacity a cell of this launch works with.  A batched launch's
 // layout may hold more vertices than a diagram's cap (it is sized for every
 // diagram); capacity-dependent choices follow the diagram's own cap, so a
@@ -2320,6 +2470,11 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
   bool reached = false, exhausted = false, outside = false;
   const bool early = GRID && a.early_out && a.grid.sat != nullptr && a.wmin != nullptr && a.border_d == 0;
   double plain2 = early ? plain_radius2(a.grid, s, lane) : -1.0;
+  // once the cell is proven outside (out_known), clipping stops where the
+  // rest of the reference's clipping surely succeeds (last_clip,
+  // cutters_ahead, caps_hold), else goes on, and the cell, once it succeeds,
+  // skips the restriction
+  bool out_known = false;
   // the weighted security-radius guard (radius_reached): w_s - min w when
   // on (computed where used, so the default loop carries nothing), else -1
   auto safe_dw = [&]() -> double {
@@ -2386,8 +2541,13 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
         if (r > 0) {
           R2 = cell_radius2<VS>(w, lane);
           if (R2 <= plain2) {
-            outside = true;
-            break;
+            out_known = true;
+            const int e = last_clip(a, nrow, s, i0 + j, R2, safe_dw(), lane);
+            if (e >= 0 && caps_hold(e, i0 + j, cutters_ahead<PREC>(w, a, nrow, s, i0 + j, e, sqrt(R2), lane), w.np,
+                                    w.nv, a.P, a.V)) {
+              outside = true;
+              break;
+            }
           }
         }
         if (radius_reached(d2j, R2, safe_dw())) {
@@ -2410,8 +2570,14 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
               out = R2 <= plain2;
             }
             if (out) {
-              outside = true;
-              break;
+              // the FP64 vertices are not kept here: every later neighbour
+              // counts as a cut
+              out_known = true;
+              const int e = last_clip(a, nrow, s, i0 + j, R2 >= 0.0 ? R2 : double(R2hi), safe_dw(), lane);
+              if (caps_hold(e, i0 + j, e - i0 - j, w.np, w.nv, a.P, a.V)) {
+                outside = true;
+                break;
+              }
             }
           }
         }
@@ -2452,6 +2618,7 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
     if (status == kSuccess && !outside && a.border_d == 0) promote(w, lane);
   }
   if (status == kSuccess && !reached && !exhausted && !outside) status = kSecurityRadiusNotReached;
+  if (status == kSuccess && out_known) outside = true;
   const int np_cell = w.np;  // the clipped cell's planes (cone planes come after)
   if (a.border_d > 0) {
     // bordering pass (ConvexCell.cl:756-809): the clipped cell marks its
@@ -2613,8 +2780,14 @@ __device__ __forceinline__ void probe_row(const ProbeLaunch &p, const Layout &L,
       }
       return __shfl_sync(kFull, a0, owner) - (__shfl_sync(kFull, incl, owner) - __shfl_sync(kFull, cnt, owner)) + c;
     };
-    // cage test over every candidate
+    // cage test over the candidates within 2 r of the seed.  The reference's
+    // clipping stops at a neighbour z past twice the cell's radius R_z;
+    // either it has clipped every cage candidate (its cell lies in the cage)
+    // or one at distance d_c >= d_z > 2 R_z is left, and R_z < d_c / 2 <= r:
+    // with weights, where its cell can be larger than the power cell, it
+    // still lies in the ball
     const float inv_r = float(1.0 / sqrt(plain2)) * 1.001f;
+    const float max_d2 = float(4.0 * plain2) * 0.999f;
     unsigned mask = 0;
     float mind2 = INFINITY;
     for (int base = 0; base < total; base += 32) {
@@ -2627,7 +2800,7 @@ __device__ __forceinline__ void probe_row(const ProbeLaunch &p, const Layout &L,
         const float len = sqrtf(d2), inv = 1.0f / len;
         const float off = q.w <= kNoCellLimits ? len : (d2 + (q.w - s.w)) * (0.5f * inv);
         mind2 = fminf(mind2, d2);
-        mask |= cage_bits(dx * inv, dy * inv, dz * inv, off * inv_r);
+        if (d2 <= max_d2) mask |= cage_bits(dx * inv, dy * inv, dz * inv, off * inv_r);
       }
     }
 #pragma unroll
@@ -2659,9 +2832,9 @@ __device__ __forceinline__ void probe_row(const ProbeLaunch &p, const Layout &L,
         best = bitonic_merge32(umin64(best, __shfl_sync(kFull, sorted, 31 - lane)), lane);
       }
       // lane j: the bisector with the j-th nearest candidate (as cell_row
-      // builds it)
+      // builds it); those past 2 r are left out, as in the cage test
       Plane pl{0.0, 0.0, 0.0, 0.0};
-      const bool valid = best != kEmptyKey;
+      const bool valid = best != kEmptyKey && __uint_as_float(unsigned(best >> 32)) <= max_d2;
       if (valid) {
         const float4 b = __ldg(&p.stored[unsigned(best & 0xffffffffull)]);
         const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);

@@ -1015,15 +1015,16 @@ static int launch_impl(rpd_solver *s, const rpd_params *pp, const PartSpec *part
     if ((e = s->used.ensure(size_t(n))) != cudaSuccess) return map_cuda(ctx, e, "alloc used");
     cudaMemsetAsync(s->used.ptr, 0, size_t(n), st);
   }
-  // outside probe: with a domain, most seeds outside it are proven empty
-  // from a few neighbours and the first pass searches the full K nearest of
-  // the others only.  On the first launch after the seeds were set (or with
-  // fresh neighbours); later launches build the whole neighbour table once,
-  // which weight-only re-solves then keep.
+  // outside probe (RPD_FLAG_OUTSIDE_PROBE): with a domain, most seeds outside
+  // it are proven empty from a few neighbours and the first pass searches the
+  // full K nearest of the others only.  On the first launch after the seeds
+  // were set (or with fresh neighbours); later launches build the whole
+  // neighbour table once, which weight-only re-solves then keep.
   const bool table_kept = s->knn_full_K == p.K && !s->fresh_knn;
   bool probe = grid && early && s->grid.sat && !counters && s->hess_h == 0 &&
                !(s->used_on && s->keep_volume <= 0.0) && !table_kept &&
-               (s->launches_since_points == 0 || s->fresh_knn) && !(p.flags & RPD_FLAG_NO_PROBE);
+               (s->launches_since_points == 0 || s->fresh_knn) && (p.flags & RPD_FLAG_OUTSIDE_PROBE) &&
+               !(p.flags & RPD_FLAG_NO_PROBE);
   if (probe) {
     // a domain that fills (nearly) the whole box leaves nothing to prove
     const long long S = s->grid.size, S1 = S + 1;

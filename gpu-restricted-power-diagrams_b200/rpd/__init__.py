@@ -151,13 +151,14 @@ FLAG_NO_PROBE = 64
 FLAG_NO_T_AHEAD = 128
 FLAG_KNN_WARP = 256
 FLAG_SAFE_RADIUS = 1024
+FLAG_OUTSIDE_PROBE = 2048
 FLAG_KNN_THREAD = 512
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRECISION_FP32 = 2
 COUNTER_NAMES = ["planes_tested", "clips", "vertex_tests", "vertices_made", "boundary_cells", "triangles",
                  "exports", "export_vertices", "outside_early", "cone_empty", "cones_skipped",
-                 "escalated_tests", "escalated_vertices", "escalated_radii"]
+                 "escalated_tests", "escalated_vertices", "escalated_radii", "start_corner_cells"]
 
 
 class Params(C.Structure):
@@ -181,7 +182,7 @@ class Stats(C.Structure):
     _fields_ = [("npasses", C.c_int), ("pass_cells", C.c_int * 8), ("pass_K", C.c_int * 8),
                 ("pass_P", C.c_int * 8), ("pass_V", C.c_int * 8), ("pass_T", C.c_int * 8),
                 ("pass_knn_ms", C.c_float * 8), ("pass_cell_ms", C.c_float * 8), ("status_hist", C.c_int * 11),
-                ("counters", C.c_ulonglong * 14), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
+                ("counters", C.c_ulonglong * 15), ("knn_candidates", C.c_ulonglong), ("total_ms", C.c_float),
                 ("kernel_launches", C.c_int), ("pass_cell_kernel_ms", C.c_float * 8), ("probe_outside", C.c_int),
                 ("probe_ms", C.c_float), ("pass_knn_variant", C.c_int * 8)]
 

@@ -201,13 +201,21 @@ rpd_grid *rpd_solver_export_grid(rpd_solver *s, int *err);
 #define RPD_FLAG_FRESH_NEIGHBOURS 32u /* recompute the neighbour table even when the
                                          seeds' positions and K are unchanged since
                                          the last launch (same results) */
-#define RPD_FLAG_NO_PROBE 64u       /* no outside probe before the first pass: every
-                                       seed gets its full K-nearest search (same
-                                       results) */
+#define RPD_FLAG_NO_PROBE 64u       /* no outside probe (the default; overrides
+                                       RPD_FLAG_OUTSIDE_PROBE) */
 #define RPD_FLAG_NO_T_AHEAD 128u    /* leave every triangle overflow of the first pass
                                        to the retry passes instead of restricting at
                                        once the cells the retries would settle (same
                                        results) */
+#define RPD_FLAG_OUTSIDE_PROBE 2048u /* before the first pass, settle the cells that a probe of
+                                       their 3x3x3 bins proves outside the domain (mass 0,
+                                       status success) without their K-nearest search and
+                                       clipping.  Moments equal the reference's; a status can
+                                       differ: where the reference's clipping of such a cell
+                                       fails in every pass (security radius not reached or a
+                                       cap overflow) it reports that failure, this success,
+                                       and a failure the reference counts can grow its retry
+                                       caps where these do not */
 #define RPD_FLAG_SAFE_RADIUS 1024u  /* --safeRadius: stop clipping on the weighted security-radius
                                        guard instead of the reference's Voronoi test d^2 > 4 R^2
                                        (ConvexCell.cl:364-382): with the neighbours sorted by
@@ -289,6 +297,10 @@ enum {
   RPD_CTR_ESCALATED_VERTICES, /* RPD_PRECISION_MIXED: vertices made in FP64 */
   RPD_CTR_ESCALATED_RADII,    /* RPD_PRECISION_MIXED: security-radius / outside tests
                                  decided on the exact FP64 radius */
+  RPD_CTR_START_CORNER,       /* boundary cells whose cones run from the reference's
+                                 start corner: no grid corner inside the cell, or caps
+                                 too tight to rule out an overflow of the reference's
+                                 cone clipping (P < planes + 4 or V < vertices + 8) */
   RPD_CTR_NUM
 };
 

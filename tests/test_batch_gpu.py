@@ -37,10 +37,10 @@ def build(rpd, sp, with_grid):
 
 def alone(rpd, x, g, p):
     """The diagram solved on its own: a first launch after its seeds were
-    set, so with the outside probe as in every batch replay (the probe can
-    settle in the first pass an empty cell outside the domain that a full
-    clip would retry, so per-pass cell counts depend on it).  Both settle
-    triangle overflows ahead."""
+    set, so with the outside probe where its flags ask for it, as in every
+    batch replay (the probe settles in the first pass cells outside the
+    domain that a full clip may retry, so per-pass cell counts depend on
+    it).  Both settle triangle overflows ahead."""
     s = rpd.Solver().set_points(x)
     if g is not None:
         s.set_grid(g)
@@ -72,8 +72,10 @@ def test_batch_equals_solves_alone(rpd):
             p.flags |= rpd.FLAG_FIRST_PASS_ONLY
         if i == 7:
             p.flags |= rpd.FLAG_REFERENCE_APEX
+        if i in (1, 2, 4, 8):
+            p.flags |= rpd.FLAG_OUTSIDE_PROBE
         if i == 9:
-            p.flags |= rpd.FLAG_NO_PROBE
+            p.flags |= rpd.FLAG_OUTSIDE_PROBE | rpd.FLAG_NO_PROBE
         if i == 10:
             p.flags |= rpd.FLAG_SAFE_RADIUS
         params.append(p)
@@ -83,7 +85,7 @@ def test_batch_equals_solves_alone(rpd):
     assert st["diagrams"] == 12 and st["cells"] == sum(len(s["xyzw"]) for s in sp)
     assert st["max_passes"] >= 3 and st["captures"] == 1
     assert st["probe_outside"] > 0  # the domains leave plainly-outside seeds to prove
-    assert solvers[9].stats()["probe_outside"] == 0
+    assert solvers[9].stats()["probe_outside"] == 0 and solvers[0].stats()["probe_outside"] == 0
     for i, s in enumerate(sp):
         assert_same(solvers[i], alone(rpd, s["xyzw"], grids[i], params[i]))
 
@@ -140,3 +142,22 @@ def test_batch_rejects_unsupported(rpd):
         rpd.Batch(solvers, rpd.Params.default(keep_distance=1)).launch()
     with pytest.raises(rpd.RpdError):
         rpd.Batch(solvers, rpd.Params.default(precision=rpd.PRECISION_MIXED))
+
+
+def test_batch_parity_with_oracle_larger(rpd):
+    """A larger uneven batch (12 diagrams up to 40K seeds, K 20/50/70, own
+    blobs at 24^3..56^3, one without a domain) against the FP64 oracle,
+    every cell of every diagram."""
+    sp = specs(12, seed=21, nmin=5000, nmax=40_000)
+    grids, solvers = build(rpd, sp, with_grid=lambda i: i != 4)
+    params = [rpd.Params.default(K=s["K"], P=30, V=40, T=100) for s in sp]
+    b = rpd.Batch(solvers, params)
+    b.launch()
+    for i, s in enumerate(sp):
+        ga = None
+        if grids[i] is not None:
+            a = grids[i].arrays()
+            ga = oracle.GridArrays(a["size"], a["in_domain"], a["points"], a["triangles"], a["tri_list"], a["offsets"])
+        ref, rst = oracle.solve(s["xyzw"].astype(np.float64), grid=ga, use_double=True, knn_mode=1, K=s["K"], P=30,
+                                V=40, T=100)
+        assert_parity(compare(solvers[i].moments(), solvers[i].status(), ref, rst))

@@ -134,32 +134,35 @@ def test_early_out_and_parking_do_not_change_results(rpd):
 
 
 def test_outside_probe_does_not_change_results(rpd):
-    """The outside probe (cells proven empty outside the domain from the 32
-    nearest of their 3x3x3 bins) changes no bit of any result."""
+    """The outside probe (RPD_FLAG_OUTSIDE_PROBE: cells proven empty outside
+    the domain from the seeds of their 3x3x3 bins) changes no bit of the
+    moments, nor here of the statuses (every cell it settles is one the
+    reference's clipping settles too)."""
     g = rpd.Grid.blob(60, 5, 2)
     x = jittered(40, seed=6, weights=True)
     s = rpd.Solver().set_points(x).set_grid(g)
+    probe = rpd.FLAG_OUTSIDE_PROBE
     fresh = rpd.FLAG_FRESH_NEIGHBOURS
-    s.launch(K=50, P=30, V=40, T=60, flags=fresh)
+    s.launch(K=50, P=30, V=40, T=60, flags=fresh | probe)
     st = s.stats()
     m1, s1 = s.moments(), s.status()
     print("probe", st["probe_outside"], "of", len(x), st["probe_ms"], "ms", st["passes"][0])
     assert st["probe_outside"] > len(x) // 4
     assert st["passes"][0]["cells"] == len(x)
-    s.launch(K=50, P=30, V=40, T=60, flags=fresh | rpd.FLAG_NO_PROBE)
+    s.launch(K=50, P=30, V=40, T=60, flags=fresh)
     assert s.stats()["probe_outside"] == 0
     assert np.array_equal(s.status(), s1)
     assert np.array_equal(s.moments(), m1)
     # a weight-only re-solve after a probed first launch builds the whole
     # neighbour table (no probe), which the next one keeps
     t = rpd.Solver().set_points(x).set_grid(g)
-    t.launch(K=50, P=30, V=40, T=60)
+    t.launch(K=50, P=30, V=40, T=60, flags=probe)
     assert t.stats()["probe_outside"] > 0
     x2 = x.copy()
     for it in range(2):
         x2[:, 3] = x[:, 3] * (0.5 + 0.25 * it)
         t.set_weights(x2[:, 3])
-        t.launch(K=50, P=30, V=40, T=60)
+        t.launch(K=50, P=30, V=40, T=60, flags=probe)
         st = t.stats()
         assert st["probe_outside"] == 0
         f = rpd.Solver().set_points(x2).set_grid(g)
@@ -202,7 +205,7 @@ def test_empty_cells_outside_the_domain(rpd):
     corner = (x[:, :3] < 150).all(axis=1) | (x[:, :3] > 850).all(axis=1)
     idx = np.where(corner)[0][::3]
     x[idx, 3] = 4 * h2
-    for flags in (0, rpd.FLAG_NO_PROBE):
+    for flags in (rpd.FLAG_OUTSIDE_PROBE, 0):
         met, got, gst, ref, rst, stats = run_case(rpd, x, grid=g, K=50, P=30, V=40,
                                                   flags=flags | rpd.FLAG_FRESH_NEIGHBOURS)
         assert (rst[idx] == 6).sum() > len(idx) // 2
