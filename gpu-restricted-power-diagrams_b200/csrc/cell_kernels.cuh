@@ -2364,48 +2364,74 @@ __device__ int last_clip(const CellLaunch &a, const unsigned *nrow, float4 s, in
   return -1;
 }
 
-// How many of the neighbours j+1 .. e may cut the current cell: their plane
-// (built as the clipping loop builds it) has a vertex of the cell on its far
-// side, with a margin of 1e-9 of the plane offset plus the cell radius R.
-// Every later cell lies in the current one, whose farthest point beyond a
-// plane is a vertex, so a neighbour that cuts none of its vertices cuts no
-// later cell either; the margin covers the rounding of the later cells'
-// vertices.  One neighbour per lane, every vertex in turn.
-template <int PREC>
-__device__ int cutters_ahead(const WarpCell &w, const CellLaunch &a, const unsigned *nrow, float4 s, int j, int e,
-                             double R, int lane) {
-  int cnt = 0;
-  for (int c0 = (j + 1) & ~31; c0 <= e; c0 += 32) {
-    const int i = c0 + lane;
-    bool cut = false;
-    if (i > j && i <= e) {
-      const float4 b = __ldg(&a.stored[__ldg(&nrow[i])]);
-      const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
-      const double nd2 = bx * bx + by * by + bz * bz;
-      const double len = sqrt(nd2), inv = 1.0 / len;
-      const double off = b.w <= kNoCellLimits ? len : (nd2 + (double(b.w) - double(s.w))) * (0.5 * inv);
-      Plane pl{-bx * inv, -by * inv, -bz * inv, off};
-      if constexpr (PREC == 2) pl = Plane{double(float(pl.x)), double(float(pl.y)), double(float(pl.z)), double(float(pl.w))};
-      const double tol = kTieEps - 1e-9 * (fabs(off) + R);
-      for (int v = 0; v < w.nv && !cut; ++v) {
-        const double cw = w.cw[v];
-        cut = plane_side(w.cx[v], w.cy[v], w.cz[v], cw, pl) > tol * fabs(cw);
-      }
+// Whether the reference's clipping of a cell proven outside the domain,
+// continued past neighbour j (clipped; the cell has w.np planes, w.nv
+// vertices and squared radius R2), surely ends in success.  It goes on to
+// the last neighbour e (last_clip; the lanes' bisectors pl / squared
+// distances nd2 / valid flags of neighbours i0 + lane serve the current
+// chunk), and of the neighbours j+1 .. e only those whose bisector has a
+// vertex of the current cell on its far side can cut a later cell: every
+// later cell lies in this one, whose farthest point beyond a plane is a
+// vertex (a margin of 1e-9 of the plane offset plus the radius covers the
+// rounding of the later cells' vertices).  With c of them, np + c < P keeps
+// every plane check before a clip below P and nv + 2c <= V every clip within
+// V (a cut adds at most one face to the closed cell, whose f faces make
+// 2f - 4 vertices); counting stops once c passes that.  The cell cannot
+// become empty (nonempty_cell gates the exits).  A later clip that meets a
+// degenerate cavity (inconsistent_boundary) is the one failure this cannot
+// foresee.  The FP32 clipping keeps no FP64 vertices: there every later
+// neighbour counts as a cut.  One neighbour per lane, every vertex in turn.
+template <int VS, int PREC>
+__device__ bool outside_certain(const WarpCell &w, const CellLaunch &a, const unsigned *nrow, float4 s, int i0, int j,
+                                const Plane &pl, double nd2, bool valid, double R2, double dw, int lane) {
+  const int cmax = min(a.P - w.np - 1, (a.V - w.nv) >> 1);  // the most cuts the caps allow
+  // the last neighbour clipped: in the current chunk from the lanes' data,
+  // past it from the table
+  int e;
+  {
+    const int i = i0 + lane;
+    const bool stop = i >= j && i < a.K && (!valid || radius_reached(nd2, R2 * (1.0 + 1e-9), dw));
+    const unsigned m = __ballot_sync(kFull, stop);
+    if (m) {
+      const int src = __ffs(m) - 1;
+      e = i0 + src - (__shfl_sync(kFull, valid, src) ? 0 : 1);
+    } else {
+      e = i0 + 32 < a.K ? last_clip(a, nrow, s, i0 + 32, R2, dw, lane) : -1;
     }
-    cnt += __popc(__ballot_sync(kFull, cut));
   }
-  return cnt;
-}
-
-// Whether clipping the neighbours after j up to e, of which c may cut the
-// cell, surely overflows no cap: the plane count grows by one per cut
-// (np + c < P keeps every plane check before a clip below P), and a cut adds
-// at most one face to the closed cell, whose f faces make 2f - 4 vertices
-// (nv + 2c <= V).  The cell cannot become empty either (nonempty_cell gates
-// the exits).  A later clip that meets a degenerate cavity
-// (inconsistent_boundary) is the one failure this cannot foresee.
-__device__ __forceinline__ bool caps_hold(int e, int j, int c, int np, int nv, int P, int V) {
-  return e >= 0 && (e == j || (np + c < P && nv + 2 * c <= V));
+  if (e < 0) return false;
+  if (e - j <= max(cmax, 0)) return e - j == 0 || cmax >= e - j;
+  if (cmax < 0) return false;
+  if constexpr (PREC > 0) {
+    return false;
+  } else {
+    const double R = sqrt(R2);
+    int c = 0;
+    for (int c0 = i0; c0 <= e; c0 += 32) {
+      const int i = c0 + lane;
+      Plane pc = pl;
+      if (c0 > i0 && i <= e) {
+        // a later chunk: the lanes build its bisectors as the clipping loop does
+        const float4 b = __ldg(&a.stored[__ldg(&nrow[i])]);
+        const double bx = double(b.x) - double(s.x), by = double(b.y) - double(s.y), bz = double(b.z) - double(s.z);
+        const double d2 = bx * bx + by * by + bz * bz;
+        const double len = sqrt(d2), inv = 1.0 / len;
+        const double off = b.w <= kNoCellLimits ? len : (d2 + (double(b.w) - double(s.w))) * (0.5 * inv);
+        pc = Plane{-bx * inv, -by * inv, -bz * inv, off};
+      }
+      bool cut = false;
+      if (i > j && i <= e) {
+        const double tol = kTieEps - 1e-9 * (fabs(pc.w) + R);
+        for (int v = 0; v < w.nv && !cut; ++v) {
+          const double cw = w.cw[v];
+          cut = plane_side(w.cx[v], w.cy[v], w.cz[v], cw, pc) > tol * fabs(cw);
+        }
+      }
+      c += __popc(__ballot_sync(kFull, cut));
+      if (c > cmax) return false;
+    }
+    return true;
+  }
 }
 
 // The vertex capacity a cell of this launch works with.  A batched launch's
@@ -2471,9 +2497,8 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
   const bool early = GRID && a.early_out && a.grid.sat != nullptr && a.wmin != nullptr && a.border_d == 0;
   double plain2 = early ? plain_radius2(a.grid, s, lane) : -1.0;
   // once the cell is proven outside (out_known), clipping stops where the
-  // rest of the reference's clipping surely succeeds (last_clip,
-  // cutters_ahead, caps_hold), else goes on, and the cell, once it succeeds,
-  // skips the restriction
+  // rest of the reference's clipping surely succeeds (outside_certain), else
+  // goes on, and the cell, once it succeeds, skips the restriction
   bool out_known = false;
   // the weighted security-radius guard (radius_reached): w_s - min w when
   // on (computed where used, so the default loop carries nothing), else -1
@@ -2542,9 +2567,7 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
           R2 = cell_radius2<VS>(w, lane);
           if (R2 <= plain2) {
             out_known = true;
-            const int e = last_clip(a, nrow, s, i0 + j, R2, safe_dw(), lane);
-            if (e >= 0 && caps_hold(e, i0 + j, cutters_ahead<PREC>(w, a, nrow, s, i0 + j, e, sqrt(R2), lane), w.np,
-                                    w.nv, a.P, a.V)) {
+            if (outside_certain<VS, PREC>(w, a, nrow, s, i0, i0 + j, pl, nd2, valid, R2, safe_dw(), lane)) {
               outside = true;
               break;
             }
@@ -2570,11 +2593,9 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
               out = R2 <= plain2;
             }
             if (out) {
-              // the FP64 vertices are not kept here: every later neighbour
-              // counts as a cut
               out_known = true;
-              const int e = last_clip(a, nrow, s, i0 + j, R2 >= 0.0 ? R2 : double(R2hi), safe_dw(), lane);
-              if (caps_hold(e, i0 + j, e - i0 - j, w.np, w.nv, a.P, a.V)) {
+              if (outside_certain<VS, PREC>(w, a, nrow, s, i0, i0 + j, pl, nd2, valid,
+                                            R2 >= 0.0 ? R2 : double(R2hi), safe_dw(), lane)) {
                 outside = true;
                 break;
               }
