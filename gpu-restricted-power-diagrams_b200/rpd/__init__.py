@@ -10,8 +10,10 @@ without an sm_100 device raises.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -38,6 +40,26 @@ class RpdError(RuntimeError):
 
 
 _lib = None
+
+# Live library objects, closed in dependency order when the interpreter exits
+# (servers, batches and solvers before the contexts and grids they use), so
+# that no handle is released after the library or the CUDA runtime is torn
+# down.
+_live = {kind: weakref.WeakSet() for kind in ("server", "batch", "solver", "grid", "context")}
+
+
+def _track(kind, obj):
+    _live[kind].add(obj)
+
+
+@atexit.register
+def _close_all():
+    for kind in ("server", "batch", "solver", "grid", "context"):
+        for obj in list(_live[kind]):
+            try:
+                obj.close()
+            except Exception:
+                pass
 
 # rpd_part_reduce_fn: (sums, nsum, maxes, nmax, user) -> 0
 PART_REDUCE = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_longlong), C.c_int, C.POINTER(C.c_longlong), C.c_int, C.c_void_p)
@@ -213,6 +235,7 @@ class Context:
         self.h = lib().rpd_context_create(device, C.byref(err))
         if not self.h:
             raise RpdError(err.value, f"no usable sm_100 device {device}")
+        _track("context", self)
 
     def error(self) -> str:
         return lib().rpd_context_error(self.h).decode()
@@ -295,6 +318,7 @@ class Solver:
         self.h = lib().rpd_solver_create(self.ctx.h, C.byref(err))
         if not self.h:
             raise RpdError(err.value, self.ctx.error())
+        _track("solver", self)
 
     def set_points(self, xyzw):
         x = as_xyzw(xyzw)
@@ -546,6 +570,7 @@ class Batch:
         if not self.h:
             raise RpdError(err.value, self.ctx.error())
         self._keep = (hs, pa)
+        _track("batch", self)
 
     def launch(self):
         self.ctx.check(lib().rpd_batch_launch(self.h))
@@ -597,6 +622,7 @@ class Grid:
 
     def __init__(self, handle=None):
         self.h = handle
+        _track("grid", self)
 
     @classmethod
     def from_arrays(cls, size, in_domain, points, triangles, tri_list, offsets):
@@ -780,6 +806,7 @@ class Server:
         self.h = lib().rpd_server_create(device, slots, mem_budget, C.byref(err))
         if not self.h:
             raise RpdError(err.value, "server create")
+        _track("server", self)
         self._out = {}     # ticket -> moments buffer (kept alive until waited for)
         self._grids = []   # grids used: they must outlive the server
 
