@@ -1404,6 +1404,9 @@ void solver_trim(rpd_solver *s) {
   s->defer_fail.release();
   s->defer_ctr.release();
   s->defer_chunk_slot.release();
+  s->hess.release();  // --hessian rows are read out before a trim
+  s->hessid.release();
+  s->hess_h = 0;
 }
 
 size_t solver_device_bytes(const rpd_solver *s) {

@@ -54,6 +54,8 @@ struct Request {
   const rpd_grid *grid = nullptr;
   rpd_params params{};
   double *moments = nullptr;
+  double *hessian = nullptr;  // --hessian rows (hessian_h > 0), user order
+  int *hessian_ids = nullptr;
   size_t need = 0;          // transient device bytes while it runs
   size_t new_resident = 0;  // resident bytes it adds (a new session, a new grid)
   Clock::time_point submitted, admitted, done;
@@ -95,8 +97,10 @@ size_t transient_bytes(int n, const rpd_params &p) {
   const size_t P = size_t(std::min(255, p.P * 8)), V = size_t(std::min(256, p.V * 8)),
                T = size_t(std::min(4096, p.T * 8));
   const size_t slot = 144 + 32 * P + 44 * V + 4 * T;
+  // --hessian: the rows on the device and their user-order staging
+  const size_t hess = p.hessian_h > 0 ? 2 * size_t(n) * size_t(p.hessian_h) * (8 * size_t(p.hessian_hc) + 4) : 0;
   return size_t(n) * (12 + 16 + 32 + 12) + cap * (slot / 4 + 40 * (T / 32 + 1) / 4) +
-         size_t(n) / 4 * size_t(p.K) * 8 * 4 + (size_t(1) << 20);
+         size_t(n) / 4 * size_t(p.K) * 8 * 4 + hess + (size_t(1) << 20);
 }
 
 }  // namespace
@@ -205,6 +209,7 @@ struct rpd_server {
       }
       if (rc == RPD_OK && s->solver) rc = rpd_solver_launch(s->solver, &r->params);
       if (rc == RPD_OK && r->moments) rc = rpd_solver_get_moments(s->solver, r->moments, RPD_HOST);
+      if (rc == RPD_OK && r->hessian) rc = rpd_solver_get_hessian(s->solver, r->hessian, r->hessian_ids, RPD_HOST);
       if (s->solver) {
         rpd_solver_get_stats(s->solver, &st);
         rpd::solver_trim(s->solver);
@@ -335,6 +340,13 @@ void rpd_server_destroy(rpd_server *sv) {
 
 int rpd_server_submit_solve(rpd_server *sv, const float *xyzw, int n, const rpd_grid *grid, const rpd_params *p,
                             double *moments, int *session) {
+  if (p && p->hessian_h != 0) return RPD_ERR_INVALID;  // rows only through the _hessian form
+  return rpd_server_submit_solve_hessian(sv, xyzw, n, grid, p, moments, nullptr, nullptr, session);
+}
+
+int rpd_server_submit_solve_hessian(rpd_server *sv, const float *xyzw, int n, const rpd_grid *grid,
+                                    const rpd_params *p, double *moments, double *hessian, int *hessian_ids,
+                                    int *session) {
   if (!sv || !xyzw || n <= 0) return RPD_ERR_INVALID;
   auto r = std::make_unique<Request>();
   r->n = n;
@@ -342,8 +354,12 @@ int rpd_server_submit_solve(rpd_server *sv, const float *xyzw, int n, const rpd_
   r->grid = grid;
   if (p) r->params = *p;
   else rpd_params_default(&r->params);
-  if (r->params.hessian_h != 0) return RPD_ERR_INVALID;  // requests return moments only
+  if (r->params.hessian_h < 0 || (r->params.hessian_h > 0 && (!hessian || !hessian_ids))) return RPD_ERR_INVALID;
   r->moments = moments;
+  if (r->params.hessian_h > 0) {
+    r->hessian = hessian;
+    r->hessian_ids = hessian_ids;
+  }
   r->need = transient_bytes(n, r->params);
   r->new_resident = resident_bytes(n, r->params);
   std::lock_guard<std::mutex> lock(sv->mu);
@@ -363,14 +379,24 @@ int rpd_server_submit_solve(rpd_server *sv, const float *xyzw, int n, const rpd_
 }
 
 int rpd_server_submit_reweight(rpd_server *sv, int session, const float *w, const rpd_params *p, double *moments) {
+  if (p && p->hessian_h != 0) return RPD_ERR_INVALID;  // rows only through the _hessian form
+  return rpd_server_submit_reweight_hessian(sv, session, w, p, moments, nullptr, nullptr);
+}
+
+int rpd_server_submit_reweight_hessian(rpd_server *sv, int session, const float *w, const rpd_params *p,
+                                       double *moments, double *hessian, int *hessian_ids) {
   if (!sv || !w) return RPD_ERR_INVALID;
   auto r = std::make_unique<Request>();
   r->reweight = true;
   r->session = session;
   if (p) r->params = *p;
   else rpd_params_default(&r->params);
-  if (r->params.hessian_h != 0) return RPD_ERR_INVALID;  // requests return moments only
+  if (r->params.hessian_h < 0 || (r->params.hessian_h > 0 && (!hessian || !hessian_ids))) return RPD_ERR_INVALID;
   r->moments = moments;
+  if (r->params.hessian_h > 0) {
+    r->hessian = hessian;
+    r->hessian_ids = hessian_ids;
+  }
   std::lock_guard<std::mutex> lock(sv->mu);
   if (sv->stop) return RPD_ERR_INVALID;
   auto it = sv->sessions.find(session);

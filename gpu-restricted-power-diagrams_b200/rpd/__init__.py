@@ -103,6 +103,10 @@ def lib():
         L.rpd_server_submit_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.POINTER(C.c_int)]
         L.rpd_server_submit_reweight.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.rpd_server_submit_solve_hessian.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                                      C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+        L.rpd_server_submit_reweight_hessian.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                         C.c_void_p, C.c_void_p]
         L.rpd_server_wait.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.rpd_server_release.argtypes = [C.c_void_p, C.c_int]
         L.rpd_server_bytes_in_use.restype = C.c_size_t
@@ -810,19 +814,28 @@ class Server:
         self._out = {}     # ticket -> moments buffer (kept alive until waited for)
         self._grids = []   # grids used: they must outlive the server
 
+    @staticmethod
+    def _hessian_buffers(n, p):
+        if p.hessian_h <= 0:
+            return None
+        return (np.zeros((n, p.hessian_h, p.hessian_hc), np.float64), np.zeros((n, p.hessian_h), np.int32))
+
     def solve(self, xyzw, grid=None, params=None, **kw):
-        """Submits a new session's solve; returns (ticket, session)."""
+        """Submits a new session's solve; returns (ticket, session).  With
+        hessian_h > 0 the request also returns its Hessian rows (wait)."""
         x = as_xyzw(xyzw)
         p = params if params is not None else Params.default(**kw)
         out = np.zeros((len(x), 4), np.float64)
+        hb = self._hessian_buffers(len(x), p)
         sess = C.c_int(-1)
         if grid is not None:
             self._grids.append(grid)
-        t = lib().rpd_server_submit_solve(self.h, _ptr(x), len(x), grid.h if grid is not None else None,
-                                          C.byref(p), _ptr(out), C.byref(sess))
+        t = lib().rpd_server_submit_solve_hessian(self.h, _ptr(x), len(x), grid.h if grid is not None else None,
+                                                  C.byref(p), _ptr(out), _ptr(hb[0]) if hb else None,
+                                                  _ptr(hb[1]) if hb else None, C.byref(sess))
         if t < 0:
             raise RpdError(t, "submit solve")
-        self._out[t] = out
+        self._out[t] = (out, hb)
         return t, sess.value
 
     def reweight(self, session: int, w, params=None, **kw) -> int:
@@ -830,19 +843,30 @@ class Server:
         w = np.ascontiguousarray(w, np.float32)
         p = params if params is not None else Params.default(**kw)
         out = np.zeros((len(w), 4), np.float64)
-        t = lib().rpd_server_submit_reweight(self.h, session, _ptr(w), C.byref(p), _ptr(out))
+        hb = self._hessian_buffers(len(w), p)
+        t = lib().rpd_server_submit_reweight_hessian(self.h, session, _ptr(w), C.byref(p), _ptr(out),
+                                                     _ptr(hb[0]) if hb else None, _ptr(hb[1]) if hb else None)
         if t < 0:
             raise RpdError(t, "submit reweight")
-        self._out[t] = out
+        self._out[t] = (out, hb)
         return t
 
-    def wait(self, ticket: int):
+    def wait(self, ticket: int, hessian: bool = False):
+        """(moments (n,4) in user order, request info); with hessian=True
+        also the Hessian rows ((n,H) areas for HC=1 or (n,H,4), ids (n,H)),
+        or None when the request asked for none."""
         info = RequestInfo()
         rc = lib().rpd_server_wait(self.h, ticket, C.byref(info))
-        out = self._out.pop(ticket)
+        out, hb = self._out.pop(ticket)
         if rc != RPD_OK:
             raise RpdError(rc, f"request {ticket}: {info.error.decode(errors='replace')}")
-        return out, info.as_dict()
+        if not hessian:
+            return out, info.as_dict()
+        rows = None
+        if hb is not None:
+            vals, ids = hb
+            rows = (vals[:, :, 0] if vals.shape[2] == 1 else vals), ids
+        return out, info.as_dict(), rows
 
     def release(self, session: int):
         rc = lib().rpd_server_release(self.h, session)

@@ -430,6 +430,17 @@ int rpd_server_submit_solve(rpd_server *sv, const float *xyzw, int n, const rpd_
 /* A weight-only re-solve of a session: n weights (host memory, user order),
  * copied; runs after the session's earlier requests. */
 int rpd_server_submit_reweight(rpd_server *sv, int session, const float *w, const rpd_params *p, double *moments);
+/* The same requests with --hessian output: with p->hessian_h > 0 the
+ * request also writes the Hessian rows of its solve into `hessian` (n *
+ * hessian_h * hessian_hc doubles) and `hessian_ids` (n * hessian_h ints), user
+ * order, as rpd_solver_get_hessian gives them (both kept valid by the caller
+ * until the request is done; required then).  The plain submits reject
+ * hessian_h > 0. */
+int rpd_server_submit_solve_hessian(rpd_server *sv, const float *xyzw, int n, const rpd_grid *grid,
+                                    const rpd_params *p, double *moments, double *hessian, int *hessian_ids,
+                                    int *session);
+int rpd_server_submit_reweight_hessian(rpd_server *sv, int session, const float *w, const rpd_params *p,
+                                       double *moments, double *hessian, int *hessian_ids);
 /* Blocks until the ticket's request is done and returns its status; each
  * ticket is waited for once. */
 int rpd_server_wait(rpd_server *sv, int ticket, rpd_request_info *info);

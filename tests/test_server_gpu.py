@@ -114,3 +114,45 @@ def test_failed_request_reports_error(rpd):
         t2, s2 = sv.solve(jittered(10, seed=1), K=20)
         m, info = sv.wait(t2)
         assert info["status"] == 0 and abs(m[:, 3].sum() / 1e9 - 1) < 1e-6
+
+
+def test_hessian_rows_served(rpd):
+    """Requests with --hessian rows (rpd_server_submit_*_hessian): the rows a
+    served solve and a served weight-only re-solve return equal those of the
+    same launches on a solver of their own, bit for bit, while another
+    session's plain requests share the slots; the plain submit rejects
+    hessian_h > 0."""
+    g = rpd.Grid.blob(40, 5, 2)
+    x = jittered(24, seed=6, weights=True)
+    y = jittered(20, seed=7, weights=True)
+    w = np.clip(x[:, 3] * 1.5, 0, None).astype(np.float32)
+    kw1 = dict(K=50, P=30, V=40, T=100, hessian_h=40, hessian_hc=1)
+    kw4 = dict(K=50, P=30, V=40, T=100, hessian_h=40, hessian_hc=4)
+    with rpd.Server(slots=2) as sv:
+        t1, s1 = sv.solve(x, grid=g, **kw1)
+        t2, s2 = sv.solve(y, grid=g, K=50, P=30, V=40, T=100)
+        t3 = sv.reweight(s1, w, **kw4)
+        m1, _, rows1 = sv.wait(t1, hessian=True)
+        m2, _, rows2 = sv.wait(t2, hessian=True)
+        m3, _, rows3 = sv.wait(t3, hessian=True)
+        sv.release(s1)
+        sv.release(s2)
+        p = rpd.Params.default(K=50, hessian_h=8)
+        out = np.zeros((len(x), 4), np.float64)
+        sess = rpd.C.c_int(-1)
+        assert rpd.lib().rpd_server_submit_solve(sv.h, rpd._ptr(x), len(x), None, rpd.C.byref(p), rpd._ptr(out),
+                                                 rpd.C.byref(sess)) < 0
+    assert rows2 is None
+    ref = rpd.Solver().set_points(x).set_grid(g)
+    ref.launch(**kw1)
+    v1, i1 = ref.hessian(40, 1)
+    assert np.array_equal(m1, ref.moments())
+    assert np.array_equal(rows1[0], v1) and np.array_equal(rows1[1], i1)
+    assert (i1[:, 0] >= 0).sum() > len(x) // 10  # cells inside the domain have rows
+    x2 = x.copy()
+    x2[:, 3] = w
+    ref2 = rpd.Solver().set_points(x2).set_grid(g)
+    ref2.launch(**kw4)
+    v4, i4 = ref2.hessian(40, 4)
+    assert np.array_equal(m3, ref2.moments())
+    assert np.array_equal(rows3[0], v4) and np.array_equal(rows3[1], i4)
