@@ -44,6 +44,11 @@ struct DiagStatic {
   const int *wmin;  // the smallest weight of the seeds that are not walls (float_to_ordered)
   int T_ahead;      // first pass: triangle overflows up to this count parked at once (0: off)
   int probe;        // 1: the outside probe settles the seeds it can before the first pass
+  // --hessian rows (H > 0): per seed H facets of HC values and their
+  // neighbours, as rpd_solver_launch writes them (the inline kernels only)
+  double *hess;
+  int *hessid;
+  int H, HC;
   int safe_radius;  // the weighted security-radius guard (RPD_FLAG_SAFE_RADIUS)
   float cube_eps;
   DevGrid grid;
@@ -284,6 +289,10 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     a.status = g.status;
     a.out = g.out;
     a.diag = d;
+    a.hess = g.hess;
+    a.hessid = g.hessid;
+    a.H = g.H;
+    a.HC = g.HC;
     a.defer = pa.defer;
     pl.descs[d] = a;
     a.defer = DeferQueue();
@@ -449,8 +458,8 @@ int check_params(rpd_context *ctx, const rpd_params &p) {
     set_error(ctx, "batched solves collect no work counters (RPD_FLAG_COUNTERS)");
     return RPD_ERR_INVALID;
   }
-  if (p.hessian_h != 0) {
-    set_error(ctx, "batched solves return no Hessian rows (hessian_h > 0): use rpd_solver_launch");
+  if (p.hessian_h < 0 || (p.hessian_h > 0 && p.hessian_hc != 1 && p.hessian_hc != 4)) {
+    set_error(ctx, "hessian_h must be >= 0 and hessian_hc 1 or 4");
     return RPD_ERR_INVALID;
   }
   if (p.precision != RPD_PRECISION_FP64) {
@@ -525,6 +534,23 @@ int describe(rpd_batch *b, std::vector<DiagStatic> &out) {
       }
       g.probe = s->grid_nonplain < 0.95 * double(S * S * S) ? 1 : 0;
     }
+    g.hess = nullptr;
+    g.hessid = nullptr;
+    g.H = g.HC = 0;
+    if (p.hessian_h > 0) {
+      // rows are summed in the cell's own warp: no cells parked ahead, no
+      // probe (as rpd_solver_launch)
+      if ((e = s->hess.ensure(sizeof(double) * size_t(n) * p.hessian_h * p.hessian_hc)) != cudaSuccess)
+        return map_cuda(ctx, e, "alloc hessian");
+      if ((e = s->hessid.ensure(sizeof(int) * size_t(n) * p.hessian_h)) != cudaSuccess)
+        return map_cuda(ctx, e, "alloc hessian");
+      g.hess = s->hess.as<double>();
+      g.hessid = s->hessid.as<int>();
+      g.H = p.hessian_h;
+      g.HC = p.hessian_hc;
+      g.T_ahead = 0;
+      g.probe = 0;
+    }
     g.grid = s->grid;
     g.status = s->status.as<int>();
     g.out = s->out.as<double4>();
@@ -550,6 +576,7 @@ int capture(rpd_batch *b) {
   long long cells = 0, table = 0;
   int Kmin = kMaxK, Kmax = 0, Pmax = 0, Vmax = 0, Tmax = 0, J = 0;
   bool any_grid = false, any_plain = false, defer = true, any_safe = false;
+  int hess_hc = 0;  // the Hessian rows' HC of the diagrams that ask for rows (one for the batch)
   bool class_used[kKnnClasses] = {};
   long class_rows[kKnnClasses] = {};
   long rows_grid0 = 0, rows_plain0 = 0;  // the first pass's rows
@@ -568,6 +595,14 @@ int capture(rpd_batch *b) {
     (g.grid.size > 0 ? any_grid : any_plain) = true;
     if (g.safe_radius) any_safe = true;
     if (b->params[d].flags & RPD_FLAG_NO_DEFER) defer = false;
+    if (g.H > 0) {
+      if (hess_hc && hess_hc != g.HC) {
+        set_error(ctx, "batch: Hessian rows with one hessian_hc for every diagram that asks for them");
+        return RPD_ERR_INVALID;
+      }
+      hess_hc = g.HC;
+      defer = false;  // rows are summed in the cell's own warp
+    }
     for (int c = 0; c < kKnnClasses; ++c)
       if (knn_slots(g.K0) == kKnnClassSlots[c]) {
         class_used[c] = true;
@@ -612,7 +647,8 @@ int capture(rpd_batch *b) {
   for (int j = 0; j <= J; ++j) {
     const int P = std::min(grow(Pmax, j), kMaxP), V = std::min(grow(Vmax, j), kMaxV),
               T = std::min(grow(Tmax, j), kMaxT), K = std::min(grow(Kmax, j), kMaxK);
-    if ((any_grid && !cell_caps_fit(P, V, T, true)) || (any_plain && !cell_caps_fit(P, V, T, false))) break;
+    if ((any_grid && !cell_caps_fit(P, V, T, true, hess_hc)) || (any_plain && !cell_caps_fit(P, V, T, false, hess_hc)))
+      break;
     Pb.push_back(P);
     Vb.push_back(V);
     Tb.push_back(T);
@@ -842,6 +878,7 @@ int capture(rpd_batch *b) {
     cb.V = Vb[j];
     cb.T = Tb[j];
     cb.T_slot = j == 0 && dq.slots ? Tslot0 : 0;
+    cb.HC = hess_hc;
     cb.after_cell = j == 0 ? b->ev[2] : nullptr;
     // the first pass's rows are every cell: one warp per row; the retries'
     // rows are known on the device only: persistent, rows from a counter
@@ -998,7 +1035,8 @@ int rpd_batch_launch(rpd_batch *b) {
     s->knn_full_K = b->statics[d].probe ? 0 : b->params[d].K;
     s->used_on = false;
     s->used_count = -1;
-    s->hess_h = 0;
+    s->hess_h = b->statics[d].H;
+    s->hess_hc = b->statics[d].HC;
     s->have_results = true;
   }
   // diagrams whose schedule outgrew the capture: solved alone

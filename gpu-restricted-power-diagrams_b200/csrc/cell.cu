@@ -6,13 +6,16 @@ namespace rpd {
 
 size_t cell_warp_smem(int P, int V, int T, bool grid) { return make_layout(P, V, T, grid).total; }
 
-bool cell_caps_fit(int P, int V, int T, bool grid) { return warps_per_block_for(make_layout(P, V, T, grid)) > 0; }
+bool cell_caps_fit(int P, int V, int T, bool grid, int hc) {
+  return warps_per_block_for(make_layout(P, V, T, grid, hc)) > 0;
+}
 
 cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches) {
   if (b.ndiag <= 0) return cudaSuccess;
   if (b.safe) return cell_batch_launch_safe(b, st, sm_count, launches);
   if (b.P > kMaxP || b.V > kMaxV || b.T > kMaxT || b.P < 7 || b.V < 8) return cudaErrorInvalidValue;
-  const Layout Lg = make_layout(b.P, b.V, b.T, true, 0, b.T_slot), Lp = make_layout(b.P, b.V, b.T, false);
+  if (b.HC && b.defer.slots) return cudaErrorInvalidValue;  // Hessian rows are summed inline
+  const Layout Lg = make_layout(b.P, b.V, b.T, true, b.HC, b.T_slot), Lp = make_layout(b.P, b.V, b.T, false, b.HC);
   if (b.defer.slots && (b.defer.slot_bytes < slot_bytes_for(Lg, Lg.T) || b.defer.max_chunks * b.defer.chunk < Lg.T))
     return cudaErrorInvalidValue;
   const int vs = Lg.Vc / 32;

@@ -172,7 +172,7 @@ cudaError_t probe_batch_launch(const ProbeLaunch *probes, const int *start, int 
                                cudaStream_t st);
 
 // Whether one warp's layout for these caps fits a block's shared memory.
-bool cell_caps_fit(int P, int V, int T, bool grid);
+bool cell_caps_fit(int P, int V, int T, bool grid, int hc = 0);
 
 // The cells of many diagrams in shared persistent launches (batched
 // solves).  Row prefixes and launch records live on the device, written by
@@ -193,6 +193,7 @@ struct CellBatch {
   long rows_grid = -1, rows_plain = -1;
   int *work = nullptr;  // one device int: the row counter of persistent launches (optional)
   bool safe = false;    // a diagram uses the weighted security-radius guard (its launch record decides)
+  int HC = 0;           // Hessian rows' components (a diagram with rows; then no defer queue), else 0
 };
 cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches = nullptr);
 // The same with the guard compiled in (cell_safe.cu).

@@ -25,7 +25,8 @@ cudaError_t cell_launch_safe(const CellLaunch &a, cudaStream_t st, int sm_count,
 cudaError_t cell_batch_launch_safe(const CellBatch &b, cudaStream_t st, int sm_count, int *launches) {
   if (b.ndiag <= 0) return cudaSuccess;
   if (b.P > kMaxP || b.V > kMaxV || b.T > kMaxT || b.P < 7 || b.V < 8) return cudaErrorInvalidValue;
-  const Layout Lg = make_layout(b.P, b.V, b.T, true, 0, b.T_slot), Lp = make_layout(b.P, b.V, b.T, false);
+  if (b.HC && b.defer.slots) return cudaErrorInvalidValue;  // Hessian rows are summed inline
+  const Layout Lg = make_layout(b.P, b.V, b.T, true, b.HC, b.T_slot), Lp = make_layout(b.P, b.V, b.T, false, b.HC);
   if (b.defer.slots && (b.defer.slot_bytes < slot_bytes_for(Lg, Lg.T) || b.defer.max_chunks * b.defer.chunk < Lg.T))
     return cudaErrorInvalidValue;
   const int vs = Lg.Vc / 32;

@@ -500,8 +500,14 @@ int rpd_compare_moments(const double *a, const double *b, size_t n, rpd_moment_d
  * rpd_solver_launch would give it (statuses, moments, stats' passes and
  * histogram), read with the solver's own getters.  Changing a solver's seeds
  * or domain is allowed between launches (the graph is captured again);
- * changing weights (rpd_solver_set_weights) is not a change.  Not supported:
- * RPD_FLAG_COUNTERS and used cells (keep_distance >= 0 with a domain). */
+ * changing weights (rpd_solver_set_weights) is not a change.  --hessian rows
+ * (hessian_h > 0, one hessian_hc for every diagram that asks for them) are
+ * read with rpd_solver_get_hessian; their cells are summed in the cell's own
+ * warp, so a batch with rows parks no boundary cell for the chunked kernel
+ * and settles no triangle overflow ahead for any of its diagrams: per-pass
+ * counts then equal those of rpd_solver_launch with RPD_FLAG_NO_DEFER (the
+ * results, every solve's alike).  Not supported: RPD_FLAG_COUNTERS, used
+ * cells (keep_distance >= 0 with a domain), precision other than FP64. */
 typedef struct rpd_batch rpd_batch;
 typedef struct rpd_batch_stats {
   int diagrams;

@@ -161,3 +161,37 @@ def test_batch_parity_with_oracle_larger(rpd):
         ref, rst = oracle.solve(s["xyzw"].astype(np.float64), grid=ga, use_double=True, knn_mode=1, K=s["K"], P=30,
                                 V=40, T=100)
         assert_parity(compare(solvers[i].moments(), solvers[i].status(), ref, rst))
+
+
+def test_batch_hessian_rows(rpd):
+    """Batched diagrams with --hessian rows (rpd_solver_get_hessian on each
+    solver): rows, moments and statuses equal those of each diagram solved
+    alone, bit for bit; the batch then sums boundary cells in their own warps
+    (no parked cells, no triangle overflows settled ahead), so its per-pass
+    counts are those of a lone solve with RPD_FLAG_NO_DEFER.  Diagrams with
+    rows must share hessian_hc."""
+    sp = specs(6, seed=13, nmin=2000, nmax=12_000)
+    grids, solvers = build(rpd, sp, with_grid=lambda i: i != 2)
+    params = []
+    for i, s in enumerate(sp):
+        kw = dict(K=s["K"], P=30, V=40, T=60)
+        if i % 2 == 0:
+            kw.update(hessian_h=40, hessian_hc=1)
+        params.append(rpd.Params.default(**kw))
+    b = rpd.Batch(solvers, params)
+    b.launch()
+    for i, s in enumerate(sp):
+        p = params[i]
+        if p.hessian_h == 0:
+            p = rpd.Params.default(K=s["K"], P=30, V=40, T=60, flags=rpd.FLAG_NO_DEFER)
+        ref = alone(rpd, s["xyzw"], grids[i], p)
+        assert_same(solvers[i], ref)
+        if params[i].hessian_h:
+            v, ids = solvers[i].hessian(40, 1)
+            rv, rids = ref.hessian(40, 1)
+            assert np.array_equal(v, rv) and np.array_equal(ids, rids)
+            assert (ids[:, 0] >= 0).any()
+        ref.close()
+    mixed = [rpd.Params.default(K=s["K"], hessian_h=20, hessian_hc=1 + 3 * (i % 2)) for i, s in enumerate(sp)]
+    with pytest.raises(rpd.RpdError):
+        rpd.Batch(solvers, mixed).launch()
