@@ -49,6 +49,7 @@ struct DiagStatic {
   double *hess;
   int *hessid;
   int H, HC;
+  int *tri_count;  // n: the triangle overflows' counts (CellLaunch::tri_count; null: none)
   int safe_radius;  // the weighted security-radius guard (RPD_FLAG_SAFE_RADIUS)
   float cube_eps;
   DevGrid grid;
@@ -293,6 +294,8 @@ __global__ void __launch_bounds__(1024) k_plan(const DiagStatic *__restrict__ ds
     a.hessid = g.hessid;
     a.H = g.H;
     a.HC = g.HC;
+    a.tri_count = g.tri_count;
+    a.tri_first = pa.pass == 0 ? 1 : 0;
     a.defer = pa.defer;
     pl.descs[d] = a;
     a.defer = DeferQueue();
@@ -537,6 +540,11 @@ int describe(rpd_batch *b, std::vector<DiagStatic> &out) {
     g.hess = nullptr;
     g.hessid = nullptr;
     g.H = g.HC = 0;
+    g.tri_count = nullptr;
+    if (grid && s->grid.tsat) {
+      if ((e = s->tri_count.ensure(sizeof(int) * size_t(n))) != cudaSuccess) return map_cuda(ctx, e, "alloc");
+      g.tri_count = s->tri_count.as<int>();
+    }
     if (p.hessian_h > 0) {
       // rows are summed in the cell's own warp: no cells parked ahead, no
       // probe (as rpd_solver_launch)

@@ -85,6 +85,13 @@ struct CellLaunch {
   float cube_eps = 0.f;            // box [-eps, 1000+eps]^3
   int out_domain = 0;              // GRID_OUT_DOMAIN fallback for the start corner
   int early_out = 1;               // stop clipping cells proven outside the domain (needs grid.sat)
+  // Triangle counts of the cells that failed with triangle_overflow (n ints,
+  // stored order; optional, with disjoint lists): the first pass of a launch
+  // (tri_first) writes every row's (0: none); a later pass settles a row whose
+  // count is above its T at once -- the clip would give the same cell and
+  // the same overflow
+  int *tri_count = nullptr;
+  int tri_first = 0;
   const int *wmin = nullptr;       // the smallest weight of the seeds that are not walls
                                    // (float_to_ordered); null: no early exit
   int inner_apex = 1;              // cone apex at a grid corner inside the cell when there is one

@@ -2101,7 +2101,10 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
       // more than T: the retry passes would clip this cell again to the
       // same cell and restrict it with a larger T; within T_ahead it is
       // parked now, its ids gathered straight into its slot
-      if (INL || count > a.T_ahead || !a.defer.slots) return kTriangleOverflow;
+      if (INL || count > a.T_ahead || !a.defer.slots) {
+        if (a.tri_count && lane == 0) a.tri_count[sid_of_cell] = count;
+        return kTriangleOverflow;
+      }
       ahead = true;
     }
   }
@@ -2110,7 +2113,7 @@ __device__ int restrict_to_domain(WarpCell &w, const CellLaunch &a, const Layout
   if (ahead) {
     if (lane == 0) slot = atomicAdd(&dq.counters[0], 1);
     slot = __shfl_sync(kFull, slot, 0);
-    if (slot >= dq.capacity) return kTriangleOverflow;  // the retry passes take it
+    if (slot >= dq.capacity) return kTriangleOverflow;  // the retry passes take it (count unknown to them)
     tl = slot_list(dq, slot, L);
     tcap = L.T;
   }
@@ -2459,6 +2462,20 @@ __device__ __forceinline__ void cell_row(const CellLaunch &a, const Layout &L, u
   // Hessian rows run inline only (no defer queue)
   if constexpr (INL) {
     if (a.hess && lane == 0) a.hessid[size_t(sid) * a.H] = -1;  // an empty row until the cell succeeds
+  }
+  if constexpr (GRID) {
+    if (a.tri_count && a.border_d == 0) {
+      if (a.tri_first) {
+        if (lane == 0) a.tri_count[sid] = 0;
+      } else if (a.tri_count[sid] > a.T) {
+        // clipped again it would be the same cell, past T again
+        if (lane == 0) {
+          a.status[sid] = kTriangleOverflow;
+          a.out[sid] = make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+        return;
+      }
+    }
   }
   const float4 s = a.stored[sid];
   double *tr = (a.trace && sid == a.trace_seed) ? a.trace : nullptr;

@@ -477,6 +477,11 @@ int run_pass(rpd_solver *s, const int *ids, int num, int K, int P, int V, int T,
   }
   a.grid = s->grid;
   a.precision = s->precision;
+  if (s->grid.tsat && border_d == 0) {
+    if ((e = s->tri_count.ensure(sizeof(int) * size_t(s->n))) != cudaSuccess) return map_cuda(ctx, e, "alloc");
+    a.tri_count = s->tri_count.as<int>();
+    a.tri_first = pi == 0 ? 1 : 0;
+  }
   a.status = s->status.as<int>();
   a.out = s->out.as<double4>();
   a.counters = ctr;
@@ -1392,6 +1397,7 @@ void solver_share_grid(rpd_solver *dst, const rpd_solver *src) {
 void solver_trim(rpd_solver *s) {
   s->bin_ws.release();
   s->knn_part.release();
+  s->tri_count.release();
   s->knn_user.release();
   s->ids_a.release();
   s->ids_b.release();
@@ -1411,7 +1417,7 @@ void solver_trim(rpd_solver *s) {
 
 size_t solver_device_bytes(const rpd_solver *s) {
   const DevBuf *b[] = {&s->user, &s->stored, &s->perm, &s->user_to_stored, &s->weights, &s->counters, &s->bin_ws,
-                       &s->ring_bound, &s->knn, &s->knn_part, &s->knn_user, &s->counter64, &s->g_flags, &s->g_points,
+                       &s->ring_bound, &s->knn, &s->knn_part, &s->tri_count, &s->knn_user, &s->counter64, &s->g_flags, &s->g_points,
                        &s->g_tris, &s->g_list, &s->g_offsets, &s->g_sat, &s->g_tsat, &s->out, &s->status, &s->ids_a, &s->ids_b,
                        &s->ids_c, &s->fail_ws, &s->hist, &s->gather, &s->defer_slots, &s->defer_part, &s->defer_fail,
                        &s->defer_ctr, &s->defer_chunk_slot, &s->wmin, &s->used, &s->hess, &s->hessid};

@@ -96,6 +96,7 @@ struct rpd_solver {
   rpd::DevBuf status;          // int[n]
   rpd::DevBuf ids_a, ids_b, ids_c;  // int[n] failing-id lists
   rpd::DevBuf ids_range;       // int[count]: a part's stored ids (rpd_solver_launch_part)
+  rpd::DevBuf tri_count;       // int[n]: triangle counts of the triangle overflows (CellLaunch::tri_count)
   rpd::DevBuf fail_ws;         // flags + scans
   rpd::DevBuf hist;            // int[16]: status histogram + counts
   rpd::DevBuf gather;          // user-order staging for outputs
