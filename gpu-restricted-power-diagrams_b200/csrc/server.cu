@@ -2,7 +2,8 @@
 //
 // A session is one diagram kept on the device: its seeds and bins, its
 // neighbour table, its results, and a device copy of its domain grid shared
-// with every session on the same rpd_grid.  Requests (a new session's solve,
+// with every session on the same rpd_grid -- or its own domain, built on the
+// device from a seeded blob or a sampled implicit function.  Requests (a new session's solve,
 // or a weight-only re-solve of a session) wait in arrival order; a slot -- a
 // host thread with its own context and CUDA stream -- takes the first one
 // that can run: its session is not busy, and the device memory it needs fits
@@ -52,6 +53,11 @@ struct Request {
   std::vector<float> data;  // seeds (xyzw) or weights
   int n = 0;
   const rpd_grid *grid = nullptr;
+  // a domain built on the device by the session's own solver (no host grid)
+  int dom_kind = 0;          // kDomHost (none, or `grid`), kDomBlob, kDomField
+  int dom_size = 0, dom_nell = 0;
+  uint64_t dom_seed = 0;
+  std::vector<float> field;  // kDomField: (dom_size+1)^3 values, copied
   rpd_params params{};
   double *moments = nullptr;
   double *hessian = nullptr;  // --hessian rows (hessian_h > 0), user order
@@ -62,6 +68,8 @@ struct Request {
   bool finished = false;
   rpd_request_info info{};
 };
+
+constexpr int kDomHost = 0, kDomBlob = 1, kDomField = 2;
 
 struct GridHolder {
   rpd_solver *solver = nullptr;  // owns the device grid
@@ -78,6 +86,21 @@ size_t grid_bytes(const rpd_grid *g) {
   // triangles, lists
   return S * S * S * (1 + 4) + (S + 1) * (S + 1) * (S + 1) * 8 + size_t(np) * 16 + size_t(nt) * 12 +
          size_t(nl) * 4 + 4096;
+}
+
+// Device bytes of a domain built on the device at size^3 voxels: flags,
+// offsets, summed tables, and for the reservation a surface of 48 size^2
+// triangles (the session's actual bytes replace it after its solve).
+size_t device_grid_bytes(int size) {
+  const size_t S = size_t(size), S1 = S + 1;
+  return S * S * S * (1 + 4) + S1 * S1 * S1 * 8 + 48 * S * S * (12 + 4) + 24 * S * S * 16 + 4096;
+}
+
+// The build's workspace: per lattice point the field, edge mask, counts and
+// bases; per voxel the triangle counts; scan tiles.
+size_t device_grid_build_bytes(int size) {
+  const size_t S = size_t(size), S1 = S + 1;
+  return S1 * S1 * S1 * (4 + 1 + 4 + 4) + (S * S * S + 1) * 4 + (size_t(1) << 20);
 }
 
 // Device bytes a session keeps: seeds (given and binned), permutation and
@@ -199,6 +222,11 @@ struct rpd_server {
           const rpd_solver *g = grid_for(gh, r->grid, c);
           if (g) rpd::solver_share_grid(s->solver, g);
           else rc = RPD_ERR_CUDA;
+        } else if (s->solver && r->dom_kind == kDomBlob) {
+          rc = rpd_solver_set_grid_blob(s->solver, r->dom_size, r->dom_nell, r->dom_seed);
+        } else if (s->solver && r->dom_kind == kDomField) {
+          rc = rpd_solver_set_grid_field(s->solver, r->dom_size, r->field.data(), RPD_HOST);
+          std::vector<float>().swap(r->field);
         }
         if (s->solver && rc == RPD_OK) rc = rpd_solver_set_points(s->solver, r->data.data(), r->n, RPD_HOST);
       } else if (!s->solver || s->failed) {
@@ -344,14 +372,17 @@ int rpd_server_submit_solve(rpd_server *sv, const float *xyzw, int n, const rpd_
   return rpd_server_submit_solve_hessian(sv, xyzw, n, grid, p, moments, nullptr, nullptr, session);
 }
 
-int rpd_server_submit_solve_hessian(rpd_server *sv, const float *xyzw, int n, const rpd_grid *grid,
-                                    const rpd_params *p, double *moments, double *hessian, int *hessian_ids,
-                                    int *session) {
+}  // extern "C"
+
+namespace {
+
+// A new session's solve; r carries its domain (a host grid, or one to build
+// on the device, with the build's workspace in its transient bytes).
+int submit_new(rpd_server *sv, std::unique_ptr<Request> r, const float *xyzw, int n, const rpd_params *p,
+               double *moments, double *hessian, int *hessian_ids, int *session) {
   if (!sv || !xyzw || n <= 0) return RPD_ERR_INVALID;
-  auto r = std::make_unique<Request>();
   r->n = n;
   r->data.assign(xyzw, xyzw + size_t(n) * 4);
-  r->grid = grid;
   if (p) r->params = *p;
   else rpd_params_default(&r->params);
   if (r->params.hessian_h < 0 || (r->params.hessian_h > 0 && (!hessian || !hessian_ids))) return RPD_ERR_INVALID;
@@ -362,11 +393,15 @@ int rpd_server_submit_solve_hessian(rpd_server *sv, const float *xyzw, int n, co
   }
   r->need = transient_bytes(n, r->params);
   r->new_resident = resident_bytes(n, r->params);
+  if (r->dom_kind != kDomHost) {
+    r->need += device_grid_build_bytes(r->dom_size);
+    r->new_resident += device_grid_bytes(r->dom_size);
+  }
   std::lock_guard<std::mutex> lock(sv->mu);
   if (sv->stop) return RPD_ERR_INVALID;
-  if (grid && !sv->grids.count(grid)) {
-    sv->grids[grid] = std::make_unique<GridHolder>();
-    r->new_resident += grid_bytes(grid);  // reserved with the first session on it
+  if (r->grid && !sv->grids.count(r->grid)) {
+    sv->grids[r->grid] = std::make_unique<GridHolder>();
+    r->new_resident += grid_bytes(r->grid);  // reserved with the first session on it
   }
   auto s = std::make_unique<Session>();
   s->id = sv->next_session++;
@@ -376,6 +411,45 @@ int rpd_server_submit_solve_hessian(rpd_server *sv, const float *xyzw, int n, co
   if (session) *session = s->id;
   sv->sessions[s->id] = std::move(s);
   return sv->submit(std::move(r));
+}
+
+constexpr int kMaxDeviceGridSize = 1024;  // as rpd_solver_set_grid_blob / _field
+
+}  // namespace
+
+extern "C" {
+
+int rpd_server_submit_solve_hessian(rpd_server *sv, const float *xyzw, int n, const rpd_grid *grid,
+                                    const rpd_params *p, double *moments, double *hessian, int *hessian_ids,
+                                    int *session) {
+  auto r = std::make_unique<Request>();
+  r->grid = grid;
+  return submit_new(sv, std::move(r), xyzw, n, p, moments, hessian, hessian_ids, session);
+}
+
+int rpd_server_submit_solve_blob(rpd_server *sv, const float *xyzw, int n, int grid_size, int nellipsoids,
+                                 uint64_t grid_seed, const rpd_params *p, double *moments, double *hessian,
+                                 int *hessian_ids, int *session) {
+  if (grid_size < 1 || grid_size > kMaxDeviceGridSize || nellipsoids < 1 || nellipsoids > 4096)
+    return RPD_ERR_INVALID;
+  auto r = std::make_unique<Request>();
+  r->dom_kind = kDomBlob;
+  r->dom_size = grid_size;
+  r->dom_nell = nellipsoids;
+  r->dom_seed = grid_seed;
+  return submit_new(sv, std::move(r), xyzw, n, p, moments, hessian, hessian_ids, session);
+}
+
+int rpd_server_submit_solve_field(rpd_server *sv, const float *xyzw, int n, int grid_size, const float *field,
+                                  const rpd_params *p, double *moments, double *hessian, int *hessian_ids,
+                                  int *session) {
+  if (grid_size < 1 || grid_size > kMaxDeviceGridSize || !field) return RPD_ERR_INVALID;
+  auto r = std::make_unique<Request>();
+  r->dom_kind = kDomField;
+  r->dom_size = grid_size;
+  const size_t S1 = size_t(grid_size) + 1;
+  r->field.assign(field, field + S1 * S1 * S1);
+  return submit_new(sv, std::move(r), xyzw, n, p, moments, hessian, hessian_ids, session);
 }
 
 int rpd_server_submit_reweight(rpd_server *sv, int session, const float *w, const rpd_params *p, double *moments) {

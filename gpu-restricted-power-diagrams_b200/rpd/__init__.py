@@ -107,6 +107,12 @@ def lib():
                                                       C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
         L.rpd_server_submit_reweight_hessian.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                                          C.c_void_p, C.c_void_p]
+        L.rpd_server_submit_solve_blob.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint64,
+                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                   C.POINTER(C.c_int)]
+        L.rpd_server_submit_solve_field.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.POINTER(C.c_int)]
         L.rpd_server_wait.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.rpd_server_release.argtypes = [C.c_void_p, C.c_int]
         L.rpd_server_bytes_in_use.restype = C.c_size_t
@@ -820,19 +826,37 @@ class Server:
             return None
         return (np.zeros((n, p.hessian_h, p.hessian_hc), np.float64), np.zeros((n, p.hessian_h), np.int32))
 
-    def solve(self, xyzw, grid=None, params=None, **kw):
-        """Submits a new session's solve; returns (ticket, session).  With
+    def solve(self, xyzw, grid=None, params=None, blob=None, field=None, **kw):
+        """Submits a new session's solve; returns (ticket, session).  The
+        domain: a host Grid (shared by the sessions on it), or one built on
+        the device for this session alone -- blob=(size, nellipsoids, seed)
+        (rpd_grid_make_blob's domain) or field= an (S+1)^3 corner-lattice
+        field, domain {field < 0} (Solver.set_grid_field's layout).  With
         hessian_h > 0 the request also returns its Hessian rows (wait)."""
+        if sum(d is not None for d in (grid, blob, field)) > 1:
+            raise ValueError("one domain: grid, blob or field")
         x = as_xyzw(xyzw)
         p = params if params is not None else Params.default(**kw)
         out = np.zeros((len(x), 4), np.float64)
         hb = self._hessian_buffers(len(x), p)
+        hv, hi = (_ptr(hb[0]), _ptr(hb[1])) if hb else (None, None)
         sess = C.c_int(-1)
-        if grid is not None:
-            self._grids.append(grid)
-        t = lib().rpd_server_submit_solve_hessian(self.h, _ptr(x), len(x), grid.h if grid is not None else None,
-                                                  C.byref(p), _ptr(out), _ptr(hb[0]) if hb else None,
-                                                  _ptr(hb[1]) if hb else None, C.byref(sess))
+        if blob is not None:
+            size, nell, seed = blob
+            t = lib().rpd_server_submit_solve_blob(self.h, _ptr(x), len(x), int(size), int(nell), int(seed),
+                                                   C.byref(p), _ptr(out), hv, hi, C.byref(sess))
+        elif field is not None:
+            f = np.ascontiguousarray(field, np.float32).reshape(-1)
+            s1 = round(len(f) ** (1.0 / 3.0))
+            if s1 ** 3 != len(f) or s1 < 2:
+                raise ValueError("field must hold (S+1)^3 values")
+            t = lib().rpd_server_submit_solve_field(self.h, _ptr(x), len(x), s1 - 1, _ptr(f), C.byref(p),
+                                                    _ptr(out), hv, hi, C.byref(sess))
+        else:
+            if grid is not None:
+                self._grids.append(grid)
+            t = lib().rpd_server_submit_solve_hessian(self.h, _ptr(x), len(x), grid.h if grid is not None else None,
+                                                      C.byref(p), _ptr(out), hv, hi, C.byref(sess))
         if t < 0:
             raise RpdError(t, "submit solve")
         self._out[t] = (out, hb)

@@ -441,6 +441,22 @@ int rpd_server_submit_solve_hessian(rpd_server *sv, const float *xyzw, int n, co
                                     int *session);
 int rpd_server_submit_reweight_hessian(rpd_server *sv, int session, const float *w, const rpd_params *p,
                                        double *moments, double *hessian, int *hessian_ids);
+/* A new session whose domain is built on the device by its own solver, as
+ * rpd_solver_set_grid_blob / rpd_solver_set_grid_field build it: no host grid
+ * and no host preprocessing, e.g. for served requests with new domains (no
+ * counterpart in the reference, whose domains come from its host tool).
+ * The session keeps the domain for its re-solves; it is not shared with other
+ * sessions.  field: (grid_size+1)^3 floats (host memory, copied; the domain
+ * is {field < 0}).  grid_size <= 1024.  hessian / hessian_ids as in the
+ * _hessian forms (required when p->hessian_h > 0, else may be NULL).  The
+ * build's workspace counts in the request's memory, the domain in the
+ * session's. */
+int rpd_server_submit_solve_blob(rpd_server *sv, const float *xyzw, int n, int grid_size, int nellipsoids,
+                                 uint64_t grid_seed, const rpd_params *p, double *moments, double *hessian,
+                                 int *hessian_ids, int *session);
+int rpd_server_submit_solve_field(rpd_server *sv, const float *xyzw, int n, int grid_size, const float *field,
+                                  const rpd_params *p, double *moments, double *hessian, int *hessian_ids,
+                                  int *session);
 /* Blocks until the ticket's request is done and returns its status; each
  * ticket is waited for once. */
 int rpd_server_wait(rpd_server *sv, int ticket, rpd_request_info *info);

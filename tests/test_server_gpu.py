@@ -156,3 +156,69 @@ def test_hessian_rows_served(rpd):
     v4, i4 = ref2.hessian(40, 4)
     assert np.array_equal(m3, ref2.moments())
     assert np.array_equal(rows3[0], v4) and np.array_equal(rows3[1], i4)
+
+
+def test_domains_built_on_the_device(rpd):
+    """Sessions whose domains are built on the device (rpd_server_submit_solve_blob
+    / _field): a blob request equals a solver on the host-built blob (the same
+    triangles voxel by voxel), a field request equals a solver with the same
+    field, their weight-only re-solves keep the session's domain, and a
+    session on a shared host grid runs beside them; Hessian rows come back
+    through the blob form."""
+    x = jittered(24, seed=11, weights=True)
+    y = uniform(15000, seed=12)
+    z = jittered(20, seed=13, weights=True)
+    S = 40
+    g = np.arange(S + 1) / S
+    zz, yy, xx = np.meshgrid(g, g, g, indexing="ij")
+    f = (np.sqrt((xx - 0.5) ** 2 + (yy - 0.45) ** 2 + (zz - 0.55) ** 2) - 0.32).astype(np.float32)
+    host = rpd.Grid.blob(32, 5, 9)
+    kw = dict(K=50, P=30, V=40, T=100)
+    kwh = dict(kw, hessian_h=40, hessian_hc=1)
+    w = np.clip(x[:, 3] * 1.3, 0, None).astype(np.float32)
+    wy = np.full(len(y), 50.0, np.float32)
+    with rpd.Server(slots=3) as sv:
+        t1, s1 = sv.solve(x, blob=(48, 5, 2), **kwh)
+        t2, s2 = sv.solve(y, field=f, **kw)
+        t3, s3 = sv.solve(z, grid=host, **kw)
+        t4 = sv.reweight(s1, w, **kw)
+        t5 = sv.reweight(s2, wy, **kw)
+        m1, i1, rows1 = sv.wait(t1, hessian=True)
+        m2, i2 = sv.wait(t2)
+        m3, i3 = sv.wait(t3)
+        m4, i4 = sv.wait(t4)
+        m5, i5 = sv.wait(t5)
+        for s in (s1, s2, s3):
+            sv.release(s)
+        with pytest.raises(ValueError):
+            sv.solve(x, grid=host, blob=(48, 5, 2))
+        p = rpd.Params.default(**kw)
+        out = np.zeros((len(x), 4), np.float64)
+        sess = rpd.C.c_int(-1)
+        assert rpd.lib().rpd_server_submit_solve_blob(sv.h, rpd._ptr(x), len(x), 2000, 5, 2, rpd.C.byref(p),
+                                                      rpd._ptr(out), None, None, rpd.C.byref(sess)) < 0
+        assert rpd.lib().rpd_server_submit_solve_field(sv.h, rpd._ptr(x), len(x), 16, None, rpd.C.byref(p),
+                                                       rpd._ptr(out), None, None, rpd.C.byref(sess)) < 0
+    assert all(i["status"] == 0 for i in (i1, i2, i3, i4, i5))
+    ref = rpd.Solver().set_points(x).set_grid(rpd.Grid.blob(48, 5, 2))
+    ref.launch(**kwh)
+    assert np.array_equal(m1, ref.moments())
+    v, ids = ref.hessian(40, 1)
+    assert np.array_equal(rows1[0], v) and np.array_equal(rows1[1], ids)
+    x2 = x.copy()
+    x2[:, 3] = w
+    ref = rpd.Solver().set_points(x2).set_grid(rpd.Grid.blob(48, 5, 2))
+    ref.launch(**kw)
+    assert np.array_equal(m4, ref.moments())
+    ref = rpd.Solver().set_points(y).set_grid_field(f)
+    ref.launch(**kw)
+    assert np.array_equal(m2, ref.moments())
+    assert (m2[:, 3] > 0).sum() > len(y) // 10  # cells inside the domain
+    y2 = y.copy()
+    y2[:, 3] = wy
+    ref = rpd.Solver().set_points(y2).set_grid_field(f)
+    ref.launch(**kw)
+    assert np.array_equal(m5, ref.moments())
+    ref = rpd.Solver().set_points(z).set_grid(host)
+    ref.launch(**kw)
+    assert np.array_equal(m3, ref.moments())
