@@ -907,14 +907,16 @@ def run_batch_reference(args, cfg, rank):
     print(json.dumps(line), flush=True)
 
 
-def serve_stream(sv, rpd, cfg, rate, nreq, seed, grid_for, pool, keep_n=250_000):
+def serve_stream(sv, rpd, cfg, rate, nreq, seed, grid_for, pool, keep_n=250_000, device_domains=False):
     """One seeded Poisson stream of `nreq` requests at `rate` per second
     through the server: requests are submitted at their arrival times and a
     waiter thread collects them; the server's own clock gives each request's
     latency (submitted -> moments on the host).  Returns the finished
     requests (kind, n, info, moments, weights or None, grid size, t_done),
     the first arrival's wall time and the arrival times.  The weights of new
-    diagrams of at most keep_n seeds are kept (their seeds are pool[:n])."""
+    diagrams of at most keep_n seeds are kept (their seeds are pool[:n]).
+    device_domains: each new diagram's request brings its domain as a blob
+    that its session builds on the device, instead of a shared host grid."""
     import threading
 
     rng = np.random.default_rng(seed)
@@ -969,7 +971,10 @@ def serve_stream(sv, rpd, cfg, rate, nreq, seed, grid_for, pool, keep_n=250_000)
             h2 = (1000.0 / n ** (1 / 3)) ** 2
             x[:, 3] = rng.uniform(0.0, 0.1 * h2, n).astype(np.float32)
             S, g = grid_for(n)
-            t, sess = sv.solve(x, grid=g, **kw)
+            if device_domains:
+                t, sess = sv.solve(x, blob=(S, cfg["nell"], cfg["gseed"]), **kw)
+            else:
+                t, sess = sv.solve(x, grid=g, **kw)
             resident.append((sess, n, x[:, 3].copy()))
             if len(resident) > cfg["resident"]:
                 old = resident.pop(0)
@@ -1033,14 +1038,17 @@ def run_serve(args, cfg, rank):
         sv.wait(t)
         sv.wait(sv.reweight(sess, pool[:200_000, 3], **kw))
         sv.release(sess)
-        done, t0, arr = serve_stream(sv, rpd, cfg, cfg["rate"], cfg["requests"], cfg["sseed"] + 1, grid_for, pool)
+        dd = bool(args.device_domains)
+        done, t0, arr = serve_stream(sv, rpd, cfg, cfg["rate"], cfg["requests"], cfg["sseed"] + 1, grid_for, pool,
+                                     device_domains=dd)
         main = serve_summary(done, t0, arr, vols)
         capacity = main["value"]
         cells_per_req = sum(d[1] for d in done) / len(done)
         loads = {}
         for frac, seed in ((0.5, cfg["sseed"] + 2), (0.9, cfg["sseed"] + 3)):
             rate = frac * capacity / cells_per_req
-            dl, tl, al = serve_stream(sv, rpd, cfg, rate, cfg["requests_at_load"], seed, grid_for, pool)
+            dl, tl, al = serve_stream(sv, rpd, cfg, rate, cfg["requests_at_load"], seed, grid_for, pool,
+                                      device_domains=dd)
             loads[f"{int(frac * 100)}pct"] = dict(rate_per_s=rate, **serve_summary(dl, tl, al, vols))
     # served diagrams against the FP64 oracle, cell by cell
     import oracle
@@ -1093,7 +1101,9 @@ def run_serve(args, cfg, rank):
     line = {
         "metric": "served cells/s and p50/p99 latency", "value": main["value"], "unit": "cells/s",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f64 geometry on f32 seeds", "data": "synthetic",
-        "config": {"workload": "serve-200rps", "description": cfg["desc"], "slots": slots},
+        "config": {"workload": "serve-200rps", "description": cfg["desc"], "slots": slots,
+                   "domains": ("built on the device by each new session (rpd_server_submit_solve_blob)"
+                               if args.device_domains else "host grids, one per size, shared by the sessions")},
         "p50_ms": main["p50_ms"], "p99_ms": main["p99_ms"], "configured_rate": main,
         "at_load": loads,
         "note": "the configured 200 requests/s offers more cells than one GPU sustains, so its latency is queue "
@@ -1117,6 +1127,8 @@ def main():
                     help="single-diagram configs with --gpus N > 1: the ranks split one diagram (strong scaling) "
                          "instead of solving one each")
     ap.add_argument("--slots", type=int, default=None, help="serving configs: concurrent slots (default: the config's)")
+    ap.add_argument("--device-domains", action="store_true",
+                    help="serving configs: each new session builds its domain on the device")
     ap.add_argument("--outside-probe", action="store_true",
                     help="solve with RPD_FLAG_OUTSIDE_PROBE: cells proven outside the domain are settled before "
                          "the first pass (moments equal; a cell the reference never settles reads success)")
