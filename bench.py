@@ -357,7 +357,7 @@ def precision_modes(solver, cfg, sample, flush, steps=6, warmup=3):
             e["bitwise_equal_to_fp64_mode"] = bool(np.array_equal(m, base[0]) and np.array_equal(stt, base[1]))
         out[name] = e
     out["mixed_over_fp32"] = out["mixed"]["value"] / out["fp32"]["value"]
-    out["target"] = ("north-star target: the mixed form >= 1.5x the plain FP32 path at <= 1e-5 mass error; " +
+    out["target"] = ("target: the mixed form >= 1.5x the plain FP32 path at <= 1e-5 mass error; " +
                      ("met" if out["mixed_over_fp32"] >= 1.5 else "missed") +
                      f" ({out['mixed_over_fp32']:.2f}x)")
     return out

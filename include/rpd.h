@@ -30,7 +30,7 @@ typedef enum rpd_error {
   RPD_ERR_IO = -5,          /* file could not be read or written */
   RPD_ERR_FORMAT = -6,      /* malformed grid or seed file */
   RPD_ERR_DEGENERATE = -7,  /* seeds too clustered for the bin grid */
-  RPD_ERR_CAPACITY = -8     /* a cap (K, P, V, T) beyond what this build supports */
+  RPD_ERR_CAPACITY = -8     /* a cap (K, P, V, T) beyond what the library supports */
 } rpd_error;
 
 /* Per-cell status, the values of the reference's Status enum (Status.h:4-16). */
