@@ -11,13 +11,16 @@
 // writes the next pass's launch records and row prefixes; the neighbour and
 // cell kernels are persistent and read their rows from those prefixes.  The
 // launch shapes are fixed at capture: pass j's shared-memory layout holds
-// the largest caps any diagram can reach by pass j (the first-pass maxima
-// grown j times), so a pass never needs the host.
+// the first-pass maxima of K and T grown j times and of P and V grown at most
+// kLayoutGrowths times (P and V grow only in diagrams with plane or vertex
+// overflows, T in every pass of the heavy boundary cells), so a pass never
+// needs the host.
 //
-// A diagram whose schedule does not fit the capture (its retry neighbour
-// rows overflow the shared table, or it would run more passes than were
-// captured) is marked unfinished and solved again on its own afterwards;
-// results are deterministic, so they are the same either way.
+// A diagram whose schedule does not fit the capture (its caps outgrow the
+// pass's layout, its retry neighbour rows overflow the shared table, or it
+// would run more passes than were captured) is marked unfinished and solved
+// again on its own afterwards; results are deterministic, so they are the
+// same either way.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -400,6 +403,12 @@ int grow(int x, int times) {
   return x;
 }
 
+// Growths of P and V the retry passes' layouts hold.  Layouts sized for
+// every possible growth (V x7.6 by the sixth pass) ran the late passes at a
+// quarter of the warps; on the uneven 256-diagram batch no diagram grows P
+// or V more than twice.
+constexpr int kLayoutGrowths = 2;
+
 }  // namespace batch_detail
 }  // namespace rpd
 
@@ -650,10 +659,12 @@ int capture(rpd_batch *b) {
   const long probe_rows = probe_start.back();
   all_start[nd] = int(cells);
   b->cells = cells;
-  // caps the launches of pass j hold: the first-pass maxima grown j times
+  // caps the launches of pass j hold: the first-pass maxima grown j times,
+  // P and V at most kLayoutGrowths times
   std::vector<int> Pb, Vb, Tb, Kb;
   for (int j = 0; j <= J; ++j) {
-    const int P = std::min(grow(Pmax, j), kMaxP), V = std::min(grow(Vmax, j), kMaxV),
+    const int jl = std::min(j, kLayoutGrowths);
+    const int P = std::min(grow(Pmax, jl), kMaxP), V = std::min(grow(Vmax, jl), kMaxV),
               T = std::min(grow(Tmax, j), kMaxT), K = std::min(grow(Kmax, j), kMaxK);
     if ((any_grid && !cell_caps_fit(P, V, T, true, hess_hc)) || (any_plain && !cell_caps_fit(P, V, T, false, hess_hc)))
       break;

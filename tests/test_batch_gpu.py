@@ -84,6 +84,7 @@ def test_batch_equals_solves_alone(rpd):
     st = b.stats()
     assert st["diagrams"] == 12 and st["cells"] == sum(len(s["xyzw"]) for s in sp)
     assert st["max_passes"] >= 3 and st["captures"] == 1
+    print("solved alone", st["solved_alone"], [v.stats()["passes"][-1] for v in solvers])
     assert st["probe_outside"] > 0  # the domains leave plainly-outside seeds to prove
     assert solvers[9].stats()["probe_outside"] == 0 and solvers[0].stats()["probe_outside"] == 0
     for i, s in enumerate(sp):
