@@ -758,13 +758,38 @@ def run_batch(args, cfg, rank, world, local):
     cell_avg_ms = sum(cell_ms) / len(cell_ms)
     achieved = alg_bytes / (cell_avg_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_cell_{args.config}_traffic.txt")
-    if os.path.exists(prof):
-        with open(prof) as f:
-            for ln in f:
-                if ln.startswith("bytes_per_launch"):
-                    traffic = int(ln.split("=")[1].strip())
+    # the bound is instruction issue, as for the single solve's cell kernel:
+    # warp instructions per cell from the committed ncu counters of the
+    # batch's first 32 diagrams (every cell a row), scaled to this launch
+    rows = n - int(bstats.get("probe_outside", 0))
+    prof = profile_counters(args.config, "k_cell_batch")
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    issue_peak = 148 * SMSP_PER_SM * sm_mhz * 1e6 / 1e9
+    roofline = {"kernel": "k_cell_batch (first pass, all diagrams)", "bound": "issue",
+                "unit": "G warp-instructions/s", "peak": issue_peak,
+                "peak_source": f"148 SMs x {SMSP_PER_SM} schedulers x {sm_mhz:.0f} MHz (SM clock sampled during "
+                               "the timed steps)", "launch_ms": cell_avg_ms, "rows": rows,
+                "note": "timed by event nodes inside the graph"}
+    if prof.get("rows") and not args.outside_probe:
+        scale = rows / prof["rows"]
+        inst = prof["warp_instructions_per_launch"] * scale
+        fp64 = prof["fp64_flops_per_launch"] * scale
+        roofline.update({"achieved": inst / (cell_avg_ms / 1e3) / 1e9,
+                         "frac": inst / (cell_avg_ms / 1e3) / 1e9 / issue_peak,
+                         "warp_instructions_per_launch": inst, "traffic": int(prof["bytes_per_launch"] * scale),
+                         "fp64": {"achieved": fp64 / (cell_avg_ms / 1e3) / 1e12, "unit": "TFLOP/s",
+                                  "peak": MEASURED_FP64_TFLOPS, "peak_source": "measured (DFMA microbenchmark)",
+                                  "frac": fp64 / (cell_avg_ms / 1e3) / 1e12 / MEASURED_FP64_TFLOPS,
+                                  "flops_per_launch": fp64,
+                                  "work": "executed FP64 instructions (2 DFMA + DADD + DMUL)"},
+                         "counters_source": f"profiles/k_cell_batch_{args.config}_counters.txt (ncu, the first 32 "
+                                            "diagrams' launch, scaled per cell)"})
+    else:
+        roofline.update({"achieved": None, "frac": None, "traffic": None,
+                         "note": "timed by event nodes inside the graph; committed ncu counters are of the "
+                                 "launch without the outside probe"})
+    roofline["hbm"] = {"achieved": achieved, "unit": "GB/s", "peak": peak, "peak_source": peak_kind,
+                       "frac": achieved / peak, "alg_bytes_per_launch": alg_bytes}
     sizes = [len(s["xyzw"]) for s in specs]
     line = {
         "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
@@ -781,10 +806,7 @@ def run_batch(args, cfg, rank, world, local):
                 "path": "rpd_solver_set_points(host) x256 + rpd_batch_launch + rpd_solver_get_moments(host) x256",
                 "recaptures": recaptured},
         "gpu_launches": int(bstats["kernel_launches"] * args.steps),
-        "roofline": {"kernel": "k_cell_batch (first pass, all diagrams)", "bound": "hbm", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "launch_ms": cell_avg_ms,
-                     "note": "timed by event nodes inside the graph; an issue-bound FP64 clipping kernel"},
+        "roofline": roofline,
         "clocks": clk,
         "sequential": {"value": seq_rate, "unit": "cells/s", "device_only_value": seq_dev_rate,
                        "path": "rpd_solver_launch per diagram, one after another (wall clock, host syncs "
