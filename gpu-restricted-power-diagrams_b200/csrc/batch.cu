@@ -592,7 +592,7 @@ int capture(rpd_batch *b) {
   const std::vector<DiagStatic> &G = b->statics;
   long long cells = 0, table = 0;
   int Kmin = kMaxK, Kmax = 0, Pmax = 0, Vmax = 0, Tmax = 0, J = 0;
-  bool any_grid = false, any_plain = false, defer = true, any_safe = false;
+  bool any_grid = false, any_plain = false, defer = true, any_safe = false, all_disjoint = true;
   int hess_hc = 0;  // the Hessian rows' HC of the diagrams that ask for rows (one for the batch)
   bool class_used[kKnnClasses] = {};
   long class_rows[kKnnClasses] = {};
@@ -610,6 +610,7 @@ int capture(rpd_batch *b) {
     Tmax = std::max(Tmax, g.T0);
     J = std::max(J, g.max_extra);
     (g.grid.size > 0 ? any_grid : any_plain) = true;
+    if (g.grid.size > 0 && !g.grid.lists_disjoint) all_disjoint = false;
     if (g.safe_radius) any_safe = true;
     if (b->params[d].flags & RPD_FLAG_NO_DEFER) defer = false;
     if (g.H > 0) {
@@ -898,6 +899,7 @@ int capture(rpd_batch *b) {
     cb.T = Tb[j];
     cb.T_slot = j == 0 && dq.slots ? Tslot0 : 0;
     cb.HC = hess_hc;
+    cb.disjoint = all_disjoint;
     cb.after_cell = j == 0 ? b->ev[2] : nullptr;
     // the first pass's rows are every cell: one warp per row; the retries'
     // rows are known on the device only: persistent, rows from a counter

@@ -15,7 +15,8 @@ cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count,
   if (b.safe) return cell_batch_launch_safe(b, st, sm_count, launches);
   if (b.P > kMaxP || b.V > kMaxV || b.T > kMaxT || b.P < 7 || b.V < 8) return cudaErrorInvalidValue;
   if (b.HC && b.defer.slots) return cudaErrorInvalidValue;  // Hessian rows are summed inline
-  const Layout Lg = make_layout(b.P, b.V, b.T, true, b.HC, b.T_slot), Lp = make_layout(b.P, b.V, b.T, false, b.HC);
+  const Layout Lg = make_layout(b.P, b.V, b.T, true, b.HC, b.T_slot, 0, b.disjoint),
+               Lp = make_layout(b.P, b.V, b.T, false, b.HC);
   if (b.defer.slots && (b.defer.slot_bytes < slot_bytes_for(Lg, Lg.T) || b.defer.max_chunks * b.defer.chunk < Lg.T))
     return cudaErrorInvalidValue;
   const int vs = Lg.Vc / 32;
@@ -35,7 +36,8 @@ cudaError_t cell_launch(const CellLaunch &a, cudaStream_t st, int sm_count, int 
   if (a.P > kMaxP || a.V > kMaxV || a.T > kMaxT || a.P < 7 || a.V < 8) return cudaErrorInvalidValue;
   if (a.hess && (a.defer.slots || a.H < 1 || (a.HC != 1 && a.HC != 4))) return cudaErrorInvalidValue;
   if (a.T_ahead > kMaxT || (a.T_ahead > a.T && (!a.defer.slots || a.hess))) return cudaErrorInvalidValue;
-  const Layout L = make_layout(a.P, a.V, a.T, a.grid.size > 0, a.hess ? a.HC : 0, a.T_ahead);
+  const Layout L = make_layout(a.P, a.V, a.T, a.grid.size > 0, a.hess ? a.HC : 0, a.T_ahead, 0,
+                               a.grid.lists_disjoint != 0);
   if (a.defer.slots && (a.defer.slot_bytes < slot_bytes_for(L, L.T) || a.defer.max_chunks * a.defer.chunk < L.T))
     return cudaErrorInvalidValue;
   const int vs = L.Vc / 32;

@@ -201,6 +201,7 @@ struct CellBatch {
   int *work = nullptr;  // one device int: the row counter of persistent launches (optional)
   bool safe = false;    // a diagram uses the weighted security-radius guard (its launch record decides)
   int HC = 0;           // Hessian rows' components (a diagram with rows; then no defer queue), else 0
+  bool disjoint = false;  // every diagram's grid lists each triangle in one voxel (a smaller id buffer)
 };
 cudaError_t cell_batch_launch(const CellBatch &b, cudaStream_t st, int sm_count, int *launches = nullptr);
 // The same with the guard compiled in (cell_safe.cu).

@@ -80,15 +80,18 @@ __host__ __device__ inline int pow2_at_least(int x) {
 
 // T: the pass's triangle cap (the warp's id buffer); t_slot: the ids a
 // parked cell's slot holds, when more than T (triangle overflows parked
-// ahead, CellLaunch::T_ahead).
+// ahead, CellLaunch::T_ahead).  disjoint: every grid of the launch lists
+// each triangle in one voxel only (DevGrid::lists_disjoint), so a cell's ids
+// are gathered without repeats and the buffer needs T of them; otherwise 2T,
+// the gathered ids being sorted and their repeats dropped in place.
 __host__ __device__ inline Layout make_layout(int P, int V, int T, bool grid, int hc = 0, int t_slot = 0,
-                                              int prec = 0) {
+                                              int prec = 0, bool disjoint = false) {
   Layout L;
   L.HC = hc;
   L.prec = prec;
   L.Pc = (P + 3) & ~3;
   L.Vc = (V + 31) & ~31;
-  L.G = grid ? pow2_at_least(2 * T) : 0;
+  L.G = grid ? (disjoint ? (T + 31) & ~31 : pow2_at_least(2 * T)) : 0;
   L.Mw = (L.Pc + 31) / 32;
   L.T = T > t_slot ? T : t_slot;
   unsigned o = 0;
