@@ -51,8 +51,10 @@ struct DeferQueue {
   unsigned char *slots = nullptr;  // capacity slots of slot_bytes
   int capacity = 0;
   size_t slot_bytes = 0;
-  // [0] cells parked, [1] next work item, [2] chunks taken, [3] the largest
-  // triangle count parked ahead (CellLaunch::T_ahead); zeroed before a pass
+  // [0] cells parked, [1] next work item (cells with an inner apex), [2]
+  // chunks taken, [3] the largest triangle count parked ahead
+  // (CellLaunch::T_ahead), [4] next work item (cells with the reference's
+  // start corner); zeroed before a pass
   int *counters = nullptr;
   // Work items are chunks, numbered compactly: a parked cell takes its
   // chunks' range from counters[2] and writes its slot for each of them
@@ -125,7 +127,7 @@ struct CellLaunch {
 };
 constexpr int kParkOverflow = 101;  // internal status: the queue was full
 constexpr int kProbeMiss = 102;     // internal status: the outside probe proved nothing
-constexpr int kDeferCounters = 4;   // ints of DeferQueue::counters
+constexpr int kDeferCounters = 5;   // ints of DeferQueue::counters
 constexpr int kTraceRecord = 12;
 
 // Largest caps of one build: P <= 255 (uchar plane ids in the reference,

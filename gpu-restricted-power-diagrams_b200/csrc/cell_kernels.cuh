@@ -2985,14 +2985,22 @@ struct BatchDesc {
   __device__ __forceinline__ const CellLaunch &operator()(int d) const { return descs[d]; }
 };
 
-template <int VS, class Desc>
+// MODE: kConeAll every work item; kConeInner the items of cells with an
+// apex inside (facet pieces), kConeCorner those with the reference's start
+// corner (cone clipping), each from its own counter.  Two launches, one per
+// kind, keep each kernel's code small: a warp running one kind beside warps
+// running the other stalls on instruction fetch.
+constexpr int kConeAll = 0, kConeInner = 1, kConeCorner = 2;
+
+template <int VS, class Desc, int MODE = kConeAll>
 __device__ __forceinline__ void cone_items(const DeferQueue &dq, const Layout &L, Desc desc, unsigned char *wsmem,
                                            int lane) {
   WarpCell w = bind(wsmem, L);
   const int items = min(*(volatile int *)&dq.counters[2], dq.capacity * dq.max_chunks);
+  int *next = &dq.counters[MODE == kConeCorner ? 4 : 1];
   for (;;) {
     int item = 0;
-    if (lane == 0) item = atomicAdd(&dq.counters[1], 1);
+    if (lane == 0) item = atomicAdd(next, 1);
     item = __shfl_sync(kFull, item, 0);
     if (item >= items) break;
     const int slot = dq.chunk_slot[item];
@@ -3001,6 +3009,8 @@ __device__ __forceinline__ void cone_items(const DeferQueue &dq, const Layout &L
     const int nuniq = h->nuniq, chunk = item - h->chunk_base;
     const int t0 = chunk * dq.chunk;
     if (t0 >= nuniq) continue;
+    if (MODE == kConeInner && h->inner == 0) continue;
+    if (MODE == kConeCorner && h->inner != 0) continue;
     const int t1 = min(t0 + dq.chunk, nuniq);
     const int nv = h->nv, np = h->np, sid = h->sid;
     const Plane *pl = reinterpret_cast<const Plane *>(base + sizeof(DeferHeader));
@@ -3008,7 +3018,7 @@ __device__ __forceinline__ void cone_items(const DeferQueue &dq, const Layout &L
     const double *vy = vx + L.Vc, *vz = vy + L.Vc, *vw = vz + L.Vc, *vd = vw + L.Vc;
     const unsigned *vt = reinterpret_cast<const unsigned *>(vd + L.Vc);
     const int *tl = reinterpret_cast<const int *>(vt + L.Vc);
-    const bool inner = h->inner != 0;
+    const bool inner = MODE == kConeAll ? h->inner != 0 : MODE == kConeInner;
     const CellLaunch &a = desc(h->diag);
     if constexpr (Desc::kBatch) w.vc = vertex_capacity(a, L);
     for (int i = lane; i < np; i += 32) w.plane[i] = pl[i];
@@ -3054,18 +3064,20 @@ __device__ __forceinline__ void cone_items(const DeferQueue &dq, const Layout &L
   }
 }
 
-template <int VS>
+template <int VS, int MODE>
 __global__ void __launch_bounds__(128, 4) k_cone(const __grid_constant__ CellLaunch a, const __grid_constant__ Layout L) {
   extern __shared__ __align__(16) unsigned char smem[];
-  cone_items<VS>(a.defer, L, SingleDesc{&a}, smem + size_t(threadIdx.x >> 5) * L.total, threadIdx.x & 31);
+  cone_items<VS, SingleDesc, MODE>(a.defer, L, SingleDesc{&a}, smem + size_t(threadIdx.x >> 5) * L.total,
+                                   threadIdx.x & 31);
 }
 
-template <int VS>
+template <int VS, int MODE>
 __global__ void __launch_bounds__(128, 4)
     k_cone_batch(const CellLaunch *__restrict__ descs, const __grid_constant__ DeferQueue dq,
                  const __grid_constant__ Layout L) {
   extern __shared__ __align__(16) unsigned char smem[];
-  cone_items<VS>(dq, L, BatchDesc{descs}, smem + size_t(threadIdx.x >> 5) * L.total, threadIdx.x & 31);
+  cone_items<VS, BatchDesc, MODE>(dq, L, BatchDesc{descs}, smem + size_t(threadIdx.x >> 5) * L.total,
+                                  threadIdx.x & 31);
 }
 
 // Per parked cell: its in-domain part plus the chunk partials in order; the
@@ -3172,11 +3184,13 @@ cudaError_t launch_vs(const CellLaunch &a, const Layout &L, cudaStream_t st, int
     if (e != cudaSuccess) return e;
     k_cell<VS, true, false, PREC, SAFE><<<blocks, warps_per_block * 32, smem, st>>>(a, L);
     if (a.after_cell) cudaEventRecord(a.after_cell, st);
-    e = allow_smem(reinterpret_cast<const void *>(k_cone<VS>), smem);
-    if (e != cudaSuccess) return e;
-    k_cone<VS><<<sm_count * 4, warps_per_block * 32, smem, st>>>(a, L);
+    if ((e = allow_smem(reinterpret_cast<const void *>(k_cone<VS, kConeInner>), smem)) != cudaSuccess ||
+        (e = allow_smem(reinterpret_cast<const void *>(k_cone<VS, kConeCorner>), smem)) != cudaSuccess)
+      return e;
+    k_cone<VS, kConeInner><<<sm_count * 4, warps_per_block * 32, smem, st>>>(a, L);
+    k_cone<VS, kConeCorner><<<sm_count * 4, warps_per_block * 32, smem, st>>>(a, L);
     k_cone_finish<<<(a.defer.capacity + 127) / 128, 128, 0, st>>>(a, L);
-    if (launches) *launches += 3;
+    if (launches) *launches += 4;
   } else if (a.grid.size > 0) {
     e = allow_smem(reinterpret_cast<const void *>(k_cell<VS, true, true, PREC, SAFE>), smem);
     if (e != cudaSuccess) return e;
@@ -3258,14 +3272,18 @@ cudaError_t launch_batch_vs(const CellBatch &b, const Layout &Lg, const Layout &
   if ((e = record_after_cell(b, st)) != cudaSuccess) return e;
   const int wpb = warps_per_block_for(Lg);
   const size_t smem = size_t(Lg.total) * wpb;
-  auto kc = k_cone_batch<VS>;
-  if ((e = allow_smem(reinterpret_cast<const void *>(kc), smem)) != cudaSuccess) return e;
-  kc<<<resident_blocks(kc, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(b.descs, b.defer, Lg);
+  auto ki = k_cone_batch<VS, kConeInner>;
+  auto kr = k_cone_batch<VS, kConeCorner>;
+  if ((e = allow_smem(reinterpret_cast<const void *>(ki), smem)) != cudaSuccess ||
+      (e = allow_smem(reinterpret_cast<const void *>(kr), smem)) != cudaSuccess)
+    return e;
+  ki<<<resident_blocks(ki, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(b.descs, b.defer, Lg);
+  kr<<<resident_blocks(kr, wpb * 32, smem, sm_count), wpb * 32, smem, st>>>(b.descs, b.defer, Lg);
   k_cone_finish_batch<<<sm_count * 4, 128, 0, st>>>(b.descs, b.defer, Lg);
   if ((e = batch_cells<VS, true, true, SAFE>(b.descs_inline, b.start_grid, b.ndiag, Lg, kParkOverflow, b.defer.counters,
                                        b.defer.capacity, -1, b.work, st, sm_count)) != cudaSuccess)
     return e;
-  if (launches) *launches += 4;
+  if (launches) *launches += 5;
   return cudaGetLastError();
 }
 
